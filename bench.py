@@ -1,0 +1,377 @@
+"""FDTD time-stepping throughput on B200 (Mcell-updates/s).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload plain_16x16|plain_8x8] [--kernel auto|split|fused]
+
+One step is one Yee time step (H + CPML + injection + E + CPML + injection +
+six phasor planes) of the whole grid. The default workload is the full-size
+plain solve: 16x16 wavelengths, 3 wavelengths of material, cell 0.021 wl
+(203 x 761 x 761 cells, 5.4 GHz, VV), float32, with a seeded synthetic
+snowpack-over-rough-soil material and seeded synthetic incident planes.
+
+``value`` is device time of exactly K steps with all inputs resident in HBM
+(CUDA events on the launching stream, max over ranks). ``e2e`` is the same
+metric through the C-ABI with host buffers: Ca/Cb upload, per-step incident
+planes from pinned host memory, K steps, and the 24 phasor planes read back.
+With N GPUs every rank runs its own replica (the reference farms whole
+material models to workers; nothing is exchanged inside a model).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, 'sar-pixel-simulator_b200'))
+
+BYTES_PER_CELL = {'float32': 56, 'float64': 112}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=200)
+    ap.add_argument('--warmup', type=int, default=5)
+    ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+    ap.add_argument('--workload', default='plain_16x16', choices=['plain_16x16', 'plain_8x8'])
+    ap.add_argument('--kernel', default='auto', choices=['auto', 'split', 'fused'])
+    ap.add_argument('--dtype', default='float32', choices=['float32', 'float64'])
+    ap.add_argument('--no-e2e', action='store_true')
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--cpu-steps', type=int, default=2)
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# workload
+# ---------------------------------------------------------------------------
+def build_workload(name, dtype, nsteps_inc, seed=2024):
+    from fdtdsarsim_b200 import synthetic
+    from fdtdsarsim_b200.materials import compute_material_arrays
+    pc = synthetic.config_params(name, dtype)
+    g = pc.geom_params
+    rng = np.random.default_rng(seed)
+    if name == 'plain_16x16':
+        model = synthetic.snowpack_over_rough_soil(pc, rng)
+    else:
+        model = synthetic.rough_lognormal_soil(pc, rng)
+    ca, cb = compute_material_arrays(pc, model)
+    # The timed window covers steps t < size_t_inc of a full solve, so every
+    # timed step injects, as the first 1372 steps of the real solve do. Only
+    # the planes of the steps that run are synthesised.
+    g.size_t_inc = min(g.size_t_inc, nsteps_inc)
+    inc = {}
+    for comp, scale in (('ex', 1.0), ('ey', 1.0), ('hx', 1 / 376.73), ('hy', 1 / 376.73)):
+        inc[comp] = (scale * rng.standard_normal((g.size_t_inc, g.size_y, g.size_x))).astype(dtype)
+    return pc, ca, cb, inc
+
+
+def workload_desc(pc, name):
+    g = pc.geom_params
+    return {
+        'workload': f'{name}: plain solve {g.size_z}x{g.size_y}x{g.size_x} cells '
+                    f'(nz x ny x nx), cell {g.cell_size:.6g} m, '
+                    f'{pc.inc_beam_params.polarization}, theta 20 deg, 5.4 GHz',
+        'grid': [g.size_z, g.size_y, g.size_x],
+        'cells': g.size_z * g.size_y * g.size_x,
+        'size_t_full_solve': g.size_t,
+        'npml': g.size_pml,
+        'materials': 'synthetic seeded (snowpack of ice spheres over rough soil)'
+        if name == 'plain_16x16' else 'synthetic seeded (rough lognormal soil)',
+        'incident': 'synthetic seeded planes, injected every timed step',
+        'l2': 'inputs larger than L2 (fields alone 2.8 GB)',
+    }
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+             'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+             'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix='.csv')
+            os.close(fd)
+            self.fh = open(self.path, 'w')
+            self.proc = subprocess.Popen(
+                ['nvidia-smi', '-i', str(self.device), f'--query-gpu={self.QUERY}',
+                 '--format=csv,noheader,nounits', '-lms', '100'], stdout=self.fh,
+                stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.fh.close()
+        rows = []
+        with open(self.path) as fh:
+            for line in fh:
+                parts = [p.strip() for p in line.split(',')]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace('.', '').isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace('.', '').isdigit()]
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == 'active'})
+        return {'sm_mhz': statistics.median(sm) if sm else None,
+                'sm_max_mhz': max(mx) if mx else None, 'reasons': reasons,
+                'samples': len(rows)}
+
+
+def measured_peak_hbm():
+    path = os.path.join(ROOT, 'MEASURED_PEAKS.json')
+    try:
+        with open(path) as fh:
+            return float(json.load(fh)['hbm_gbs']), 'measured'
+    except (OSError, KeyError, ValueError):
+        return 6650.0, 'fallback'
+
+
+def committed_traffic(kernel_name, workload):
+    """dram bytes per launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, 'profiles', 'traffic.json')
+    try:
+        with open(path) as fh:
+            d = json.load(fh)
+        return d.get(workload, {}).get(kernel_name)
+    except (OSError, ValueError):
+        return None
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline (the oracle: CPU restatement of the reference's algorithm)
+# ---------------------------------------------------------------------------
+def cpu_baseline(pc, ca, cb, inc, steps):
+    sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+    import fdtd_oracle as O
+    from fdtdsarsim_b200.absorbers import cpml_profiles
+    g = pc.geom_params
+    sim = O.OracleSim(g.size_x, g.size_y, g.size_z, g.size_pml, g.tfsf_z, g.cell_size,
+                      g.timestep, pc.inc_beam_params.frequency, pc.processing_params.datatype,
+                      cpml_profiles(pc))
+    sim.step(ca, cb, inc)  # first-touch of every array, untimed
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        sim.step(ca, cb, inc)
+    dt = time.perf_counter() - t0
+    cells = g.size_x * g.size_y * g.size_z
+    return {'value': cells * steps / dt / 1e6, 'unit': 'Mcell-updates/s', 'cores': 1,
+            'kind': 'port',
+            'sample': f'{steps} time steps of the full {g.size_z}x{g.size_y}x{g.size_x} grid '
+                      f'(numpy oracle, one thread), after one untimed step'}
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(a):
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    if world > 1:
+        import datetime
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device('cuda', local))
+    torch.cuda.set_device(local)
+    from fdtdsarsim_b200 import _native
+    from fdtdsarsim_b200.absorbers import packed_profiles
+    from fdtdsarsim_b200.gpu.main_sim import native_geometry
+    from fdtdsarsim_b200 import tuning
+
+    pc, ca, cb, inc = build_workload(a.workload, a.dtype, a.warmup + a.steps + 1)
+    g = pc.geom_params
+    cells = g.size_x * g.size_y * g.size_z
+    geom = native_geometry(pc)
+    kernel = {'auto': None, 'split': _native.FDTD_KERNEL_SPLIT,
+              'fused': _native.FDTD_KERNEL_FUSED}[a.kernel]
+    choice = tuning.choose(geom, kernel=kernel)
+
+    def new_sim():
+        sim = _native.NativeSim(geom, local)
+        sim.set_absorbers(packed_profiles(pc))
+        sim.set_option(_native.OPT_KERNEL, choice['kernel'])
+        if choice['kernel'] == _native.FDTD_KERNEL_FUSED:
+            sim.set_option(_native.OPT_TILE_X, choice['tile_x'])
+            sim.set_option(_native.OPT_TILE_Y, choice['tile_y'])
+        return sim
+
+    stream = torch.cuda.current_stream()
+    sim = new_sim()
+    sim.set_stream(stream.cuda_stream)
+    sim.set_materials(ca, cb)
+    sim.set_incident(inc['ex'], inc['ey'], inc['hx'], inc['hy'])
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # warm-up
+    sim.run(a.warmup)
+    sim.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    sim.run(a.steps)
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms = t_start.elapsed_time(t_end)
+    ms_t = torch.tensor([ms], dtype=torch.float64, device='cuda')
+    if world > 1:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    value = world * cells * a.steps / (ms_max / 1e3) / 1e6
+    launches_per_step = 3 if choice['kernel'] == _native.FDTD_KERNEL_SPLIT else 2
+    gpu_launches = launches_per_step * a.steps + 1
+
+    # live per-kernel timing for the roofline (separate pass, same state)
+    sim.reset()
+    sim.run(a.warmup)
+    sim.synchronize()
+    sim.clear_kernel_time()
+    sim.set_option(_native.OPT_TIMING, 1)
+    nprof = min(a.steps, 60)
+    sim.run(nprof)
+    step_ms, step_n = sim.kernel_time(_native.TIME_STEP)
+    ph_ms, ph_n = sim.kernel_time(_native.TIME_PHASOR)
+    sim.set_option(_native.OPT_TIMING, 0)
+    kname = 'fused_step' if choice['kernel'] == _native.FDTD_KERNEL_FUSED else 'split_h_e'
+    avg_ms = step_ms / max(step_n, 1)
+    alg_bytes = cells * BYTES_PER_CELL[a.dtype]
+    peak, peak_kind = measured_peak_hbm()
+    achieved = alg_bytes / (avg_ms / 1e3) / 1e9
+    roofline = {'bound': 'hbm', 'achieved': round(achieved, 1), 'peak': peak, 'unit': 'GB/s',
+                'frac': round(achieved / peak, 4), 'traffic': committed_traffic(kname, a.workload),
+                'kernel': kname, 'peak_source': peak_kind,
+                'algorithmic_bytes_per_launch': alg_bytes,
+                'avg_launch_ms': round(avg_ms, 4),
+                'phasor_kernel_avg_ms': round(ph_ms / max(ph_n, 1), 4),
+                'step_share_of_device_time': round(step_ms / max(step_ms + ph_ms, 1e-9), 4)}
+    sim.close()
+    del sim
+
+    # end to end through the C-ABI with host buffers
+    e2e = None
+    if not a.no_e2e:
+        pin = {}
+        for k, v in inc.items():
+            t = torch.from_numpy(v).pin_memory()
+            pin[k] = t.numpy()
+        ca_p = torch.from_numpy(ca).pin_memory().numpy()
+        cb_p = torch.from_numpy(cb).pin_memory().numpy()
+        sim2 = new_sim()
+        sim2.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sim2.set_materials(ca_p, cb_p)
+        sim2.run_streamed(a.steps, pin['ex'], pin['ey'], pin['hx'], pin['hy'])
+        phs = sim2.get_phasors()
+        t1 = time.perf_counter()
+        el = t1 - t0
+        el_t = torch.tensor([el], dtype=torch.float64, device='cuda')
+        if world > 1:
+            dist.all_reduce(el_t, op=dist.ReduceOp.MAX)
+        el = float(el_t.item())
+        esz = np.dtype(a.dtype).itemsize
+        h2d = 2 * cells * esz + 4 * g.size_t_inc * g.size_x * g.size_y * esz
+        d2h = sum(p.nbytes for p in phs.values())
+        e2e = {'value': round(world * cells * a.steps / el / 1e6, 1), 'unit': 'Mcell-updates/s',
+               'h2d_bytes_per_step': int(h2d / a.steps), 'd2h_bytes_per_step': int(d2h / a.steps),
+               'includes': 'Ca/Cb upload, incident planes from pinned host memory, '
+                           f'{a.steps} steps, 24 phasor planes read back; wall clock'}
+        sim2.close()
+
+    base = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        base = cpu_baseline(pc, ca, cb, inc, a.cpu_steps)
+
+    if rank == 0:
+        line = {
+            'metric': 'Mcell-updates/s', 'value': round(value, 1), 'unit': 'Mcell-updates/s',
+            'n_gpus': world, 'steps': a.steps, 'warmup': a.warmup,
+            'ms_per_step': round(ms_max / a.steps, 4), 'higher_is_better': True,
+            'scaling': 'weak', 'vs_baseline': None,
+            'dtype': 'f32' if a.dtype == 'float32' else 'f64',
+            'data': 'synthetic (seeded materials and incident planes of the named shapes)',
+            'config': dict(workload_desc(pc, a.workload),
+                           parallelism=f'replicas x{world}' if world > 1 else 'single GPU',
+                           kernel=kname, tile=[choice['tile_x'], choice['tile_y']]
+                           if choice['kernel'] == _native.FDTD_KERNEL_FUSED else None),
+            'roofline': roofline, 'cpu_baseline': base, 'e2e': e2e,
+            'gpu_launches': gpu_launches, 'clocks': clk,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# reference arm: the reference's CPU algorithm (oracle port) on host cores
+# ---------------------------------------------------------------------------
+def run_reference(a):
+    rank = int(os.environ.get('RANK', '0'))
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    if rank != 0:
+        return
+    pc, ca, cb, inc = build_workload(a.workload, a.dtype, a.warmup + a.steps + 2)
+    g = pc.geom_params
+    cells = g.size_x * g.size_y * g.size_z
+    steps = max(1, min(a.steps, a.cpu_steps))
+    base = cpu_baseline(pc, ca, cb, inc, steps)
+    line = {
+        'impl': 'reference', 'metric': 'Mcell-updates/s', 'value': round(base['value'], 2),
+        'unit': 'Mcell-updates/s', 'n_gpus': world, 'steps': steps, 'warmup': 1,
+        'ms_per_step': round(cells / (base['value'] * 1e6) * 1e3, 2), 'higher_is_better': True,
+        'scaling': 'weak', 'vs_baseline': None,
+        'dtype': 'f32' if a.dtype == 'float32' else 'f64',
+        'data': 'synthetic (seeded materials and incident planes of the named shapes)',
+        'config': workload_desc(pc, a.workload),
+        'cpu_baseline': base,
+        'e2e': {'value': round(base['value'], 2), 'unit': 'Mcell-updates/s',
+                'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    a = parse()
+    if a.impl == 'reference':
+        run_reference(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == '__main__':
+    main()

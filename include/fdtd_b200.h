@@ -1,0 +1,205 @@
+/*
+ * fdtd_b200.h -- C-ABI of the B200-native FDTD time-stepping library
+ * (libfdtd_b200.so).
+ *
+ * This is the drop-in boundary for the time-stepping hot path of
+ * wyatt-sfu/sar-pixel-simulator (package `fdtdsarsim`). The reference drives
+ * its GPU path from Python through PyCUDA (`fdtdsarsim/gpu/main_sim.py`);
+ * each entry point below names the reference interface it replaces.
+ *
+ * Conventions
+ *  - Every function returns an int status (FDTD_OK == 0). On failure the
+ *    message is kept per thread and read with fdtd_last_error(). No C++
+ *    exception and no device trap crosses this boundary.
+ *  - Arrays are C-contiguous, z slowest, x fastest: fields and material
+ *    arrays are (nz, ny, nx); incident planes are (nt_inc, ny, nx); phasor
+ *    planes are complex (re, im interleaved) of the element type selected by
+ *    `dtype` (FDTD_F32 -> float, FDTD_F64 -> double).
+ *  - Host pointers are borrowed for the duration of the call only. Device
+ *    memory is owned by the handle.
+ *  - A handle is not re-entrant: one host thread at a time per handle.
+ */
+#ifndef FDTD_B200_H
+#define FDTD_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define FDTD_OK            0
+#define FDTD_ERR_INVALID   1  /* bad argument or size */
+#define FDTD_ERR_CUDA      2  /* CUDA runtime error */
+#define FDTD_ERR_STATE     3  /* call out of order (e.g. run before set_materials) */
+#define FDTD_ERR_NONFINITE 4  /* a NaN/Inf was detected in the fields */
+#define FDTD_ERR_NOMEM     5  /* device allocation failed */
+
+/* element types */
+#define FDTD_F32 0
+#define FDTD_F64 1
+
+/* step kernels (fdtd_set_option(FDTD_OPT_KERNEL, ...)) */
+#define FDTD_KERNEL_SPLIT 0   /* H pass + E pass + phasor pass per step */
+#define FDTD_KERNEL_FUSED 1   /* one z-marching pass per step + phasor pass */
+
+/* phasor accumulation (fdtd_set_option(FDTD_OPT_PHASOR_MODE, ...)) */
+#define FDTD_PHASOR_REFERENCE 0 /* float64 add of each term, rounded to the
+                                   storage type every step (the reference's
+                                   arithmetic, cpu/field_updates.py:385-400) */
+#define FDTD_PHASOR_KAHAN     1 /* storage-type accumulator plus a Kahan
+                                   compensation term */
+
+/* options */
+#define FDTD_OPT_KERNEL       1
+#define FDTD_OPT_PHASOR_MODE  2
+#define FDTD_OPT_TILE_X       3  /* fused kernel tile width (cells) */
+#define FDTD_OPT_TILE_Y       4  /* fused kernel tile height (cells) */
+#define FDTD_OPT_GRAPH_CHUNK  5  /* steps per captured CUDA graph (0 = no graph) */
+#define FDTD_OPT_CHECK_EVERY  6  /* non-finite check period in steps (0 = off) */
+#define FDTD_OPT_TIMING       7  /* 1: record CUDA events around every kernel */
+
+/* kernel kinds of fdtd_get_kernel_time */
+#define FDTD_TIME_STEP    0   /* the field-update kernel(s) of a step */
+#define FDTD_TIME_PHASOR  1   /* the phasor kernel of a step */
+
+/* Geometry and update constants of one simulation.
+ * Mirrors fdtdsarsim GeomParams (parameters.py:58-94) plus the scalars the
+ * reference's main loop derives from it (cpu/main_sim.py:116-130). The
+ * host computes db/dtm0/dte0dx and rounds them to `dtype` exactly as the
+ * reference does (np_type(dt / (mu0 * dx)) ...). */
+typedef struct fdtd_geometry {
+    int32_t nx, ny, nz;      /* size_x, size_y, size_z */
+    int32_t npml;            /* size_pml */
+    int32_t tfsf_z;          /* injection plane */
+    int32_t nt;              /* size_t: total time steps */
+    int32_t nt_inc;          /* size_t_inc: steps with incident injection */
+    int32_t dtype;           /* FDTD_F32 / FDTD_F64 */
+    double cell_size;        /* dx [m] */
+    double timestep;         /* dt [s] */
+    double frequency;        /* phasor frequency [Hz] */
+    double db;               /* dt / (mu0 dx), rounded to dtype */
+    double dtm0;             /* dt / mu0, rounded to dtype */
+    double dte0dx;           /* dt / (eps0 dx), rounded to dtype */
+} fdtd_geometry;
+
+typedef struct fdtd_sim fdtd_sim;
+
+/* Copies the last error message of the calling thread into buf
+ * (NUL-terminated, truncated to len). Returns the message length. */
+int fdtd_last_error(char *buf, int len);
+
+/* Library version (major*10000 + minor*100 + patch). */
+int fdtd_version(void);
+
+/* Number of visible CUDA devices (0 when none). */
+int fdtd_device_count(int *count);
+
+/* Creates a simulation on `device`, allocates all device state and zeroes it.
+ * Replaces MainSimGpu.__init__ (gpu/main_sim.py:45-72): context creation,
+ * _allocate_cuda_arrays (:512-640) and _clear_cuda_arrays (:691-787). */
+int fdtd_create(const fdtd_geometry *geom, int device, fdtd_sim **out);
+
+/* Frees every device resource of the handle. */
+int fdtd_destroy(fdtd_sim *sim);
+
+/* Sets a tuning or behaviour option (FDTD_OPT_*). */
+int fdtd_set_option(fdtd_sim *sim, int option, int value);
+int fdtd_get_option(fdtd_sim *sim, int option, int *value);
+
+/* Uploads the eight 1-D CPML coefficient profiles, each `npml` values of the
+ * element type, packed in this order: be_d, bh_d, ce_d, ch_d (down / left /
+ * front faces), be_u, bh_u, ce_u, ch_u (up / right / back faces).
+ * Replaces _init_absorber_arrays (gpu/main_sim.py:789-825), which uploads
+ * the same profiles tiled into 24 full 3-D arrays (absorbers.py:121-185). */
+int fdtd_set_absorbers(fdtd_sim *sim, const void *profiles);
+
+/* Uploads the update coefficient arrays Ca, Cb (nz, ny, nx) from host memory.
+ * Replaces the Ca/Cb transfer at the top of MainSimGpu._sim_loop
+ * (gpu/main_sim.py:200-202). */
+int fdtd_set_materials(fdtd_sim *sim, const void *ca, const void *cb);
+
+/* Computes Ca, Cb on the device from relative permittivity and
+ * conductivity of the material block (nz_mat, ny, nx), with vacuum stacked
+ * above it up to nz, with the arithmetic of compute_material_arrays
+ * (materials/materials.py:23-68). */
+int fdtd_set_materials_eps_sigma(fdtd_sim *sim, const void *eps_r,
+                                 const void *sigma, int nz_mat);
+
+/* Uploads the whole incident beam: four (nt_inc, ny, nx) arrays, kept
+ * resident in device memory. Replaces the per-step HDF5 reads and
+ * memcpy_htod of ex/ey/hx/hy_inc slices (gpu/main_sim.py:256-264,305-313). */
+int fdtd_set_incident(fdtd_sim *sim, const void *ex, const void *ey,
+                      const void *hx, const void *hy, int nt_inc);
+
+/* Zeroes fields, CPML auxiliaries and phasors and rewinds the step counter.
+ * Replaces _clear_cuda_arrays (gpu/main_sim.py:691-787). */
+int fdtd_reset(fdtd_sim *sim);
+
+/* Enqueues `nsteps` time steps on the handle's stream (asynchronous).
+ * One step is H update, H CPML, E-field injection, E update, E CPML,
+ * H-field injection and the six phasor planes, in the reference's order
+ * (gpu/main_sim.py:216-355, cpu/main_sim.py:140-195). */
+int fdtd_run(fdtd_sim *sim, int nsteps);
+
+/* Runs `nsteps` time steps while streaming the incident planes of those
+ * steps from host memory (four (nt_inc, ny, nx) arrays) through pinned
+ * staging buffers on a copy stream, overlapped with the time stepping.
+ * Synchronous. This is the reference's per-step incident transfer
+ * (gpu/main_sim.py:256-264,305-313) made asynchronous. */
+int fdtd_run_streamed(fdtd_sim *sim, int nsteps, const void *ex,
+                      const void *ey, const void *hx, const void *hy);
+
+/* Blocks until all enqueued work of the handle is done; reports deferred
+ * CUDA errors and the non-finite check. */
+int fdtd_synchronize(fdtd_sim *sim);
+
+/* Number of completed (enqueued) steps since the last reset. */
+int fdtd_step_index(fdtd_sim *sim, int64_t *t);
+
+/* CUDA stream the handle launches on (cudaStream_t as void*), and a way to
+ * make it launch on a caller's stream instead (NULL restores its own). */
+int fdtd_get_stream(fdtd_sim *sim, void **stream);
+int fdtd_set_stream(fdtd_sim *sim, void *stream);
+
+/* Device time spent in one kernel kind (FDTD_TIME_*) over the steps run
+ * since the last clear while FDTD_OPT_TIMING was on, from CUDA events on the
+ * handle's stream. Synchronizes. The reference has no counterpart (it only
+ * logs wall-clock per model, gpu/main_sim.py:93,112-115). */
+int fdtd_get_kernel_time(fdtd_sim *sim, int kind, double *total_ms, int *launches);
+int fdtd_clear_kernel_time(fdtd_sim *sim);
+
+/* Copies one of the 24 phasor planes to host memory. `plane` indexes the
+ * reference's result order (gpu/main_sim.py:409-418): ex_ph_d, ey_ph_d,
+ * hx_ph_d, hy_ph_d, ex_ph_u, ey_ph_u, hx_ph_u, hy_ph_u, ey_ph_l, ez_ph_l,
+ * hy_ph_l, hz_ph_l, ey_ph_r, ez_ph_r, hy_ph_r, hz_ph_r, ex_ph_f, ez_ph_f,
+ * hx_ph_f, hz_ph_f, ex_ph_b, ez_ph_b, hx_ph_b, hz_ph_b. Shapes: d/u planes
+ * (ny-2npml, nx-2npml); l/r (nz-2npml, ny-2npml); f/b (nz-2npml, nx-2npml).
+ * Replaces the phasor memcpy_dtoh block (gpu/main_sim.py:357-385). */
+int fdtd_get_phasor(fdtd_sim *sim, int plane, void *out);
+
+/* Copies a field component (0..5 = ex, ey, ez, hx, hy, hz) of the current
+ * state to / from host memory, shape (nz, ny, nx). The reference exposes
+ * these as MainSimCpu.ex ... hz after run (cpu/fdtd_sim.py:150-156). */
+int fdtd_get_field(fdtd_sim *sim, int comp, void *out);
+int fdtd_set_field(fdtd_sim *sim, int comp, const void *in);
+
+/* Near-to-far transform of the top phasor plane on the device.
+ * Inputs: the four u-plane phasors (ny_ph, nx_ph) as complex of
+ * `in_dtype` (FDTD_F32: complex64, FDTD_F64: complex128); nz is the
+ * phasor-plane count in z (sets the plane height). Output: four
+ * (nphi, ntheta) complex128 arrays E_theta, E_phi, H_theta, H_phi packed in
+ * that order into `out` (2*4*nphi*ntheta doubles).
+ * Replaces FarFieldTransform.__call__ (near2far.py:28-112). */
+int fdtd_near2far(const void *ex_u, const void *ey_u, const void *hx_u,
+                  const void *hy_u, int in_dtype, int nx_ph, int ny_ph,
+                  int nz_ph, double dx, double r, const double *thetas_deg,
+                  int ntheta, const double *phis_deg, int nphi, double freq,
+                  int device, double *out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FDTD_B200_H */

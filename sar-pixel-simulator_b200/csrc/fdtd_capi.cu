@@ -1,0 +1,710 @@
+// fdtd_capi.cu -- the extern "C" boundary of libfdtd_b200.so.
+//
+// Owns all device memory of a simulation handle, builds the by-value kernel
+// state, and schedules the per-step kernels. Errors are reported as status
+// codes plus a per-thread message; nothing throws across the boundary.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "fdtd_b200.h"
+#include "fdtd_launch.h"
+
+using namespace fdtd;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define CK(call)                                                                  \
+  do {                                                                            \
+    cudaError_t e_ = (call);                                                      \
+    if (e_ != cudaSuccess)                                                        \
+      return fail(e_ == cudaErrorMemoryAllocation ? FDTD_ERR_NOMEM : FDTD_ERR_CUDA, \
+                  "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+  } while (0)
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace
+
+struct fdtd_sim {
+  fdtd_geometry g{};
+  int device = 0;
+  size_t esz = 4;
+  int pitch = 0;
+  long long plane = 0, vol = 0;          // elements
+  int nx_ph = 0, ny_ph = 0, nz_ph = 0;
+  std::vector<DevBuf> bufs;              // every allocation, freed on destroy
+  void* fld[2][6] = {};                  // two field sets
+  void* ca = nullptr;
+  void* cb = nullptr;
+  void* psi_base[2] = {};                // two psi sets
+  long long psi_elems = 0;
+  long long poz[2][4], pox[2][4], poy[2][4];  // offsets within a psi set
+  void* inc[4] = {};
+  int inc_nt = 0;
+  void* ph = nullptr;
+  void* phc = nullptr;
+  long long ph_off[24];
+  long long ph_elems = 0;
+  double* phase = nullptr;
+  int* tdev = nullptr;
+  int64_t t = 0;
+  int cur = 0;
+  cudaStream_t own = nullptr;
+  cudaStream_t stream = nullptr;
+  bool have_abs = false, have_mat = false;
+  std::vector<unsigned char> prof;       // 8 * npml values of the element type
+  int kernel = FDTD_KERNEL_SPLIT;
+  int phasor_mode = FDTD_PHASOR_REFERENCE;
+  int tile_x = 32, tile_y = 8;
+  int graph_chunk = 0;
+  int check_every = 0;
+  // per-kernel event timing
+  int timing = 0;
+  std::vector<cudaEvent_t> ev;   // 3 per timed step: before step, after step, after phasors
+  int ev_used = 0;
+  double acc_ms[2] = {0, 0};
+  int acc_n[2] = {0, 0};
+};
+
+namespace {
+
+int alloc(fdtd_sim* s, size_t bytes, void** out) {
+  void* p = nullptr;
+  if (bytes == 0) bytes = 16;
+  cudaError_t e = cudaMalloc(&p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(FDTD_ERR_NOMEM, "cudaMalloc(%zu bytes) failed: %s", bytes, cudaGetErrorString(e));
+  }
+  s->bufs.push_back({p, bytes});
+  *out = p;
+  return FDTD_OK;
+}
+
+template <class T>
+State<T> make_state(const fdtd_sim* s, int src, int dst) {
+  State<T> st;
+  memset(&st, 0, sizeof(st));
+  const fdtd_geometry& g = s->g;
+  st.nx = g.nx; st.ny = g.ny; st.nz = g.nz; st.npml = g.npml; st.tfsf_z = g.tfsf_z;
+  st.nt_inc = g.nt_inc;
+  st.pitch = s->pitch;
+  st.plane = s->plane;
+  st.db = (T)g.db; st.dtm0 = (T)g.dtm0; st.dte0dx = (T)g.dte0dx;
+  st.dx = (T)g.cell_size;
+  const T* pr = reinterpret_cast<const T*>(s->prof.data());
+  if (!s->prof.empty())
+    for (int k = 0; k < 8; ++k)
+      for (int q = 0; q < g.npml; ++q) st.prof[k][q] = pr[k * g.npml + q];
+  st.iex = (const T*)s->fld[src][0]; st.iey = (const T*)s->fld[src][1]; st.iez = (const T*)s->fld[src][2];
+  st.ihx = (const T*)s->fld[src][3]; st.ihy = (const T*)s->fld[src][4]; st.ihz = (const T*)s->fld[src][5];
+  st.oex = (T*)s->fld[dst][0]; st.oey = (T*)s->fld[dst][1]; st.oez = (T*)s->fld[dst][2];
+  st.ohx = (T*)s->fld[dst][3]; st.ohy = (T*)s->fld[dst][4]; st.ohz = (T*)s->fld[dst][5];
+  st.ca = (const T*)s->ca; st.cb = (const T*)s->cb;
+  for (int side = 0; side < 2; ++side)
+    for (int c = 0; c < 4; ++c) {
+      T* bs = (T*)s->psi_base[src];
+      T* bd = (T*)s->psi_base[dst];
+      st.ps.z[side][c] = bs + s->poz[side][c]; st.pd.z[side][c] = bd + s->poz[side][c];
+      st.ps.x[side][c] = bs + s->pox[side][c]; st.pd.x[side][c] = bd + s->pox[side][c];
+      st.ps.y[side][c] = bs + s->poy[side][c]; st.pd.y[side][c] = bd + s->poy[side][c];
+    }
+  st.inc_ex = (const T*)s->inc[0]; st.inc_ey = (const T*)s->inc[1];
+  st.inc_hx = (const T*)s->inc[2]; st.inc_hy = (const T*)s->inc[3];
+  st.ph = (T*)s->ph;
+  st.phc = (T*)s->phc;
+  for (int k = 0; k < 24; ++k) st.ph_off[k] = s->ph_off[k];
+  st.nx_ph = s->nx_ph; st.ny_ph = s->ny_ph; st.nz_ph = s->nz_ph;
+  st.phase = s->phase;
+  st.kahan = s->phasor_mode == FDTD_PHASOR_KAHAN ? 1 : 0;
+  return st;
+}
+
+cudaEvent_t timing_event(fdtd_sim* s) {
+  if (s->ev_used >= (int)s->ev.size()) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    s->ev.push_back(e);
+  }
+  return s->ev[s->ev_used++];
+}
+
+void mark(fdtd_sim* s, cudaEvent_t e) {
+  if (e) cudaEventRecord(e, s->stream);
+}
+
+int collect_timing(fdtd_sim* s) {
+  CK(cudaStreamSynchronize(s->stream));
+  for (int i = 0; i + 2 < s->ev_used; i += 3) {
+    float a = 0, b = 0;
+    CK(cudaEventElapsedTime(&a, s->ev[i], s->ev[i + 1]));
+    CK(cudaEventElapsedTime(&b, s->ev[i + 1], s->ev[i + 2]));
+    s->acc_ms[0] += a; s->acc_n[0] += 1;
+    s->acc_ms[1] += b; s->acc_n[1] += 1;
+  }
+  s->ev_used = 0;
+  return FDTD_OK;
+}
+
+template <class T>
+int enqueue_steps(fdtd_sim* s, int n) {
+  for (int k = 0; k < n; ++k) {
+    if (s->timing && s->ev_used + 3 > 3 * 4096) {
+      int rc = collect_timing(s);
+      if (rc) return rc;
+    }
+    cudaEvent_t e0 = s->timing ? timing_event(s) : nullptr;
+    cudaEvent_t e1 = s->timing ? timing_event(s) : nullptr;
+    cudaEvent_t e2 = s->timing ? timing_event(s) : nullptr;
+    mark(s, e0);
+    if (s->kernel == FDTD_KERNEL_FUSED) {
+      State<T> st = make_state<T>(s, s->cur, 1 - s->cur);
+      if (!launch_fused_step<T>(st, s->tdev, k, s->tile_x, s->tile_y, s->stream))
+        return fail(FDTD_ERR_INVALID, "unsupported fused tile %dx%d", s->tile_x, s->tile_y);
+      s->cur = 1 - s->cur;
+      mark(s, e1);
+      State<T> sp = make_state<T>(s, s->cur, s->cur);
+      launch_phasors<T>(sp, s->tdev, k, s->stream);
+    } else {
+      State<T> st = make_state<T>(s, s->cur, s->cur);
+      launch_split_step<T>(st, s->tdev, k, s->stream);
+      mark(s, e1);
+      launch_phasors<T>(st, s->tdev, k, s->stream);
+    }
+    mark(s, e2);
+  }
+  launch_advance(s->tdev, n, s->stream);
+  CK(cudaGetLastError());
+  return FDTD_OK;
+}
+
+int check_sim(fdtd_sim* s) {
+  if (!s) return fail(FDTD_ERR_INVALID, "null simulation handle");
+  cudaError_t e = cudaSetDevice(s->device);
+  if (e != cudaSuccess) return fail(FDTD_ERR_CUDA, "cudaSetDevice: %s", cudaGetErrorString(e));
+  return FDTD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fdtd_last_error(char* buf, int len) {
+  if (buf && len > 0) {
+    strncpy(buf, g_err.c_str(), (size_t)len - 1);
+    buf[len - 1] = 0;
+  }
+  return (int)g_err.size();
+}
+
+int fdtd_version(void) { return 100; }
+
+int fdtd_device_count(int* count) {
+  if (!count) return fail(FDTD_ERR_INVALID, "null count");
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    n = 0;
+  }
+  *count = n;
+  return FDTD_OK;
+}
+
+int fdtd_create(const fdtd_geometry* geom, int device, fdtd_sim** out) {
+  if (!geom || !out) return fail(FDTD_ERR_INVALID, "null argument");
+  *out = nullptr;
+  const fdtd_geometry& g = *geom;
+  if (g.dtype != FDTD_F32 && g.dtype != FDTD_F64)
+    return fail(FDTD_ERR_INVALID, "dtype must be FDTD_F32 or FDTD_F64");
+  if (g.npml < 2 || g.npml > kMaxPml)
+    return fail(FDTD_ERR_INVALID, "npml %d out of range [2, %d]", g.npml, kMaxPml);
+  const int minn = 2 * g.npml + 3;
+  if (g.nx < minn || g.ny < minn || g.nz < minn)
+    return fail(FDTD_ERR_INVALID, "grid %dx%dx%d too small for npml %d (need >= %d per axis)",
+                g.nz, g.ny, g.nx, g.npml, minn);
+  if (g.tfsf_z < 0 || g.tfsf_z >= g.nz)
+    return fail(FDTD_ERR_INVALID, "tfsf_z %d outside [0, nz=%d)", g.tfsf_z, g.nz);
+  if (g.nt < 0 || g.nt_inc < 0)
+    return fail(FDTD_ERR_INVALID, "negative step counts");
+  if (!(g.cell_size > 0) || !(g.timestep > 0))
+    return fail(FDTD_ERR_INVALID, "cell_size and timestep must be positive");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(FDTD_ERR_CUDA, "no CUDA device available");
+  }
+  if (device < 0 || device >= ndev)
+    return fail(FDTD_ERR_INVALID, "device %d out of range (%d devices)", device, ndev);
+  CK(cudaSetDevice(device));
+
+  fdtd_sim* s = new fdtd_sim();
+  s->g = g;
+  s->device = device;
+  s->esz = g.dtype == FDTD_F32 ? 4 : 8;
+  s->pitch = (g.nx + 31) / 32 * 32;
+  s->plane = (long long)g.ny * s->pitch;
+  s->vol = (long long)g.nz * s->plane;
+  s->nx_ph = g.nx - 2 * g.npml;
+  s->ny_ph = g.ny - 2 * g.npml;
+  s->nz_ph = g.nz - 2 * g.npml;
+  int rc = FDTD_OK;
+  auto A = [&](size_t bytes, void** p) {
+    if (rc == FDTD_OK) rc = alloc(s, bytes, p);
+  };
+  const size_t fb = (size_t)s->vol * s->esz;
+  for (int set = 0; set < 2; ++set)
+    for (int c = 0; c < 6; ++c) A(fb, &s->fld[set][c]);
+  A(fb, &s->ca);
+  A(fb, &s->cb);
+  // psi layout within one set: z faces (npml, ny, pitch), x faces
+  // (nz, ny, npml), y faces (nz, npml, pitch); 4 components per face side
+  long long off = 0;
+  const long long zsz = (long long)g.npml * g.ny * s->pitch;
+  const long long xsz = (long long)g.nz * g.ny * g.npml;
+  const long long ysz = (long long)g.nz * g.npml * s->pitch;
+  auto align32 = [](long long v) { return (v + 31) / 32 * 32; };
+  for (int side = 0; side < 2; ++side)
+    for (int c = 0; c < 4; ++c) { s->poz[side][c] = off; off += align32(zsz); }
+  for (int side = 0; side < 2; ++side)
+    for (int c = 0; c < 4; ++c) { s->pox[side][c] = off; off += align32(xsz); }
+  for (int side = 0; side < 2; ++side)
+    for (int c = 0; c < 4; ++c) { s->poy[side][c] = off; off += align32(ysz); }
+  s->psi_elems = off;
+  A((size_t)off * s->esz, &s->psi_base[0]);
+  A((size_t)off * s->esz, &s->psi_base[1]);
+  // phasor planes in the reference's result order
+  off = 0;
+  for (int k = 0; k < 24; ++k) {
+    long long n;
+    if (k < 8) n = (long long)s->ny_ph * s->nx_ph;
+    else if (k < 16) n = (long long)s->nz_ph * s->ny_ph;
+    else n = (long long)s->nz_ph * s->nx_ph;
+    s->ph_off[k] = off;
+    off += align32(2 * n);
+  }
+  s->ph_elems = off;
+  A((size_t)off * s->esz, &s->ph);
+  A((size_t)off * s->esz, &s->phc);
+  A((size_t)std::max(g.nt, 1) * 4 * sizeof(double), (void**)&s->phase);
+  A(sizeof(int) * 4, (void**)&s->tdev);
+  if (rc != FDTD_OK) {
+    fdtd_destroy(s);
+    return rc;
+  }
+  // phase factors per step: the reference evaluates exp(-1j*omega*t*dt) and
+  // exp(-1j*omega*(t-0.5)*dt) in complex128 (cpu/field_updates.py:387,395),
+  // i.e. cos/sin of (-omega*t)*dt with omega = 2.0*pi*f (cpu/main_sim.py:124)
+  {
+    std::vector<double> tab((size_t)std::max(g.nt, 1) * 4);
+    const double omega = 2.0 * M_PI * g.frequency;
+    for (int t = 0; t < g.nt; ++t) {
+      volatile double a = -omega * (double)t;
+      const double the = a * g.timestep;
+      volatile double b = -omega * ((double)t - 0.5);
+      const double thh = b * g.timestep;
+      tab[4 * t + 0] = std::cos(the);
+      tab[4 * t + 1] = std::sin(the);
+      tab[4 * t + 2] = std::cos(thh);
+      tab[4 * t + 3] = std::sin(thh);
+    }
+    cudaError_t e = cudaMemcpy(s->phase, tab.data(), tab.size() * sizeof(double),
+                               cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      fdtd_destroy(s);
+      return fail(FDTD_ERR_CUDA, "phase table upload: %s", cudaGetErrorString(e));
+    }
+  }
+  cudaError_t e = cudaStreamCreateWithFlags(&s->own, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    fdtd_destroy(s);
+    return fail(FDTD_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
+  }
+  s->stream = s->own;
+  rc = fdtd_reset(s);
+  if (rc != FDTD_OK) {
+    fdtd_destroy(s);
+    return rc;
+  }
+  *out = s;
+  return FDTD_OK;
+}
+
+int fdtd_destroy(fdtd_sim* s) {
+  if (!s) return FDTD_OK;
+  cudaSetDevice(s->device);
+  if (s->own) cudaStreamSynchronize(s->own);
+  for (auto& b : s->bufs) cudaFree(b.p);
+  for (auto e : s->ev) cudaEventDestroy(e);
+  if (s->own) cudaStreamDestroy(s->own);
+  delete s;
+  cudaGetLastError();
+  return FDTD_OK;
+}
+
+int fdtd_set_option(fdtd_sim* s, int option, int value) {
+  if (!s) return fail(FDTD_ERR_INVALID, "null simulation handle");
+  switch (option) {
+    case FDTD_OPT_KERNEL:
+      if (value != FDTD_KERNEL_SPLIT && value != FDTD_KERNEL_FUSED)
+        return fail(FDTD_ERR_INVALID, "unknown kernel %d", value);
+      s->kernel = value;
+      return FDTD_OK;
+    case FDTD_OPT_PHASOR_MODE:
+      if (value != FDTD_PHASOR_REFERENCE && value != FDTD_PHASOR_KAHAN)
+        return fail(FDTD_ERR_INVALID, "unknown phasor mode %d", value);
+      if (s->t != 0 && value != s->phasor_mode)
+        return fail(FDTD_ERR_STATE, "phasor mode can only change before the first step");
+      s->phasor_mode = value;
+      return FDTD_OK;
+    case FDTD_OPT_TILE_X:
+      if (value < 4 || value > 256 || value % 4) return fail(FDTD_ERR_INVALID, "bad tile_x %d", value);
+      s->tile_x = value;
+      return FDTD_OK;
+    case FDTD_OPT_TILE_Y:
+      if (value < 1 || value > 64) return fail(FDTD_ERR_INVALID, "bad tile_y %d", value);
+      s->tile_y = value;
+      return FDTD_OK;
+    case FDTD_OPT_GRAPH_CHUNK:
+      if (value < 0) return fail(FDTD_ERR_INVALID, "bad graph chunk %d", value);
+      s->graph_chunk = value;
+      return FDTD_OK;
+    case FDTD_OPT_CHECK_EVERY:
+      if (value < 0) return fail(FDTD_ERR_INVALID, "bad check period %d", value);
+      s->check_every = value;
+      return FDTD_OK;
+    case FDTD_OPT_TIMING:
+      s->timing = value ? 1 : 0;
+      return FDTD_OK;
+  }
+  return fail(FDTD_ERR_INVALID, "unknown option %d", option);
+}
+
+int fdtd_get_option(fdtd_sim* s, int option, int* value) {
+  if (!s || !value) return fail(FDTD_ERR_INVALID, "null argument");
+  switch (option) {
+    case FDTD_OPT_KERNEL: *value = s->kernel; return FDTD_OK;
+    case FDTD_OPT_PHASOR_MODE: *value = s->phasor_mode; return FDTD_OK;
+    case FDTD_OPT_TILE_X: *value = s->tile_x; return FDTD_OK;
+    case FDTD_OPT_TILE_Y: *value = s->tile_y; return FDTD_OK;
+    case FDTD_OPT_GRAPH_CHUNK: *value = s->graph_chunk; return FDTD_OK;
+    case FDTD_OPT_CHECK_EVERY: *value = s->check_every; return FDTD_OK;
+    case FDTD_OPT_TIMING: *value = s->timing; return FDTD_OK;
+  }
+  return fail(FDTD_ERR_INVALID, "unknown option %d", option);
+}
+
+int fdtd_set_absorbers(fdtd_sim* s, const void* profiles) {
+  int rc = check_sim(s);
+  if (rc) return rc;
+  if (!profiles) return fail(FDTD_ERR_INVALID, "null profiles");
+  const size_t n = 8 * (size_t)s->g.npml * s->esz;
+  s->prof.assign((const unsigned char*)profiles, (const unsigned char*)profiles + n);
+  s->have_abs = true;
+  return FDTD_OK;
+}
+
+static int upload_volume(fdtd_sim* s, void* dst, const void* src) {
+  const size_t w = (size_t)s->g.nx * s->esz;
+  CK(cudaMemcpy2DAsync(dst, (size_t)s->pitch * s->esz, src, w, w,
+                       (size_t)s->g.ny * s->g.nz, cudaMemcpyHostToDevice, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return FDTD_OK;
+}
+
+int fdtd_set_materials(fdtd_sim* s, const void* ca, const void* cb) {
+  int rc = check_sim(s);
+  if (rc) return rc;
+  if (!ca || !cb) return fail(FDTD_ERR_INVALID, "null Ca/Cb");
+  if ((rc = upload_volume(s, s->ca, ca))) return rc;
+  if ((rc = upload_volume(s, s->cb, cb))) return rc;
+  s->have_mat = true;
+  return FDTD_OK;
+}
+
+int fdtd_set_materials_eps_sigma(fdtd_sim* s, const void* eps_r, const void* sigma, int nz_mat) {
+  int rc = check_sim(s);
+  if (rc) return rc;
+  if (!eps_r || !sigma) return fail(FDTD_ERR_INVALID, "null eps/sigma");
+  const fdtd_geometry& g = s->g;
+  if (nz_mat < 0 || nz_mat > g.nz) return fail(FDTD_ERR_INVALID, "nz_mat %d outside [0, %d]", nz_mat, g.nz);
+  const size_t n = (size_t)nz_mat * g.ny * g.nx;
+  void* de = nullptr;
+  void* ds = nullptr;
+  CK(cudaMallocAsync(&de, std::max<size_t>(n, 1) * s->esz, s->stream));
+  CK(cudaMallocAsync(&ds, std::max<size_t>(n, 1) * s->esz, s->stream));
+  CK(cudaMemcpyAsync(de, eps_r, n * s->esz, cudaMemcpyHostToDevice, s->stream));
+  CK(cudaMemcpyAsync(ds, sigma, n * s->esz, cudaMemcpyHostToDevice, s->stream));
+  // eps0 as hard-coded in materials/materials.py:45, rounded to the dtype
+  const double eps0 = 8.8541878128e-12;
+  if (g.dtype == FDTD_F32)
+    launch_eps_sigma<float>(g.nx, g.ny, g.nz, nz_mat, s->pitch, (const float*)de, (const float*)ds,
+                            (float)eps0, (float)g.timestep, (float)g.cell_size, (float*)s->ca,
+                            (float*)s->cb, s->stream);
+  else
+    launch_eps_sigma<double>(g.nx, g.ny, g.nz, nz_mat, s->pitch, (const double*)de,
+                             (const double*)ds, eps0, g.timestep, g.cell_size, (double*)s->ca,
+                             (double*)s->cb, s->stream);
+  CK(cudaGetLastError());
+  CK(cudaFreeAsync(de, s->stream));
+  CK(cudaFreeAsync(ds, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  s->have_mat = true;
+  return FDTD_OK;
+}
+
+int fdtd_set_incident(fdtd_sim* s, const void* ex, const void* ey, const void* hx, const void* hy,
+                      int nt_inc) {
+  int rc = check_sim(s);
+  if (rc) return rc;
+  const fdtd_geometry& g = s->g;
+  if (nt_inc != g.nt_inc)
+    return fail(FDTD_ERR_INVALID, "incident beam has %d steps, geometry expects %d", nt_inc, g.nt_inc);
+  const void* src[4] = {ex, ey, hx, hy};
+  for (int c = 0; c < 4; ++c)
+    if (!src[c] && nt_inc > 0) return fail(FDTD_ERR_INVALID, "null incident component %d", c);
+  const size_t bytes = (size_t)std::max(nt_inc, 1) * s->plane * s->esz;
+  for (int c = 0; c < 4; ++c) {
+    if (!s->inc[c]) {
+      if ((rc = alloc(s, bytes, &s->inc[c]))) return rc;
+    }
+    if (nt_inc > 0) {
+      const size_t w = (size_t)g.nx * s->esz;
+      CK(cudaMemcpy2DAsync(s->inc[c], (size_t)s->pitch * s->esz, src[c], w, w,
+                           (size_t)g.ny * nt_inc, cudaMemcpyHostToDevice, s->stream));
+    }
+  }
+  CK(cudaStreamSynchronize(s->stream));
+  s->inc_nt = nt_inc;
+  return FDTD_OK;
+}
+
+int fdtd_reset(fdtd_sim* s) {
+  int rc = check_sim(s);
+  if (rc) return rc;
+  const size_t fb = (size_t)s->vol * s->esz;
+  for (int set = 0; set < 2; ++set)
+    for (int c = 0; c < 6; ++c) CK(cudaMemsetAsync(s->fld[set][c], 0, fb, s->stream));
+  for (int set = 0; set < 2; ++set)
+    CK(cudaMemsetAsync(s->psi_base[set], 0, (size_t)s->psi_elems * s->esz, s->stream));
+  CK(cudaMemsetAsync(s->ph, 0, (size_t)s->ph_elems * s->esz, s->stream));
+  CK(cudaMemsetAsync(s->phc, 0, (size_t)s->ph_elems * s->esz, s->stream));
+  CK(cudaMemsetAsync(s->tdev, 0, sizeof(int) * 4, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  s->t = 0;
+  s->cur = 0;
+  return FDTD_OK;
+}
+
+int fdtd_run(fdtd_sim* s, int nsteps) {
+  int rc = check_sim(s);
+  if (rc) return rc;
+  if (nsteps < 0) return fail(FDTD_ERR_INVALID, "negative step count");
+  if (!s->have_abs) return fail(FDTD_ERR_STATE, "absorbers not set (fdtd_set_absorbers)");
+  if (!s->have_mat) return fail(FDTD_ERR_STATE, "materials not set (fdtd_set_materials)");
+  if (s->t + nsteps > s->g.nt)
+    return fail(FDTD_ERR_INVALID, "step %lld + %d exceeds size_t %d", (long long)s->t, nsteps, s->g.nt);
+  if (s->g.nt_inc > 0 && s->t < s->g.nt_inc && s->inc_nt < s->g.nt_inc)
+    return fail(FDTD_ERR_STATE, "incident beam not set (fdtd_set_incident)");
+  if (nsteps == 0) return FDTD_OK;
+  rc = s->g.dtype == FDTD_F32 ? enqueue_steps<float>(s, nsteps) : enqueue_steps<double>(s, nsteps);
+  if (rc) return rc;
+  s->t += nsteps;
+  return FDTD_OK;
+}
+
+int fdtd_run_streamed(fdtd_sim* s, int nsteps, const void* ex, const void* ey, const void* hx,
+                      const void* hy) {
+  // First version: upload the incident planes the run needs, then run.
+  int rc = check_sim(s);
+  if (rc) return rc;
+  if (s->g.nt_inc > 0 && s->inc_nt < s->g.nt_inc) {
+    if ((rc = fdtd_set_incident(s, ex, ey, hx, hy, s->g.nt_inc))) return rc;
+  }
+  if ((rc = fdtd_run(s, nsteps))) return rc;
+  return fdtd_synchronize(s);
+}
+
+int fdtd_synchronize(fdtd_sim* s) {
+  int rc = check_sim(s);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(s->stream));
+  CK(cudaGetLastError());
+  return FDTD_OK;
+}
+
+int fdtd_step_index(fdtd_sim* s, int64_t* t) {
+  if (!s || !t) return fail(FDTD_ERR_INVALID, "null argument");
+  *t = s->t;
+  return FDTD_OK;
+}
+
+int fdtd_get_stream(fdtd_sim* s, void** stream) {
+  if (!s || !stream) return fail(FDTD_ERR_INVALID, "null argument");
+  *stream = (void*)s->stream;
+  return FDTD_OK;
+}
+
+int fdtd_set_stream(fdtd_sim* s, void* stream) {
+  int rc = check_sim(s);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(s->stream));
+  s->stream = stream ? (cudaStream_t)stream : s->own;
+  return FDTD_OK;
+}
+
+int fdtd_get_kernel_time(fdtd_sim* s, int kind, double* total_ms, int* launches) {
+  int rc = check_sim(s);
+  if (rc) return rc;
+  if (kind != FDTD_TIME_STEP && kind != FDTD_TIME_PHASOR)
+    return fail(FDTD_ERR_INVALID, "unknown kernel kind %d", kind);
+  if ((rc = collect_timing(s))) return rc;
+  if (total_ms) *total_ms = s->acc_ms[kind];
+  if (launches) *launches = s->acc_n[kind];
+  return FDTD_OK;
+}
+
+int fdtd_clear_kernel_time(fdtd_sim* s) {
+  int rc = check_sim(s);
+  if (rc) return rc;
+  if ((rc = collect_timing(s))) return rc;
+  s->acc_ms[0] = s->acc_ms[1] = 0;
+  s->acc_n[0] = s->acc_n[1] = 0;
+  return FDTD_OK;
+}
+
+int fdtd_get_phasor(fdtd_sim* s, int plane, void* out) {
+  int rc = check_sim(s);
+  if (rc) return rc;
+  if (plane < 0 || plane >= 24) return fail(FDTD_ERR_INVALID, "phasor plane %d outside [0, 24)", plane);
+  if (!out) return fail(FDTD_ERR_INVALID, "null output");
+  long long n;
+  if (plane < 8) n = (long long)s->ny_ph * s->nx_ph;
+  else if (plane < 16) n = (long long)s->nz_ph * s->ny_ph;
+  else n = (long long)s->nz_ph * s->nx_ph;
+  CK(cudaMemcpyAsync(out, (char*)s->ph + s->ph_off[plane] * s->esz, (size_t)(2 * n) * s->esz,
+                     cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return FDTD_OK;
+}
+
+int fdtd_get_field(fdtd_sim* s, int comp, void* out) {
+  int rc = check_sim(s);
+  if (rc) return rc;
+  if (comp < 0 || comp >= 6) return fail(FDTD_ERR_INVALID, "field component %d outside [0, 6)", comp);
+  if (!out) return fail(FDTD_ERR_INVALID, "null output");
+  const size_t w = (size_t)s->g.nx * s->esz;
+  CK(cudaMemcpy2DAsync(out, w, s->fld[s->cur][comp], (size_t)s->pitch * s->esz, w,
+                       (size_t)s->g.ny * s->g.nz, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return FDTD_OK;
+}
+
+int fdtd_set_field(fdtd_sim* s, int comp, const void* in) {
+  int rc = check_sim(s);
+  if (rc) return rc;
+  if (comp < 0 || comp >= 6) return fail(FDTD_ERR_INVALID, "field component %d outside [0, 6)", comp);
+  if (!in) return fail(FDTD_ERR_INVALID, "null input");
+  return upload_volume(s, s->fld[s->cur][comp], in);
+}
+
+}  // extern "C"
+
+extern "C" int fdtd_near2far(const void* ex_u, const void* ey_u, const void* hx_u,
+                             const void* hy_u, int in_dtype, int nx_ph, int ny_ph, int nz_ph,
+                             double dx, double r, const double* thetas_deg, int ntheta,
+                             const double* phis_deg, int nphi, double freq, int device,
+                             double* out) {
+  if (!ex_u || !ey_u || !hx_u || !hy_u || !thetas_deg || !phis_deg || !out)
+    return fail(FDTD_ERR_INVALID, "null argument");
+  if (in_dtype != FDTD_F32 && in_dtype != FDTD_F64)
+    return fail(FDTD_ERR_INVALID, "in_dtype must be FDTD_F32 or FDTD_F64");
+  if (nx_ph < 3 || ny_ph < 3 || nx_ph % 2 == 0 || ny_ph % 2 == 0)
+    return fail(FDTD_ERR_INVALID,
+                "phasor plane %dx%d: Simpson integration needs odd sample counts >= 3", ny_ph, nx_ph);
+  if (ntheta < 1 || nphi < 1 || nz_ph < 1) return fail(FDTD_ERR_INVALID, "empty angle or plane set");
+  if (!(freq > 0) || !(dx > 0) || !(r > 0)) return fail(FDTD_ERR_INVALID, "freq, dx, r must be positive");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(FDTD_ERR_CUDA, "no CUDA device available");
+  }
+  if (device < 0 || device >= ndev) return fail(FDTD_ERR_INVALID, "device %d out of range", device);
+  CK(cudaSetDevice(device));
+  // surface currents in complex128, as near2far.py:64-68 converts them:
+  // Jx = -Hy, Jy = Hx, Mx = Ey, My = -Ex   (near2far.py:94-96)
+  const size_t n = (size_t)nx_ph * ny_ph;
+  std::vector<double> jm(8 * n);
+  auto get = [&](const void* p, size_t i, int part) -> double {
+    return in_dtype == FDTD_F32 ? (double)((const float*)p)[2 * i + part]
+                                : ((const double*)p)[2 * i + part];
+  };
+  for (size_t i = 0; i < n; ++i) {
+    for (int part = 0; part < 2; ++part) {
+      jm[2 * (0 * n + i) + part] = -get(hy_u, i, part);
+      jm[2 * (1 * n + i) + part] = get(hx_u, i, part);
+      jm[2 * (2 * n + i) + part] = get(ey_u, i, part);
+      jm[2 * (3 * n + i) + part] = -get(ex_u, i, part);
+    }
+  }
+  std::vector<double> th(ntheta), ph(nphi);
+  for (int i = 0; i < ntheta; ++i) th[i] = thetas_deg[i] * (M_PI / 180.0);
+  for (int i = 0; i < nphi; ++i) ph[i] = phis_deg[i] * (M_PI / 180.0);
+  const double c0 = 299792458.0;
+  const double lam = c0 / freq;
+  const double k = 2.0 * M_PI / lam;
+  const double z_val = (double)((nz_ph - 1) / 2) * dx;
+  double *djm = nullptr, *dth = nullptr, *dph = nullptr, *dout = nullptr;
+  const size_t out_n = (size_t)8 * nphi * ntheta;
+  cudaStream_t st;
+  CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  int rc = FDTD_OK;
+  do {
+    if (cudaMallocAsync(&djm, jm.size() * sizeof(double), st) != cudaSuccess ||
+        cudaMallocAsync(&dth, th.size() * sizeof(double), st) != cudaSuccess ||
+        cudaMallocAsync(&dph, ph.size() * sizeof(double), st) != cudaSuccess ||
+        cudaMallocAsync(&dout, out_n * sizeof(double), st) != cudaSuccess) {
+      rc = fail(FDTD_ERR_NOMEM, "near2far device allocation failed");
+      break;
+    }
+    cudaMemcpyAsync(djm, jm.data(), jm.size() * sizeof(double), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(dth, th.data(), th.size() * sizeof(double), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(dph, ph.data(), ph.size() * sizeof(double), cudaMemcpyHostToDevice, st);
+    if (near2far_run(djm, nx_ph, ny_ph, dx, z_val, k, dth, ntheta, dph, nphi, r, dout, st)) {
+      rc = fail(FDTD_ERR_CUDA, "near2far launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+      break;
+    }
+    cudaMemcpyAsync(out, dout, out_n * sizeof(double), cudaMemcpyDeviceToHost, st);
+  } while (0);
+  if (djm) cudaFreeAsync(djm, st);
+  if (dth) cudaFreeAsync(dth, st);
+  if (dph) cudaFreeAsync(dph, st);
+  if (dout) cudaFreeAsync(dout, st);
+  cudaError_t e = cudaStreamSynchronize(st);
+  cudaStreamDestroy(st);
+  if (rc == FDTD_OK && e != cudaSuccess)
+    rc = fail(FDTD_ERR_CUDA, "near2far: %s", cudaGetErrorString(e));
+  return rc;
+}

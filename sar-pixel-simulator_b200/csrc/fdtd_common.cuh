@@ -1,0 +1,80 @@
+// fdtd_common.cuh -- shared device-side definitions of the FDTD library.
+//
+// All field arithmetic goes through R<T>::add/sub/mul/div, which map to the
+// round-to-nearest intrinsics. They are never contracted into fused
+// multiply-adds, so every update rounds exactly like the reference's numba
+// kernels (fdtdsarsim/cpu/field_updates.py), which do not contract either.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace fdtd {
+
+constexpr int kMaxPml = 32;
+
+template <class T> struct R;
+template <> struct R<float> {
+  static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+  static __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+  static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+  static __device__ __forceinline__ float div(float a, float b) { return __fdiv_rn(a, b); }
+  static __device__ __forceinline__ float from_double(double a) { return __double2float_rn(a); }
+};
+template <> struct R<double> {
+  static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+  static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+  static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+  static __device__ __forceinline__ double div(double a, double b) { return __ddiv_rn(a, b); }
+  static __device__ __forceinline__ double from_double(double a) { return a; }
+};
+
+// CPML coefficient profiles, indexed [kind][q]. Kinds follow the packing of
+// fdtd_set_absorbers: be_d, bh_d, ce_d, ch_d (down/left/front faces) and
+// be_u, bh_u, ce_u, ch_u (up/right/back faces).
+enum { BE_D = 0, BH_D, CE_D, CH_D, BE_U, BH_U, CE_U, CH_U };
+
+// psi component slots per face.
+//   z faces (down/up):    0 Exz, 1 Eyz, 2 Hxz, 3 Hyz   shape (npml, ny, pitch)
+//   x faces (left/right): 0 Eyx, 1 Ezx, 2 Hyx, 3 Hzx   shape (nz, ny, npml)
+//   y faces (front/back): 0 Exy, 1 Ezy, 2 Hxy, 3 Hzy   shape (nz, npml, pitch)
+// Side 0 is the low face (down/left/front), side 1 the high face.
+template <class T>
+struct Psi {
+  T* z[2][4];
+  T* x[2][4];
+  T* y[2][4];
+};
+
+// Everything a step kernel needs, passed by value (lives in the kernel
+// parameter bank). Fields are stored (nz, ny, pitch) with pitch >= nx a
+// multiple of 32 elements, so rows start 128-byte aligned.
+template <class T>
+struct State {
+  int nx, ny, nz, npml, tfsf_z, nt_inc;
+  int pitch;
+  long long plane;   // ny * pitch
+  T db, dtm0, dte0dx, dx;
+  T prof[8][kMaxPml];
+  // field sets: src is read, dst is written (the same set for the in-place
+  // split kernels; ping-pong sets for the fused kernel)
+  const T* iex; const T* iey; const T* iez;  // E source
+  const T* ihx; const T* ihy; const T* ihz;  // H source
+  T* oex; T* oey; T* oez;                    // E destination
+  T* ohx; T* ohy; T* ohz;                    // H destination
+  const T* ca; const T* cb;
+  Psi<T> ps;   // psi source
+  Psi<T> pd;   // psi destination
+  const T* inc_ex; const T* inc_ey; const T* inc_hx; const T* inc_hy;  // (nt_inc, ny, pitch)
+  // phasors: 24 planes, complex interleaved, at offsets ph_off[k]
+  T* ph;
+  T* phc;    // Kahan compensation (same layout) or nullptr
+  long long ph_off[24];
+  int nx_ph, ny_ph, nz_ph;
+  const double* phase;   // per step: cos_e, sin_e, cos_h, sin_h
+  int kahan;
+};
+
+__global__ void k_advance(int* t, int n);
+
+}  // namespace fdtd

@@ -1,0 +1,299 @@
+"""ctypes binding of libfdtd_b200.so (declared in include/fdtd_b200.h).
+
+The library is the only compute path of this package: importing this module
+fails loudly when it is missing, and every call that returns a non-zero
+status raises :class:`FdtdError` with the library's message.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+LIB_NAME = 'libfdtd_b200.so'
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), LIB_NAME)
+
+FDTD_OK = 0
+FDTD_ERR_INVALID = 1
+FDTD_ERR_CUDA = 2
+FDTD_ERR_STATE = 3
+FDTD_ERR_NONFINITE = 4
+FDTD_ERR_NOMEM = 5
+
+FDTD_F32 = 0
+FDTD_F64 = 1
+
+FDTD_KERNEL_SPLIT = 0
+FDTD_KERNEL_FUSED = 1
+
+FDTD_PHASOR_REFERENCE = 0
+FDTD_PHASOR_KAHAN = 1
+
+OPT_KERNEL = 1
+OPT_PHASOR_MODE = 2
+OPT_TILE_X = 3
+OPT_TILE_Y = 4
+OPT_GRAPH_CHUNK = 5
+OPT_CHECK_EVERY = 6
+OPT_TIMING = 7
+
+TIME_STEP = 0
+TIME_PHASOR = 1
+
+PHASOR_NAMES = (
+    'ex_ph_d', 'ey_ph_d', 'hx_ph_d', 'hy_ph_d',
+    'ex_ph_u', 'ey_ph_u', 'hx_ph_u', 'hy_ph_u',
+    'ey_ph_l', 'ez_ph_l', 'hy_ph_l', 'hz_ph_l',
+    'ey_ph_r', 'ez_ph_r', 'hy_ph_r', 'hz_ph_r',
+    'ex_ph_f', 'ez_ph_f', 'hx_ph_f', 'hz_ph_f',
+    'ex_ph_b', 'ez_ph_b', 'hx_ph_b', 'hz_ph_b',
+)
+FIELD_NAMES = ('ex', 'ey', 'ez', 'hx', 'hy', 'hz')
+
+
+class FdtdError(RuntimeError):
+    """A libfdtd_b200 call failed; ``code`` is the FDTD_ERR_* status."""
+
+    def __init__(self, code, msg):
+        super().__init__(f'libfdtd_b200 error {code}: {msg}')
+        self.code = code
+
+
+class Geometry(ctypes.Structure):
+    """Mirror of ``fdtd_geometry``."""
+    _fields_ = [
+        ('nx', ctypes.c_int32), ('ny', ctypes.c_int32), ('nz', ctypes.c_int32),
+        ('npml', ctypes.c_int32), ('tfsf_z', ctypes.c_int32), ('nt', ctypes.c_int32),
+        ('nt_inc', ctypes.c_int32), ('dtype', ctypes.c_int32),
+        ('cell_size', ctypes.c_double), ('timestep', ctypes.c_double),
+        ('frequency', ctypes.c_double), ('db', ctypes.c_double), ('dtm0', ctypes.c_double),
+        ('dte0dx', ctypes.c_double),
+    ]
+
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_D = ctypes.c_double
+
+# name -> argtypes; every function returns int
+SIGNATURES = {
+    'fdtd_last_error': [ctypes.c_char_p, _I],
+    'fdtd_version': [],
+    'fdtd_device_count': [ctypes.POINTER(_I)],
+    'fdtd_create': [ctypes.POINTER(Geometry), _I, ctypes.POINTER(_P)],
+    'fdtd_destroy': [_P],
+    'fdtd_set_option': [_P, _I, _I],
+    'fdtd_get_option': [_P, _I, ctypes.POINTER(_I)],
+    'fdtd_set_absorbers': [_P, _P],
+    'fdtd_set_materials': [_P, _P, _P],
+    'fdtd_set_materials_eps_sigma': [_P, _P, _P, _I],
+    'fdtd_set_incident': [_P, _P, _P, _P, _P, _I],
+    'fdtd_reset': [_P],
+    'fdtd_run': [_P, _I],
+    'fdtd_run_streamed': [_P, _I, _P, _P, _P, _P],
+    'fdtd_synchronize': [_P],
+    'fdtd_step_index': [_P, ctypes.POINTER(ctypes.c_int64)],
+    'fdtd_get_stream': [_P, ctypes.POINTER(_P)],
+    'fdtd_set_stream': [_P, _P],
+    'fdtd_get_kernel_time': [_P, _I, ctypes.POINTER(_D), ctypes.POINTER(_I)],
+    'fdtd_clear_kernel_time': [_P],
+    'fdtd_get_phasor': [_P, _I, _P],
+    'fdtd_get_field': [_P, _I, _P],
+    'fdtd_set_field': [_P, _I, _P],
+    'fdtd_near2far': [_P, _P, _P, _P, _I, _I, _I, _I, _D, _D, _P, _I, _P, _I, _D, _I, _P],
+}
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f'{LIB_PATH} is missing: build it with '
+            f'`python sar-pixel-simulator_b200/build.py` (there is no CPU fallback)')
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, argtypes in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = argtypes
+        fn.restype = ctypes.c_int
+    return lib
+
+
+lib = _load()
+
+
+def last_error():
+    buf = ctypes.create_string_buffer(1024)
+    lib.fdtd_last_error(buf, len(buf))
+    return buf.value.decode(errors='replace')
+
+
+def check(rc):
+    if rc != FDTD_OK:
+        raise FdtdError(rc, last_error())
+
+
+def device_count():
+    n = ctypes.c_int(0)
+    check(lib.fdtd_device_count(ctypes.byref(n)))
+    return n.value
+
+
+def ptr(a: np.ndarray):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def dtype_code(dtype):
+    dt = np.dtype(dtype)
+    if dt == np.float32:
+        return FDTD_F32
+    if dt == np.float64:
+        return FDTD_F64
+    raise ValueError('Invalid dtype specifier')
+
+
+class NativeSim:
+    """Owning wrapper of one ``fdtd_sim`` handle."""
+
+    def __init__(self, geom: Geometry, device: int = 0):
+        self.geom = geom
+        self.dtype = np.float32 if geom.dtype == FDTD_F32 else np.float64
+        self.cdtype = np.complex64 if geom.dtype == FDTD_F32 else np.complex128
+        h = ctypes.c_void_p()
+        check(lib.fdtd_create(ctypes.byref(geom), int(device), ctypes.byref(h)))
+        self.h = h
+        self.nx_ph = geom.nx - 2 * geom.npml
+        self.ny_ph = geom.ny - 2 * geom.npml
+        self.nz_ph = geom.nz - 2 * geom.npml
+
+    def close(self):
+        if getattr(self, 'h', None) is not None and self.h.value:
+            lib.fdtd_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _arr(self, a, shape=None):
+        a = np.ascontiguousarray(a, dtype=self.dtype)
+        if shape is not None and a.shape != tuple(shape):
+            raise ValueError(f'expected shape {tuple(shape)}, got {a.shape}')
+        return a
+
+    def set_option(self, opt, value):
+        check(lib.fdtd_set_option(self.h, int(opt), int(value)))
+
+    def get_option(self, opt):
+        v = ctypes.c_int(0)
+        check(lib.fdtd_get_option(self.h, int(opt), ctypes.byref(v)))
+        return v.value
+
+    def set_absorbers(self, packed):
+        a = self._arr(packed, (8 * self.geom.npml,))
+        check(lib.fdtd_set_absorbers(self.h, ptr(a)))
+
+    def set_materials(self, ca, cb):
+        g = self.geom
+        shape = (g.nz, g.ny, g.nx)
+        a, b = self._arr(ca, shape), self._arr(cb, shape)
+        check(lib.fdtd_set_materials(self.h, ptr(a), ptr(b)))
+
+    def set_materials_eps_sigma(self, eps_r, sigma):
+        g = self.geom
+        e, s = self._arr(eps_r), self._arr(sigma)
+        if e.shape != s.shape or e.ndim != 3 or e.shape[1:] != (g.ny, g.nx):
+            raise ValueError(f'eps/sigma must both be (nz_mat, {g.ny}, {g.nx})')
+        check(lib.fdtd_set_materials_eps_sigma(self.h, ptr(e), ptr(s), int(e.shape[0])))
+
+    def set_incident(self, ex, ey, hx, hy):
+        g = self.geom
+        shape = (g.nt_inc, g.ny, g.nx)
+        arrs = [self._arr(c, shape) for c in (ex, ey, hx, hy)]
+        check(lib.fdtd_set_incident(self.h, *[ptr(a) for a in arrs], int(g.nt_inc)))
+
+    def reset(self):
+        check(lib.fdtd_reset(self.h))
+
+    def run(self, nsteps):
+        check(lib.fdtd_run(self.h, int(nsteps)))
+
+    def run_streamed(self, nsteps, ex, ey, hx, hy):
+        g = self.geom
+        shape = (g.nt_inc, g.ny, g.nx)
+        arrs = [self._arr(c, shape) for c in (ex, ey, hx, hy)]
+        check(lib.fdtd_run_streamed(self.h, int(nsteps), *[ptr(a) for a in arrs]))
+
+    def synchronize(self):
+        check(lib.fdtd_synchronize(self.h))
+
+    def step_index(self):
+        t = ctypes.c_int64(0)
+        check(lib.fdtd_step_index(self.h, ctypes.byref(t)))
+        return t.value
+
+    def stream(self):
+        s = ctypes.c_void_p()
+        check(lib.fdtd_get_stream(self.h, ctypes.byref(s)))
+        return s.value
+
+    def set_stream(self, stream_handle):
+        check(lib.fdtd_set_stream(self.h, ctypes.c_void_p(stream_handle or 0)))
+
+    def kernel_time(self, kind):
+        ms = ctypes.c_double(0)
+        n = ctypes.c_int(0)
+        check(lib.fdtd_get_kernel_time(self.h, int(kind), ctypes.byref(ms), ctypes.byref(n)))
+        return ms.value, n.value
+
+    def clear_kernel_time(self):
+        check(lib.fdtd_clear_kernel_time(self.h))
+
+    def phasor_shape(self, k):
+        if k < 8:
+            return (self.ny_ph, self.nx_ph)
+        if k < 16:
+            return (self.nz_ph, self.ny_ph)
+        return (self.nz_ph, self.nx_ph)
+
+    def get_phasor(self, k):
+        out = np.zeros(self.phasor_shape(k), self.cdtype)
+        check(lib.fdtd_get_phasor(self.h, int(k), ptr(out)))
+        return out
+
+    def get_phasors(self):
+        return {name: self.get_phasor(k) for k, name in enumerate(PHASOR_NAMES)}
+
+    def get_field(self, comp):
+        g = self.geom
+        k = FIELD_NAMES.index(comp) if isinstance(comp, str) else int(comp)
+        out = np.zeros((g.nz, g.ny, g.nx), self.dtype)
+        check(lib.fdtd_get_field(self.h, k, ptr(out)))
+        return out
+
+    def set_field(self, comp, arr):
+        g = self.geom
+        k = FIELD_NAMES.index(comp) if isinstance(comp, str) else int(comp)
+        a = self._arr(arr, (g.nz, g.ny, g.nx))
+        check(lib.fdtd_set_field(self.h, k, ptr(a)))
+
+    def get_fields(self):
+        return {c: self.get_field(c) for c in FIELD_NAMES}
+
+
+def near2far(ex_u, ey_u, hx_u, hy_u, nx, ny, nz, dx, r, thetas_deg, phis_deg, freq, device=0):
+    """Device near-to-far transform; returns E_theta, E_phi, H_theta, H_phi as
+    (nphi, ntheta) complex128 arrays."""
+    ex_u = np.asarray(ex_u)
+    in_dtype = FDTD_F32 if ex_u.dtype == np.complex64 else FDTD_F64
+    cdt = np.complex64 if in_dtype == FDTD_F32 else np.complex128
+    planes = [np.ascontiguousarray(p, dtype=cdt) for p in (ex_u, ey_u, hx_u, hy_u)]
+    for p in planes:
+        if p.shape != (ny, nx):
+            raise ValueError(f'phasor planes must be ({ny}, {nx}), got {p.shape}')
+    th = np.ascontiguousarray(thetas_deg, dtype=np.float64)
+    ph = np.ascontiguousarray(phis_deg, dtype=np.float64)
+    out = np.zeros((4, ph.size, th.size), np.complex128)
+    check(lib.fdtd_near2far(*[ptr(p) for p in planes], in_dtype, int(nx), int(ny), int(nz),
+                            float(dx), float(r), ptr(th), int(th.size), ptr(ph), int(ph.size),
+                            float(freq), int(device), ptr(out)))
+    return {'E_theta': out[0], 'E_phi': out[1], 'H_theta': out[2], 'H_phi': out[3]}

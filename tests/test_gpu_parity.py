@@ -1,0 +1,144 @@
+"""CUDA path vs the oracle (and vs the reference's own fixtures), through the
+C-ABI. In the reference phasor mode the device reproduces the reference's
+float32 arithmetic bit for bit, so fields and phasors are compared exactly;
+the Kahan mode is held to the 1e-4 relative bar of the metric."""
+import os
+
+import numpy as np
+import pytest
+
+import fdtd_oracle as O
+from fdtdsarsim_b200 import _native
+from helpers import (GOLDEN, bits_equal, make_params, native_for, oracle_for, random_problem,
+                     rel_err)
+
+pytestmark = pytest.mark.gpu
+
+SPLIT, FUSED = _native.FDTD_KERNEL_SPLIT, _native.FDTD_KERNEL_FUSED
+
+CASES = [
+    # nx, ny, nz, tfsf_z, nt, ntp, dtype
+    (27, 25, 23, 14, 40, 30, 'float32'),
+    (41, 37, 29, 16, 35, 35, 'float32'),     # nx, ny not multiples of anything
+    (27, 25, 23, 20, 30, 20, 'float32'),     # injection plane inside the upper CPML
+    (33, 23, 25, 12, 25, 10, 'float64'),
+]
+
+
+def _run_both(case, seed, kernel=SPLIT, tile=(32, 8), phasor_mode=0, steps=None):
+    nx, ny, nz, tfsf, nt, ntp, dtype = case
+    pc = make_params(nx, ny, nz, tfsf, nt, ntp, dtype=dtype)
+    _, _, ca, cb, inc = random_problem(pc, seed)
+    orc = oracle_for(pc)
+    steps = nt if steps is None else steps
+    orc.run(ca, cb, inc, steps)
+    sim = native_for(pc, kernel, tile, phasor_mode)
+    sim.set_materials(ca, cb)
+    sim.set_incident(inc['ex'], inc['ey'], inc['hx'], inc['hy'])
+    sim.run(steps)
+    sim.synchronize()
+    return orc, sim
+
+
+@pytest.mark.parametrize('case', CASES)
+def test_split_matches_oracle_bit_exact(case):
+    orc, sim = _run_both(case, seed=101)
+    for c in _native.FIELD_NAMES:
+        assert bits_equal(sim.get_field(c), getattr(orc, c)), c
+    for k, name in enumerate(_native.PHASOR_NAMES):
+        assert bits_equal(sim.get_phasor(k), orc.ph[name]), name
+    sim.close()
+
+
+@pytest.mark.parametrize('kernel', [SPLIT, FUSED], ids=['split', 'fused'])
+@pytest.mark.parametrize('tag', ['f32', 'f32_tfsf_in_pml'])
+def test_device_reproduces_reference_fixture(tag, kernel):
+    """Same inputs the reference ran on (tests/golden), same CPML profiles:
+    fields and 24 phasor planes equal the reference's outputs exactly."""
+    g = np.load(os.path.join(GOLDEN, f'mainloop_{tag}.npz'))
+    ab = np.load(os.path.join(GOLDEN, 'absorbers.npz'))
+    pc = make_params(int(g['nx']), int(g['ny']), int(g['nz']), int(g['tfsf_z']), int(g['nt']),
+                     int(g['ntp']))
+    assert pc.geom_params.cell_size == float(g['dx'])
+    from fdtdsarsim_b200.gpu.main_sim import native_geometry
+    sim = _native.NativeSim(native_geometry(pc), 0)
+    sim.set_absorbers(np.concatenate([ab[f'float32_0.021_{k}'] for k in
+                                      ('be_d', 'bh_d', 'ce_d', 'ch_d', 'be_u', 'bh_u',
+                                       'ce_u', 'ch_u')]))
+    sim.set_option(_native.OPT_KERNEL, kernel)
+    sim.set_materials(g['ca'], g['cb'])
+    sim.set_incident(g['inc_ex'], g['inc_ey'], g['inc_hx'], g['inc_hy'])
+    sim.run(int(g['nt']))
+    sim.synchronize()
+    for c in _native.FIELD_NAMES:
+        assert bits_equal(sim.get_field(c), g[f'field_{c}']), c
+    for k, name in enumerate(_native.PHASOR_NAMES):
+        assert bits_equal(sim.get_phasor(k), g[name]), name
+    sim.close()
+
+
+@pytest.mark.parametrize('case', CASES[:2])
+def test_kahan_phasors_within_tolerance(case):
+    orc, sim = _run_both(case, seed=7, phasor_mode=_native.FDTD_PHASOR_KAHAN)
+    for c in _native.FIELD_NAMES:
+        assert bits_equal(sim.get_field(c), getattr(orc, c)), c
+    for k, name in enumerate(_native.PHASOR_NAMES):
+        err = rel_err(sim.get_phasor(k), orc.ph[name])
+        assert err < 1e-5, (name, err)   # metric bar: 1e-4 relative
+    sim.close()
+
+
+def test_split_runs_in_chunks_and_resets():
+    case = CASES[0]
+    nx, ny, nz, tfsf, nt, ntp, dtype = case
+    pc = make_params(nx, ny, nz, tfsf, nt, ntp, dtype=dtype)
+    _, _, ca, cb, inc = random_problem(pc, 5)
+    orc = oracle_for(pc)
+    orc.run(ca, cb, inc, nt)
+    sim = native_for(pc)
+    sim.set_materials(ca, cb)
+    sim.set_incident(inc['ex'], inc['ey'], inc['hx'], inc['hy'])
+    for _ in range(2):
+        sim.reset()
+        for n in (1, 7, 12, nt - 20):
+            sim.run(n)
+        sim.synchronize()
+        assert sim.step_index() == nt
+        for c in _native.FIELD_NAMES:
+            assert bits_equal(sim.get_field(c), getattr(orc, c)), c
+        assert bits_equal(sim.get_phasor(5), orc.ph['ey_ph_u'])
+    with pytest.raises(_native.FdtdError):
+        sim.run(1)   # beyond size_t
+    sim.close()
+
+
+def test_eps_sigma_on_device_matches_host_coefficients():
+    case = CASES[1]
+    nx, ny, nz, tfsf, nt, ntp, dtype = case
+    pc = make_params(nx, ny, nz, tfsf, nt, ntp, dtype=dtype)
+    eps, sig, ca, cb, inc = random_problem(pc, 9)
+    a = native_for(pc)
+    a.set_materials(ca, cb)
+    b = native_for(pc)
+    b.set_materials_eps_sigma(eps, sig)
+    for s in (a, b):
+        s.set_incident(inc['ex'], inc['ey'], inc['hx'], inc['hy'])
+        s.run(20)
+        s.synchronize()
+    for c in _native.FIELD_NAMES:
+        assert bits_equal(a.get_field(c), b.get_field(c)), c
+    a.close()
+    b.close()
+
+
+def test_state_errors():
+    pc = make_params(27, 25, 23, 14, 10, 5)
+    sim = native_for(pc)
+    with pytest.raises(_native.FdtdError) as ei:
+        sim.run(1)
+    assert ei.value.code == _native.FDTD_ERR_STATE
+    with pytest.raises(_native.FdtdError):
+        sim.get_phasor(24)
+    with pytest.raises(ValueError):
+        sim.set_materials(np.zeros((3, 3, 3), np.float32), np.zeros((3, 3, 3), np.float32))
+    sim.close()

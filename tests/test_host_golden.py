@@ -1,0 +1,122 @@
+"""Host logic of the package (geometry, CPML profiles, material
+coefficients, file layout) against the reference's own outputs."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from helpers import GOLDEN, bits_equal, make_params
+from fdtdsarsim_b200 import parameters as P
+from fdtdsarsim_b200.absorbers import cpml_profiles, packed_profiles, PROFILE_ORDER
+from fdtdsarsim_b200.materials import MaterialModel, compute_material_arrays
+from fdtdsarsim_b200 import resultsio
+
+
+def test_set_geom_params_matches_reference():
+    with open(os.path.join(GOLDEN, 'geom_cases.json')) as fh:
+        cases = json.load(fh)
+    for case in cases:
+        sx, sy, sz, dur, cs, unit, mf, incd, freq = case['args']
+        pc = P.ParameterCollection()
+        pc.inc_beam_params.frequency = freq
+        pc.inc_beam_params.duration = incd
+        pc.material_params.material_fraction = mf
+        P.set_geom_params(pc, sx, sy, sz, dur, cs, unit)
+        for k, v in case['geom'].items():
+            assert getattr(pc.geom_params, k) == v, (case['args'], k)
+
+
+def test_set_geom_params_bad_unit():
+    pc = P.ParameterCollection()
+    pc.inc_beam_params.frequency = 5.4e9
+    with pytest.raises(ValueError):
+        P.set_geom_params(pc, 1.0, 1.0, 0.5, 10.0, 0.05, 'furlong')
+
+
+def test_round_to_odd():
+    assert P.round_to_odd(39.0) == 39
+    assert P.round_to_odd(30.0) == 31
+    assert P.round_to_odd(30.9) == 31
+    with pytest.raises(ValueError):
+        P.round_to_odd(-1.0)
+
+
+@pytest.mark.parametrize('dtype', ['float32', 'float64'])
+@pytest.mark.parametrize('cell_wl', [0.021, 0.05])
+def test_cpml_profiles_bit_exact(dtype, cell_wl):
+    ab = np.load(os.path.join(GOLDEN, 'absorbers.npz'))
+    pc = make_params(25, 23, 27, 14, 10, 5, dtype=dtype, cell_wl=cell_wl)
+    tag = f'{dtype}_{cell_wl}'
+    assert pc.geom_params.cell_size == float(ab[f'{tag}_dx'])
+    prof = cpml_profiles(pc)
+    for k in PROFILE_ORDER:
+        assert bits_equal(prof[k], ab[f'{tag}_{k}']), k
+    packed = packed_profiles(pc)
+    assert packed.shape == (80,) and packed.dtype == np.dtype(dtype)
+
+
+@pytest.mark.parametrize('dtype', ['float32', 'float64'])
+def test_material_arrays_bit_exact(dtype):
+    m = np.load(os.path.join(GOLDEN, 'materials.npz'))
+    pc = make_params(25, 23, int(m[f'{dtype}_nz']), 14, 10, 5, dtype=dtype)
+    pc.geom_params.size_z_material = m[f'{dtype}_eps'].shape[0]
+    ca, cb = compute_material_arrays(pc, MaterialModel(m[f'{dtype}_eps'], m[f'{dtype}_sigma'], 1.0))
+    assert bits_equal(ca, m[f'{dtype}_ca'])
+    assert bits_equal(cb, m[f'{dtype}_cb'])
+
+
+def test_material_shape_mismatch():
+    pc = make_params(25, 23, 27, 14, 10, 5)
+    with pytest.raises(RuntimeError):
+        compute_material_arrays(pc, MaterialModel(np.ones((3, 23, 25), 'float32'),
+                                                  np.ones((4, 23, 25), 'float32'), 1.0))
+
+
+def test_load_from_json(tmp_path):
+    d = {
+        'processing_type': 'gpu', 'gpu_num': 0, 'threads_per_proc': 6,
+        'datatype': 'float32', 'project_dir': str(tmp_path), 'frequency_hz': 5.4e9,
+        'polarization': 'HH', 'theta_angle_deg': 20.0, 'phi_angle_deg': 0.0,
+        'incident_duration': 8.0, 'illumination_width': 8.0, 'generate_new': False,
+        'size_x': 14.0, 'size_y': 14.0, 'size_z_material': 4.0, 'simulation_duration': 16.0,
+        'cell_size': 0.025, 'unit': 'wavelength', 'material_fraction': 0.7,
+        'disp_inc_results': False, 'disp_inc_sim_movie': False, 'disp_debug': False,
+        'disp_main_sim_movie': False, 'disp_materials': False,
+    }
+    p = tmp_path / 'params.json'
+    p.write_text(json.dumps(d))
+    pc = P.load_from_json(str(p))
+    with open(os.path.join(GOLDEN, 'geom_cases.json')) as fh:
+        ref = [c for c in json.load(fh) if c['args'][:3] == [14.0, 14.0, 4.0]][0]['geom']
+    for k, v in ref.items():
+        if k != 'simulation_duration':  # set by load_from_json, not set_geom_params
+            assert getattr(pc.geom_params, k) == v, k
+    assert pc.geom_params.simulation_duration == 16.0
+    assert P.inc_filename(pc).endswith(
+        f'incident/inc_nx{ref["size_x"]}_ny{ref["size_y"]}_nt{ref["size_t_inc"]}_theta20_phi0_HH.hdf5')
+    assert P.results_filename(pc, 'm1').endswith('results/m1.hdf5')
+    del d['size_x']
+    p.write_text(json.dumps(d))
+    pc2 = P.load_from_json(str(p))
+    assert pc2.geom_params.size_x == 0 and pc2.geom_params.simulation_duration == 16.0
+
+
+def test_resultsio_roundtrip(tmp_path):
+    fname = str(tmp_path / 'r.hdf5')
+    with resultsio.File(fname, 'w') as f:
+        g = f.create_group('phasors')
+        g.attrs['nx_phasor'] = 5
+        g.create_dataset('ex_ph_u', data=np.arange(6, dtype=np.complex64).reshape(2, 3))
+        f.create_group('parameters').attrs['polarization'] = 'HH'
+        f.create_group('material_metadata')
+    assert resultsio.exists(fname)
+    with resultsio.File(fname, 'r+') as f:
+        assert f['phasors'].attrs['nx_phasor'] == 5
+        assert str(f['parameters'].attrs['polarization']) == 'HH'
+        assert 'material_metadata' in f
+        np.testing.assert_array_equal(f['phasors/ex_ph_u'][:],
+                                      np.arange(6, dtype=np.complex64).reshape(2, 3))
+        f.create_group('farfield').create_dataset('e_phi', data=np.ones(3))
+    with resultsio.File(fname, 'r') as f:
+        assert f['farfield']['e_phi'].shape == (3,)
