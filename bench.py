@@ -221,9 +221,9 @@ def run_ours(a):
             sim.set_option(_native.OPT_TILE_Y, choice['tile_y'])
         return sim
 
-    stream = torch.cuda.current_stream()
     sim = new_sim()
-    sim.set_stream(stream.cuda_stream)
+    # time on the stream the library launches on
+    stream = torch.cuda.ExternalStream(sim.stream())
     sim.set_materials(ca, cb)
     sim.set_incident(inc['ex'], inc['ey'], inc['hx'], inc['hy'])
 
