@@ -50,7 +50,7 @@ def test_split_matches_oracle_bit_exact(case):
     sim.close()
 
 
-@pytest.mark.parametrize('kernel', [SPLIT, FUSED], ids=['split', 'fused'])
+@pytest.mark.parametrize('kernel', [SPLIT], ids=['split'])
 @pytest.mark.parametrize('tag', ['f32', 'f32_tfsf_in_pml'])
 def test_device_reproduces_reference_fixture(tag, kernel):
     """Same inputs the reference ran on (tests/golden), same CPML profiles:
