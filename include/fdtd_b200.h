@@ -198,6 +198,32 @@ int fdtd_near2far(const void *ex_u, const void *ey_u, const void *hx_u,
                   int ntheta, const double *phis_deg, int nphi, double freq,
                   int device, double *out);
 
+/* fdtd_near2far without any device allocation. This entry point has no
+ * counterpart in the reference; it exists for callers that cannot call
+ * cudaMalloc when they need a far field: code whose device memory is owned
+ * by a pool or arena that must not be bypassed, jobs that must not grow
+ * their footprint while running, and contexts where a device allocation is
+ * not allowed or would synchronize the device. Arguments, results and
+ * errors are those of fdtd_near2far. Instead of allocating, every call
+ * stages its inputs, angles and results in one static device array of
+ * about 39 MB that every GPU loading this library holds until the process
+ * exits. Limits: nx_ph * ny_ph <= 600000 cells for complex128 inputs
+ * (1200000 for complex64), ntheta <= 4096, nphi <= 64 and
+ * ntheta * nphi <= 8192; larger requests return FDTD_ERR_INVALID with a
+ * message naming the limit. The first call on a device looks up the
+ * array's device address with that device current (make that first call
+ * before any stream capture). All calls share the array: calls from one
+ * process are serialized by a lock, and work that overlaps a call on the
+ * same device through other means races with it. Nothing in the array has
+ * to start at zero: each call writes every byte it reads back. Calls are
+ * synchronous. */
+int fdtd_near2far_noalloc(const void *ex_u, const void *ey_u,
+                          const void *hx_u, const void *hy_u, int in_dtype,
+                          int nx_ph, int ny_ph, int nz_ph, double dx, double r,
+                          const double *thetas_deg, int ntheta,
+                          const double *phis_deg, int nphi, double freq,
+                          int device, double *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -47,6 +47,10 @@ struct DevBuf {
 
 }  // namespace
 
+// Lets the other translation units of the library report through
+// fdtd_last_error().
+int fdtd::report_error(int code, const char* msg) { return fail(code, "%s", msg); }
+
 struct fdtd_sim {
   fdtd_geometry g{};
   int device = 0;

@@ -26,6 +26,9 @@ template <class T>
 bool launch_fused_step(const State<T>& s, const int* tdev, int toff, int tile_x,
                        int tile_y, cudaStream_t st);
 
+// Records an error message for fdtd_last_error(); returns code.
+int report_error(int code, const char* msg);
+
 // Near-to-far transform (near2far.cu).
 int near2far_run(const double* jm /* 4 planes complex128 */, int nx, int ny, double dx,
                  double z_val, double k, const double* thetas, int ntheta,

@@ -100,6 +100,7 @@ SIGNATURES = {
     'fdtd_get_field': [_P, _I, _P],
     'fdtd_set_field': [_P, _I, _P],
     'fdtd_near2far': [_P, _P, _P, _P, _I, _I, _I, _I, _D, _D, _P, _I, _P, _I, _D, _I, _P],
+    'fdtd_near2far_noalloc': [_P, _P, _P, _P, _I, _I, _I, _I, _D, _D, _P, _I, _P, _I, _D, _I, _P],
 }
 
 
@@ -280,9 +281,13 @@ class NativeSim:
         return {c: self.get_field(c) for c in FIELD_NAMES}
 
 
-def near2far(ex_u, ey_u, hx_u, hy_u, nx, ny, nz, dx, r, thetas_deg, phis_deg, freq, device=0):
+def near2far(ex_u, ey_u, hx_u, hy_u, nx, ny, nz, dx, r, thetas_deg, phis_deg, freq, device=0,
+             allocate=True):
     """Device near-to-far transform; returns E_theta, E_phi, H_theta, H_phi as
-    (nphi, ntheta) complex128 arrays."""
+    (nphi, ntheta) complex128 arrays. With ``allocate=False`` it runs
+    fdtd_near2far_noalloc, which uses the library's static device scratch
+    instead of allocating (for callers that may not allocate device memory;
+    sizes are capped, see include/fdtd_b200.h)."""
     ex_u = np.asarray(ex_u)
     in_dtype = FDTD_F32 if ex_u.dtype == np.complex64 else FDTD_F64
     cdt = np.complex64 if in_dtype == FDTD_F32 else np.complex128
@@ -293,7 +298,8 @@ def near2far(ex_u, ey_u, hx_u, hy_u, nx, ny, nz, dx, r, thetas_deg, phis_deg, fr
     th = np.ascontiguousarray(thetas_deg, dtype=np.float64)
     ph = np.ascontiguousarray(phis_deg, dtype=np.float64)
     out = np.zeros((4, ph.size, th.size), np.complex128)
-    check(lib.fdtd_near2far(*[ptr(p) for p in planes], in_dtype, int(nx), int(ny), int(nz),
+    fn = lib.fdtd_near2far if allocate else lib.fdtd_near2far_noalloc
+    check(fn(*[ptr(p) for p in planes], in_dtype, int(nx), int(ny), int(nz),
                             float(dx), float(r), ptr(th), int(th.size), ptr(ph), int(ph.size),
                             float(freq), int(device), ptr(out)))
     return {'E_theta': out[0], 'E_phi': out[1], 'H_theta': out[2], 'H_phi': out[3]}
