@@ -41,6 +41,8 @@ def parse():
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--workload', default='plain_16x16', choices=['plain_16x16', 'plain_8x8'])
     ap.add_argument('--kernel', default='auto', choices=['auto', 'split', 'fused'])
+    ap.add_argument('--tile-y', type=int, default=None, help='fused kernel rows per tile')
+    ap.add_argument('--zchunk', type=int, default=0, help='fused kernel z planes per block (0: auto)')
     ap.add_argument('--dtype', default='float32', choices=['float32', 'float64'])
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-cpu-baseline', action='store_true')
@@ -210,7 +212,8 @@ def run_ours(a):
     geom = native_geometry(pc)
     kernel = {'auto': None, 'split': _native.FDTD_KERNEL_SPLIT,
               'fused': _native.FDTD_KERNEL_FUSED}[a.kernel]
-    choice = tuning.choose(geom, kernel=kernel)
+    choice = tuning.choose(geom, kernel=kernel,
+                           tile=None if a.tile_y is None else (32, a.tile_y))
 
     def new_sim():
         sim = _native.NativeSim(geom, local)
@@ -219,6 +222,7 @@ def run_ours(a):
         if choice['kernel'] == _native.FDTD_KERNEL_FUSED:
             sim.set_option(_native.OPT_TILE_X, choice['tile_x'])
             sim.set_option(_native.OPT_TILE_Y, choice['tile_y'])
+            sim.set_option(_native.OPT_ZCHUNK, a.zchunk)
         return sim
 
     sim = new_sim()

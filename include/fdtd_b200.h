@@ -54,11 +54,14 @@ extern "C" {
 /* options */
 #define FDTD_OPT_KERNEL       1
 #define FDTD_OPT_PHASOR_MODE  2
-#define FDTD_OPT_TILE_X       3  /* fused kernel tile width (cells) */
-#define FDTD_OPT_TILE_Y       4  /* fused kernel tile height (cells) */
+#define FDTD_OPT_TILE_X       3  /* fused kernel tile width in threads of
+                                    4 x cells each; 32 (128 cells) */
+#define FDTD_OPT_TILE_Y       4  /* fused kernel tile height in rows:
+                                    4, 7, 8 (float, double), 15, 16 (float) */
 #define FDTD_OPT_GRAPH_CHUNK  5  /* steps per captured CUDA graph (0 = no graph) */
 #define FDTD_OPT_CHECK_EVERY  6  /* non-finite check period in steps (0 = off) */
 #define FDTD_OPT_TIMING       7  /* 1: record CUDA events around every kernel */
+#define FDTD_OPT_ZCHUNK       8  /* fused kernel z planes per block (0 = automatic) */
 
 /* kernel kinds of fdtd_get_kernel_time */
 #define FDTD_TIME_STEP    0   /* the field-update kernel(s) of a step */

@@ -82,6 +82,7 @@ struct fdtd_sim {
   int kernel = FDTD_KERNEL_SPLIT;
   int phasor_mode = FDTD_PHASOR_REFERENCE;
   int tile_x = 32, tile_y = 8;
+  int zchunk = 0;
   int graph_chunk = 0;
   int check_every = 0;
   // per-kernel event timing
@@ -185,7 +186,7 @@ int enqueue_steps(fdtd_sim* s, int n) {
     mark(s, e0);
     if (s->kernel == FDTD_KERNEL_FUSED) {
       State<T> st = make_state<T>(s, s->cur, 1 - s->cur);
-      if (!launch_fused_step<T>(st, s->tdev, k, s->tile_x, s->tile_y, s->stream))
+      if (!launch_fused_step<T>(st, s->tdev, k, s->tile_x, s->tile_y, s->zchunk, s->stream))
         return fail(FDTD_ERR_INVALID, "unsupported fused tile %dx%d", s->tile_x, s->tile_y);
       s->cur = 1 - s->cur;
       mark(s, e1);
@@ -391,6 +392,10 @@ int fdtd_set_option(fdtd_sim* s, int option, int value) {
       if (value < 1 || value > 64) return fail(FDTD_ERR_INVALID, "bad tile_y %d", value);
       s->tile_y = value;
       return FDTD_OK;
+    case FDTD_OPT_ZCHUNK:
+      if (value < 0) return fail(FDTD_ERR_INVALID, "bad z chunk %d", value);
+      s->zchunk = value;
+      return FDTD_OK;
     case FDTD_OPT_GRAPH_CHUNK:
       if (value < 0) return fail(FDTD_ERR_INVALID, "bad graph chunk %d", value);
       s->graph_chunk = value;
@@ -413,6 +418,7 @@ int fdtd_get_option(fdtd_sim* s, int option, int* value) {
     case FDTD_OPT_PHASOR_MODE: *value = s->phasor_mode; return FDTD_OK;
     case FDTD_OPT_TILE_X: *value = s->tile_x; return FDTD_OK;
     case FDTD_OPT_TILE_Y: *value = s->tile_y; return FDTD_OK;
+    case FDTD_OPT_ZCHUNK: *value = s->zchunk; return FDTD_OK;
     case FDTD_OPT_GRAPH_CHUNK: *value = s->graph_chunk; return FDTD_OK;
     case FDTD_OPT_CHECK_EVERY: *value = s->check_every; return FDTD_OK;
     case FDTD_OPT_TIMING: *value = s->timing; return FDTD_OK;

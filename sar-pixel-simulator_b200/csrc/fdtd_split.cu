@@ -8,54 +8,12 @@
 // Each thread updates four consecutive x cells with vector loads and
 // stores; interior cells take the plain curl update, the rest (CPML faces,
 // domain edges, the injection plane) the per-cell h_cell / e_cell.
-#include "fdtd_cell.cuh"
 #include "fdtd_launch.h"
+#include "fdtd_vec.cuh"
 
 namespace fdtd {
 
 __global__ void k_advance(int* t, int n) { *t += n; }
-
-// Four consecutive x cells per thread: the pitch is a multiple of 32, so a
-// thread's cells are one aligned 16-byte (float) or 32-byte (double) vector.
-constexpr int kVec = 4;
-
-template <class T>
-__device__ __forceinline__ void ld4(T (&d)[kVec], const T* p) {
-  if constexpr (sizeof(T) == 4) {
-    const float4 v = *reinterpret_cast<const float4*>(p);
-    d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
-  } else {
-    const double2 a = reinterpret_cast<const double2*>(p)[0];
-    const double2 b = reinterpret_cast<const double2*>(p)[1];
-    d[0] = a.x; d[1] = a.y; d[2] = b.x; d[3] = b.y;
-  }
-}
-
-template <class T>
-__device__ __forceinline__ void st4(T* p, const T (&d)[kVec]) {
-  if constexpr (sizeof(T) == 4) {
-    *reinterpret_cast<float4*>(p) = make_float4(d[0], d[1], d[2], d[3]);
-  } else {
-    reinterpret_cast<double2*>(p)[0] = make_double2(d[0], d[1]);
-    reinterpret_cast<double2*>(p)[1] = make_double2(d[2], d[3]);
-  }
-}
-
-template <class T>
-__device__ __forceinline__ void zero4(T (&d)[kVec]) {
-#pragma unroll
-  for (int j = 0; j < kVec; ++j) d[j] = T(0);
-}
-
-// True when every cell of the vector and every neighbour it reads lies away
-// from the CPML faces and the domain edges and plane z does not inject: the
-// update is then the plain curl update (Taflove 3.29 / 3.30).
-template <class T>
-__device__ __forceinline__ bool interior(const State<T>& s, int z, int y, int x0, int t) {
-  const int m = s.npml;
-  return z >= m && z < s.nz - m && y >= m && y < s.ny - m && x0 >= m && x0 + kVec <= s.nx - m &&
-         !injects(s, z, t);
-}
 
 // H pass: H^{n+1/2} = H^{n-1/2} - Db curl E^n, CPML and E-field injection,
 // in place (reads E only, writes the thread's own H and psi_H).

@@ -35,6 +35,7 @@ OPT_TILE_Y = 4
 OPT_GRAPH_CHUNK = 5
 OPT_CHECK_EVERY = 6
 OPT_TIMING = 7
+OPT_ZCHUNK = 8
 
 TIME_STEP = 0
 TIME_PHASOR = 1

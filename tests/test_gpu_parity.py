@@ -25,14 +25,24 @@ CASES = [
 ]
 
 
-def _run_both(case, seed, kernel=SPLIT, tile=(32, 8), phasor_mode=0, steps=None):
+# Grids wider than one fused tile (128 x cells): several x tiles, a partial
+# last tile, an x CPML face that straddles a tile edge (nx = 261: x 251..260,
+# tile edge 256), and a pitch that is not a multiple of the tile (nx = 150).
+WIDE = [
+    (261, 45, 30, 14, 24, 16, 'float32'),
+    (150, 61, 37, 20, 20, 20, 'float32'),
+    (140, 33, 26, 12, 16, 10, 'float64'),
+]
+
+
+def _run_both(case, seed, kernel=SPLIT, tile=(32, 8), phasor_mode=0, steps=None, zchunk=0):
     nx, ny, nz, tfsf, nt, ntp, dtype = case
     pc = make_params(nx, ny, nz, tfsf, nt, ntp, dtype=dtype)
     _, _, ca, cb, inc = random_problem(pc, seed)
     orc = oracle_for(pc)
     steps = nt if steps is None else steps
     orc.run(ca, cb, inc, steps)
-    sim = native_for(pc, kernel, tile, phasor_mode)
+    sim = native_for(pc, kernel, tile, phasor_mode, zchunk)
     sim.set_materials(ca, cb)
     sim.set_incident(inc['ex'], inc['ey'], inc['hx'], inc['hy'])
     sim.run(steps)
@@ -50,7 +60,87 @@ def test_split_matches_oracle_bit_exact(case):
     sim.close()
 
 
-@pytest.mark.parametrize('kernel', [SPLIT], ids=['split'])
+def _assert_matches(orc, sim):
+    for c in _native.FIELD_NAMES:
+        assert bits_equal(sim.get_field(c), getattr(orc, c)), c
+    for k, name in enumerate(_native.PHASOR_NAMES):
+        assert bits_equal(sim.get_phasor(k), orc.ph[name]), name
+
+
+@pytest.mark.parametrize('case', CASES + WIDE)
+def test_fused_matches_oracle_bit_exact(case):
+    orc, sim = _run_both(case, seed=202, kernel=FUSED)
+    _assert_matches(orc, sim)
+    sim.close()
+
+
+@pytest.mark.parametrize('tile_y,zchunk', [(4, 3), (7, 5), (8, 0), (15, 7), (16, 1)])
+def test_fused_tiles_and_chunks(tile_y, zchunk):
+    """Every tile height, and z chunks down to one plane (each chunk then
+    recomputes the plane below it)."""
+    case = WIDE[0] if tile_y != 16 else WIDE[1]
+    orc, sim = _run_both(case, seed=303, kernel=FUSED, tile=(32, tile_y), zchunk=zchunk)
+    _assert_matches(orc, sim)
+    sim.close()
+
+
+def test_fused_rejects_unsupported_tiles():
+    pc = make_params(27, 25, 23, 14, 10, 5)
+    _, _, ca, cb, inc = random_problem(pc, 1)
+    for tile in ((16, 8), (32, 5)):
+        sim = native_for(pc, FUSED, tile)
+        sim.set_materials(ca, cb)
+        sim.set_incident(inc['ex'], inc['ey'], inc['hx'], inc['hy'])
+        with pytest.raises(_native.FdtdError) as ei:
+            sim.run(1)
+        assert ei.value.code == _native.FDTD_ERR_INVALID
+        sim.close()
+
+
+def test_kernels_can_alternate_within_a_run():
+    """Fused steps use the ping-pong field and psi sets, split steps the
+    current set in place; switching between them at any step keeps the
+    oracle's values."""
+    case = WIDE[0]
+    nx, ny, nz, tfsf, nt, ntp, dtype = case
+    pc = make_params(nx, ny, nz, tfsf, nt, ntp, dtype=dtype)
+    _, _, ca, cb, inc = random_problem(pc, 17)
+    orc = oracle_for(pc)
+    orc.run(ca, cb, inc, nt)
+    sim = native_for(pc, FUSED)
+    sim.set_materials(ca, cb)
+    sim.set_incident(inc['ex'], inc['ey'], inc['hx'], inc['hy'])
+    done = 0
+    for n, k in ((3, FUSED), (2, SPLIT), (5, FUSED), (1, SPLIT), (nt - 11, FUSED)):
+        sim.set_option(_native.OPT_KERNEL, k)
+        sim.run(n)
+        done += n
+    sim.synchronize()
+    assert done == nt
+    _assert_matches(orc, sim)
+    sim.close()
+
+
+def test_fused_runs_in_chunks_and_resets():
+    case = WIDE[1]
+    nx, ny, nz, tfsf, nt, ntp, dtype = case
+    pc = make_params(nx, ny, nz, tfsf, nt, ntp, dtype=dtype)
+    _, _, ca, cb, inc = random_problem(pc, 23)
+    orc = oracle_for(pc)
+    orc.run(ca, cb, inc, nt)
+    sim = native_for(pc, FUSED)
+    sim.set_materials(ca, cb)
+    sim.set_incident(inc['ex'], inc['ey'], inc['hx'], inc['hy'])
+    for _ in range(2):
+        sim.reset()
+        for n in (1, 4, 7, nt - 12):
+            sim.run(n)
+        sim.synchronize()
+        _assert_matches(orc, sim)
+    sim.close()
+
+
+@pytest.mark.parametrize('kernel', [SPLIT, FUSED], ids=['split', 'fused'])
 @pytest.mark.parametrize('tag', ['f32', 'f32_tfsf_in_pml'])
 def test_device_reproduces_reference_fixture(tag, kernel):
     """Same inputs the reference ran on (tests/golden), same CPML profiles:
@@ -66,6 +156,7 @@ def test_device_reproduces_reference_fixture(tag, kernel):
                                       ('be_d', 'bh_d', 'ce_d', 'ch_d', 'be_u', 'bh_u',
                                        'ce_u', 'ch_u')]))
     sim.set_option(_native.OPT_KERNEL, kernel)
+    sim.set_option(_native.OPT_ZCHUNK, 4)
     sim.set_materials(g['ca'], g['cb'])
     sim.set_incident(g['inc_ex'], g['inc_ey'], g['inc_hx'], g['inc_hy'])
     sim.run(int(g['nt']))
