@@ -83,6 +83,8 @@ struct fdtd_sim {
   int phasor_mode = FDTD_PHASOR_REFERENCE;
   int tile_x = 32, tile_y = 8;
   int zchunk = 0;
+  FusedPlan plan;
+  int plan_ok = 0, plan_tile_y = 0, plan_zchunk = 0;
   int graph_chunk = 0;
   int check_every = 0;
   // per-kernel event timing
@@ -185,10 +187,25 @@ int enqueue_steps(fdtd_sim* s, int n) {
     cudaEvent_t e2 = s->timing ? timing_event(s) : nullptr;
     mark(s, e0);
     if (s->kernel == FDTD_KERNEL_FUSED) {
-      State<T> st = make_state<T>(s, s->cur, 1 - s->cur);
-      if (!launch_fused_step<T>(st, s->tdev, k, s->tile_x, s->tile_y, s->zchunk, s->stream))
+      const int nxt = 1 - s->cur;
+      if (!fused_supported_tile(s->tile_x, s->tile_y, (int)sizeof(T)))
         return fail(FDTD_ERR_INVALID, "unsupported fused tile %dx%d", s->tile_x, s->tile_y);
-      s->cur = 1 - s->cur;
+      if (!s->plan_ok || s->plan_tile_y != s->tile_y || s->plan_zchunk != s->zchunk) {
+        const fdtd_geometry& g = s->g;
+        s->plan = make_fused_plan(g.nx, g.ny, g.nz, g.npml, g.tfsf_z, s->tile_y, s->zchunk);
+        s->plan_tile_y = s->tile_y;
+        s->plan_zchunk = s->zchunk;
+        s->plan_ok = 1;
+      }
+      // interior and shell H pass read the source set only; the shell E
+      // pass reads the destination H that both of them wrote
+      State<T> st = make_state<T>(s, s->cur, nxt);
+      launch_fused_interior<T>(st, s->plan, s->tile_y, s->stream);
+      launch_shell_pass<T>(st, s->tdev, k, s->plan.shell, true, s->stream);
+      State<T> se = st;
+      se.ihx = (const T*)s->fld[nxt][3]; se.ihy = (const T*)s->fld[nxt][4]; se.ihz = (const T*)s->fld[nxt][5];
+      launch_shell_pass<T>(se, s->tdev, k, s->plan.shell, false, s->stream);
+      s->cur = nxt;
       mark(s, e1);
       State<T> sp = make_state<T>(s, s->cur, s->cur);
       launch_phasors<T>(sp, s->tdev, k, s->stream);

@@ -75,6 +75,33 @@ struct State {
   int kahan;
 };
 
+// A box of the fused step's shell, swept by the split passes one plane per
+// block row: [x0, x1) x [y0, y1) x [z0, z1), x0 a multiple of 4. A tile is
+// `width` lanes (width * 4 x cells) by 128 / width rows; gx, gy tiles per
+// plane; `first` is the box's first block in the launch.
+struct ShellBox {
+  int x0, x1, y0, y1, z0, z1;
+  int width, gx, gy;
+  int first;
+};
+constexpr int kMaxShellBoxes = 16;
+struct ShellBoxes {
+  int n, total_blocks;
+  ShellBox b[kMaxShellBoxes];
+};
+
+// The interior box of the fused step: no CPML face, domain edge or
+// injection plane touches any of its cells or the halo cells it recomputes.
+// x in [xa, xb) (xa a multiple of 32, xb of 4), y in [ya, yb), and up to
+// two z ranges [z0[k], z1[k]) cut into chunks of `zchunk` planes.
+struct InteriorBox {
+  int xa, xb, ya, yb;
+  int nz_ranges;
+  int z0[2], z1[2];
+  int zchunk;
+  int chunks0, chunks;   // chunks of the first range, of both ranges
+};
+
 __global__ void k_advance(int* t, int n);
 
 }  // namespace fdtd

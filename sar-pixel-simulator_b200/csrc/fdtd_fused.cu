@@ -1,28 +1,39 @@
 // fdtd_fused.cu -- the fused step: H^{n+1/2} and E^{n+1} of the whole grid
-// in one z-marching pass.
+// from the source field set into the destination set (ping-pong).
 //
-// The pass reads every field, Ca and Cb once from the source set and
-// writes every field once to the destination set (ping-pong), which is the
-// 56 B per FP32 cell-update minimum; the split H/E passes move 80 B.
+// Because every cell is written to a set that nothing reads during the
+// step, any partition of the grid can be updated by independent kernels,
+// each recomputing from the source set the few H^{n+1/2} values it needs
+// from a neighbour region. The step uses two regions:
 //
-// A block owns a tile of 128 x cells (32 lanes x 4 cells) by TY rows and a
-// chunk of z planes, and marches up the chunk one plane at a time. At plane
-// z a thread holds E(z) of its vector (carried from the previous plane),
-// loads E(z+1), H(z), Ca, Cb, and
+//  * the interior box, where no CPML face, domain edge or injection plane
+//    touches a cell or the halo it recomputes (about 80 % of the cells at
+//    the benchmark sizes): one z-marching pass that reads every field, Ca
+//    and Cb once and writes every field once (56 B per FP32 cell-update),
+//    with no boundary code at all, so nothing diverges and the kernel needs
+//    few registers;
+//  * the shell (CPML slabs, the injection planes, the strips beside the
+//    interior box): the split H pass over the shell boxes (source E, H ->
+//    destination H), then the split E pass (destination H, source E ->
+//    destination E). The E pass runs after the interior pass, whose
+//    destination H it reads at the shell's inner edge.
+//
+// Interior kernel. A block owns a tile of 128 x cells (32 lanes x 4 cells)
+// by TY rows and a chunk of z planes, and marches up the chunk one plane at
+// a time. At plane z a thread holds E(z) of its vector (carried from the
+// previous plane), loads E(z+1), H(z), Ca, Cb, and
 //   1. computes H^{n+1/2}(z) of its vector; the +x neighbour comes from the
 //      next lane by shuffle, the +y neighbour from the next thread row
 //      through shared memory, the +z neighbour is E(z+1);
 //   2. computes E^{n+1}(z); the -x neighbour comes by shuffle, the -y
 //      neighbour through shared memory, the -z neighbour is H^{n+1/2}(z-1)
 //      carried in registers.
-// H^{n+1/2} values that belong to neighbouring tiles are recomputed from
-// the source set rather than exchanged: thread row 0 computes the row below
-// the tile, lane 0 the column left of the tile (one cell per row), and the
-// first plane of a chunk is preceded by the plane below it. Recomputed cells
-// never write psi; every psi element is written once, by its owner, into
-// the destination psi set. Per-cell values are the same as the split
-// kernels' (the same update functions, the same order of operations).
+// Thread row 0 recomputes the row below the tile, lane 0 the column left of
+// the tile (one cell per row), and the plane below a chunk is recomputed
+// before the chunk. Per-cell values equal the split kernels' (the same
+// update formula in the same order of operations).
 #include <algorithm>
+#include <cstring>
 
 #include "fdtd_launch.h"
 #include "fdtd_vec.cuh"
@@ -35,13 +46,13 @@ constexpr unsigned kFull = 0xffffffffu;
 constexpr int kLanes = 32;
 constexpr int kRowCells = kLanes * kVec;   // x cells of one tile row
 
-// Two resident blocks per SM for float tiles up to 8 rows, one otherwise.
 template <class T, int TY>
-constexpr int fused_min_blocks() { return sizeof(T) == 4 && TY <= 8 ? 2 : 1; }
+constexpr int interior_min_blocks() { return sizeof(T) == 4 && TY <= 8 ? 2 : 1; }
 
 template <class T, int TY>
-__global__ void __launch_bounds__(kLanes * (TY + 1), fused_min_blocks<T, TY>())
-k_fused(const __grid_constant__ State<T> s, const int* __restrict__ tp, int toff, int zchunk) {
+__global__ void __launch_bounds__(kLanes * (TY + 1), interior_min_blocks<T, TY>())
+k_fused_interior(const __grid_constant__ State<T> s, InteriorBox ib) {
+  using M = R<T>;
   // E(z) of every thread row (read by the row below as its +y neighbour)
   // and H^{n+1/2}(z) (read by the row above as its -y neighbour).
   __shared__ __align__(32) T sEx[TY + 1][kRowCells];
@@ -50,15 +61,17 @@ k_fused(const __grid_constant__ State<T> s, const int* __restrict__ tp, int toff
   __shared__ __align__(32) T sHz[TY + 1][kRowCells];
 
   const int lane = threadIdx.x, r = threadIdx.y;
-  const int nx = s.nx, ny = s.ny, nz = s.nz;
-  const int x0 = blockIdx.x * kRowCells + lane * kVec;
-  const int y = blockIdx.y * TY + r - 1;          // row 0 is the row below the tile
-  const int z0 = blockIdx.z * zchunk;
-  const int z1 = min(nz, z0 + zchunk);
-  const int zs = max(z0 - 1, 0);                  // plane below the chunk
-  const int t = *tp + toff;
-  const bool vin = x0 < s.pitch && y >= 0 && y < ny;
-  const bool own = vin && r >= 1;
+  const int x0 = ib.xa + blockIdx.x * kRowCells + lane * kVec;
+  const int y = ib.ya + blockIdx.y * TY + r - 1;   // row 0 is the row below the tile
+  int c = blockIdx.z, k = 0;
+  if (c >= ib.chunks0) { c -= ib.chunks0; k = 1; }
+  const int z0 = ib.z0[k] + c * ib.zchunk;
+  const int z1 = min(ib.z1[k], z0 + ib.zchunk);
+  const int zs = z0 - 1;                           // plane below the chunk (interior)
+  // Rows from ya - 1 >= 0 up; rows past the grid and lanes past the pitch
+  // only feed the shared-memory exchange and the shuffles (as zeros).
+  const bool vin = x0 < s.pitch && y < s.ny;
+  const bool own = vin && r >= 1 && y < ib.yb && x0 < ib.xb;
   const long long P = s.plane, W = s.pitch;
   long long i = (long long)zs * P + (vin ? (long long)y * W + x0 : 0);
   const int so = lane * kVec;
@@ -72,30 +85,30 @@ k_fused(const __grid_constant__ State<T> s, const int* __restrict__ tp, int toff
 
   for (int z = zs; z < z1; ++z, i += P) {
     const bool work = own && z >= z0;   // this thread updates and stores plane z
-    // ---- loads of plane z ------------------------------------------------
-    if (vin && z + 1 < nz) { ld4(e.exz, s.iex + i + P); ld4(e.eyz, s.iey + i + P); ld4(ezz, s.iez + i + P); }
-    else { zero4(e.exz); zero4(e.eyz); zero4(ezz); }
-    if (vin) { ld4(h.hx, s.ihx + i); ld4(h.hy, s.ihy + i); ld4(h.hz, s.ihz + i); }
-    else { zero4(h.hx); zero4(h.hy); zero4(h.hz); }
+    // ---- loads of plane z (z + 1 < nz: the interior ends npml planes below the top)
+    if (vin) {
+      ld4(e.exz, s.iex + i + P); ld4(e.eyz, s.iey + i + P); ld4(ezz, s.iez + i + P);
+      ld4(h.hx, s.ihx + i); ld4(h.hy, s.ihy + i); ld4(h.hz, s.ihz + i);
+    } else {
+      zero4(e.exz); zero4(e.eyz); zero4(ezz); zero4(h.hx); zero4(h.hy); zero4(h.hz);
+    }
     T ca[kVec], cb[kVec];
     if (work) { ld4(ca, s.ca + i); ld4(cb, s.cb + i); }
     else { zero4(ca); zero4(cb); }
     if (r == TY) {   // +y neighbour of the top row lies in the next tile
-      if (vin && y + 1 < ny) { ld4(e.exy, s.iex + i + W); ld4(e.ezy, s.iez + i + W); }
+      if (vin && y + 1 < s.ny) { ld4(e.exy, s.iex + i + W); ld4(e.ezy, s.iez + i + W); }
       else { zero4(e.exy); zero4(e.ezy); }
     }
     T eyr = T(0), ezr = T(0);   // +x neighbour of lane 31 lies in the next tile
-    if (lane == kLanes - 1 && vin && x0 + kVec < nx) { eyr = s.iey[i + kVec]; ezr = s.iez[i + kVec]; }
+    if (lane == kLanes - 1 && vin && x0 + kVec < s.pitch) { eyr = s.iey[i + kVec]; ezr = s.iez[i + kVec]; }
     // lane 0: the source values that H^{n+1/2} at (z, y, x0 - 1) needs
-    const bool xh = work && lane == 0 && x0 >= 1;
-    T gx = T(0), gy = T(0), gz = T(0), gxz = T(0), gyz = T(0), gxy = T(0), gzy = T(0);
-    T ghy = T(0), ghz = T(0);
-    if (xh) {
+    // (x0 - 1 >= xa - 1 >= 0; z + 1 and y + 1 lie inside the grid)
+    T gx = T(0), gy = T(0), gz = T(0), gxz = T(0), gxy = T(0), ghy = T(0), ghz = T(0);
+    if (work && lane == 0) {
       const long long j = i - 1;
       gx = s.iex[j]; gy = s.iey[j]; gz = s.iez[j];
       ghy = s.ihy[j]; ghz = s.ihz[j];
-      if (z + 1 < nz) { gxz = s.iex[j + P]; gyz = s.iey[j + P]; }
-      if (y + 1 < ny) { gxy = s.iex[j + W]; gzy = s.iez[j + W]; }
+      gxz = s.iex[j + P]; gxy = s.iex[j + W];
     }
     // ---- H^{n+1/2}(z) -----------------------------------------------------
     st4(&sEx[r][so], e.ex);
@@ -105,11 +118,7 @@ k_fused(const __grid_constant__ State<T> s, const int* __restrict__ tp, int toff
     e.eyn = __shfl_down_sync(kFull, e.ey[0], 1);
     e.ezn = __shfl_down_sync(kFull, e.ez[0], 1);
     if (lane == kLanes - 1) { e.eyn = eyr; e.ezn = ezr; }
-    const bool fast = interior(s, z, y, x0, t);
-    if (vin) {
-      if (fast) h_vec_interior(s, e, h.hx, h.hy, h.hz);
-      else h_vec(s, e, z, y, x0, t, work, h.hx, h.hy, h.hz);
-    }
+    h_vec_interior(s, e, h.hx, h.hy, h.hz);
     st4(&sHx[r][so], h.hx);
     st4(&sHz[r][so], h.hz);
     __syncthreads();
@@ -119,22 +128,11 @@ k_fused(const __grid_constant__ State<T> s, const int* __restrict__ tp, int toff
     if (work) {
       ld4(h.hxy, &sHx[r - 1][so]);
       ld4(h.hzy, &sHz[r - 1][so]);
-      if (lane == 0) {
-        T hyl = T(0), hzl = T(0);
-        if (xh) {
-          ENbr<T> en;
-          en.ex0 = gx; en.exz = gxz; en.exy = gxy;
-          en.ey0 = gy; en.eyz = gyz; en.eyx = e.ey[0];
-          en.ez0 = gz; en.ezy = gzy; en.ezx = e.ez[0];
-          T hxl = T(0);
-          hyl = ghy; hzl = ghz;
-          h_cell(s, en, z, y, x0 - 1, t, false, hxl, hyl, hzl);
-        }
-        h.hyp = hyl;
-        h.hzp = hzl;
+      if (lane == 0) {   // Taflove 3.30 for hy, hz at x0 - 1 (an interior cell)
+        h.hyp = M::sub(ghy, M::mul(s.db, M::sub(M::sub(gxz, gx), M::sub(e.ez[0], gz))));
+        h.hzp = M::sub(ghz, M::mul(s.db, M::sub(M::sub(e.ey[0], gy), M::sub(gxy, gx))));
       }
-      if (fast) e_vec_interior(h, ca, cb, e.ex, e.ey, e.ez);
-      else e_vec(s, h, ca, cb, z, y, x0, t, true, e.ex, e.ey, e.ez);
+      e_vec_interior(h, ca, cb, e.ex, e.ey, e.ez);
       st4(s.ohx + i, h.hx); st4(s.ohy + i, h.hy); st4(s.ohz + i, h.hz);
       st4(s.oex + i, e.ex); st4(s.oey + i, e.ey); st4(s.oez + i, e.ez);
     }
@@ -145,48 +143,118 @@ k_fused(const __grid_constant__ State<T> s, const int* __restrict__ tp, int toff
 }
 
 template <class T, int TY>
-void launch_ty(const State<T>& s, const int* tdev, int toff, int zchunk, cudaStream_t st) {
+void launch_interior_ty(const State<T>& s, const InteriorBox& ib, cudaStream_t st) {
   const dim3 blk(kLanes, TY + 1, 1);
-  const dim3 grd((s.nx + kRowCells - 1) / kRowCells, (s.ny + TY - 1) / TY,
-                 (s.nz + zchunk - 1) / zchunk);
-  k_fused<T, TY><<<grd, blk, 0, st>>>(s, tdev, toff, zchunk);
+  const dim3 grd((ib.xb - ib.xa + kRowCells - 1) / kRowCells, (ib.yb - ib.ya + TY - 1) / TY,
+                 ib.chunks);
+  k_fused_interior<T, TY><<<grd, blk, 0, st>>>(s, ib);
+}
+
+void add_box(ShellBoxes& bl, int x0, int x1, int y0, int y1, int z0, int z1) {
+  if (x0 >= x1 || y0 >= y1 || z0 >= z1) return;
+  ShellBox& b = bl.b[bl.n++];
+  b.x0 = x0; b.x1 = x1; b.y0 = y0; b.y1 = y1; b.z0 = z0; b.z1 = z1;
+  b.width = x1 - x0 >= 64 ? kLanes : 8;   // strips narrower than 64 cells: 32-cell tiles
+  b.gx = (x1 - x0 + b.width * kVec - 1) / (b.width * kVec);
+  const int rows = 128 / b.width;
+  b.gy = (y1 - y0 + rows - 1) / rows;
+  b.first = bl.total_blocks;
+  bl.total_blocks += b.gx * b.gy * (z1 - z0);
 }
 
 }  // namespace
 
-// Planes per z chunk when the caller leaves it to the library: enough
-// chunks for about eight waves of two resident blocks per SM on 148 SMs,
-// each chunk at least 16 planes (one recomputed plane per chunk).
-int fused_auto_zchunk(int nx, int ny, int nz, int tile_y) {
-  const long long per_layer = (long long)((nx + kRowCells - 1) / kRowCells) * ((ny + tile_y - 1) / tile_y);
-  const long long want = 8LL * 2 * 148;
-  long long layers = (want + per_layer - 1) / per_layer;
-  layers = std::max(1LL, std::min(layers, (long long)nz / 16));
-  return (int)((nz + layers - 1) / layers);
+bool fused_supported_tile(int tile_x, int tile_y, int elem_bytes) {
+  if (tile_x != kLanes) return false;
+  if (tile_y == 4 || tile_y == 7 || tile_y == 8) return true;
+  return elem_bytes == 4 && (tile_y == 15 || tile_y == 16);
+}
+
+// The interior box keeps every cell and every recomputed halo cell away
+// from the CPML faces (H faces cover q < npml - 1 below and the top npml
+// planes; E faces 1 <= q < npml below), from the domain edges and from the
+// injection plane tfsf_z (and tfsf_z + 1, whose recomputed plane below would
+// be the injection plane).
+FusedPlan make_fused_plan(int nx, int ny, int nz, int npml, int tfsf_z, int tile_y, int zchunk) {
+  FusedPlan p;
+  memset(&p, 0, sizeof(p));
+  const int m = npml;
+  InteriorBox& ib = p.interior;
+  ib.xa = (m + 31) / 32 * 32;
+  ib.xb = (nx - m) / kVec * kVec;
+  ib.ya = m;
+  ib.yb = ny - m;
+  // interior z ranges: [m, nz - m) without tfsf_z, tfsf_z + 1
+  int zr[2][2] = {{0, 0}, {0, 0}}, nzr = 0;
+  const int za = m, zb = nz - m;
+  if (tfsf_z >= za && tfsf_z < zb) {
+    if (tfsf_z > za) { zr[nzr][0] = za; zr[nzr][1] = tfsf_z; ++nzr; }
+    if (tfsf_z + 2 < zb) { zr[nzr][0] = tfsf_z + 2; zr[nzr][1] = zb; ++nzr; }
+  } else if (za < zb) {
+    zr[0][0] = za; zr[0][1] = zb; nzr = 1;
+  }
+  p.has_interior = m >= 1 && ib.xa < ib.xb && ib.ya < ib.yb && nzr > 0;
+  ShellBoxes& bl = p.shell;
+  if (!p.has_interior) {
+    add_box(bl, 0, nx, 0, ny, 0, nz);
+    return p;
+  }
+  int planes = 0;
+  for (int k = 0; k < nzr; ++k) planes += zr[k][1] - zr[k][0];
+  if (zchunk <= 0) {
+    // about eight waves of two resident blocks per SM on 148 SMs, chunks of
+    // at least 16 planes (each recomputes the plane below it)
+    const long long per_layer = (long long)((ib.xb - ib.xa + kRowCells - 1) / kRowCells) *
+                                ((ib.yb - ib.ya + tile_y - 1) / tile_y);
+    long long layers = (8LL * 2 * 148 + per_layer - 1) / per_layer;
+    layers = std::max(1LL, std::min(layers, (long long)planes / 16));
+    zchunk = (int)((planes + layers - 1) / layers);
+  }
+  ib.zchunk = zchunk;
+  ib.nz_ranges = nzr;
+  ib.chunks = 0;
+  for (int k = 0; k < nzr; ++k) {
+    ib.z0[k] = zr[k][0];
+    ib.z1[k] = zr[k][1];
+    const int ch = (zr[k][1] - zr[k][0] + zchunk - 1) / zchunk;
+    if (k == 0) ib.chunks0 = ch;
+    ib.chunks += ch;
+  }
+  // the shell: z planes outside the interior ranges (whole planes), then per
+  // interior range the y strips (whole rows) and the x strips
+  int zc = 0;
+  for (int k = 0; k < nzr; ++k) {
+    add_box(bl, 0, nx, 0, ny, zc, ib.z0[k]);
+    zc = ib.z1[k];
+  }
+  add_box(bl, 0, nx, 0, ny, zc, nz);
+  for (int k = 0; k < nzr; ++k) {
+    add_box(bl, 0, nx, 0, ib.ya, ib.z0[k], ib.z1[k]);
+    add_box(bl, 0, nx, ib.yb, ny, ib.z0[k], ib.z1[k]);
+    add_box(bl, 0, ib.xa, ib.ya, ib.yb, ib.z0[k], ib.z1[k]);
+    add_box(bl, ib.xb, nx, ib.ya, ib.yb, ib.z0[k], ib.z1[k]);
+  }
+  return p;
 }
 
 template <class T>
-bool launch_fused_step(const State<T>& s, const int* tdev, int toff, int tile_x, int tile_y,
-                       int zchunk, cudaStream_t st) {
-  if (tile_x != kLanes) return false;
-  if (zchunk <= 0) zchunk = fused_auto_zchunk(s.nx, s.ny, s.nz, tile_y);
+bool launch_fused_interior(const State<T>& s, const FusedPlan& p, int tile_y, cudaStream_t st) {
+  if (!p.has_interior) return true;
   switch (tile_y) {
-    case 4: launch_ty<T, 4>(s, tdev, toff, zchunk, st); return true;
-    case 7: launch_ty<T, 7>(s, tdev, toff, zchunk, st); return true;
-    case 8: launch_ty<T, 8>(s, tdev, toff, zchunk, st); return true;
+    case 4: launch_interior_ty<T, 4>(s, p.interior, st); return true;
+    case 7: launch_interior_ty<T, 7>(s, p.interior, st); return true;
+    case 8: launch_interior_ty<T, 8>(s, p.interior, st); return true;
   }
-  // taller tiles: float only (their shared memory exceeds the static limit
-  // for double)
   if constexpr (sizeof(T) == 4) {
     switch (tile_y) {
-      case 15: launch_ty<T, 15>(s, tdev, toff, zchunk, st); return true;
-      case 16: launch_ty<T, 16>(s, tdev, toff, zchunk, st); return true;
+      case 15: launch_interior_ty<T, 15>(s, p.interior, st); return true;
+      case 16: launch_interior_ty<T, 16>(s, p.interior, st); return true;
     }
   }
   return false;
 }
 
-template bool launch_fused_step<float>(const State<float>&, const int*, int, int, int, int, cudaStream_t);
-template bool launch_fused_step<double>(const State<double>&, const int*, int, int, int, int, cudaStream_t);
+template bool launch_fused_interior<float>(const State<float>&, const FusedPlan&, int, cudaStream_t);
+template bool launch_fused_interior<double>(const State<double>&, const FusedPlan&, int, cudaStream_t);
 
 }  // namespace fdtd

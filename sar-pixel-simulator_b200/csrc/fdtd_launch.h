@@ -20,15 +20,29 @@ template <class T>
 void launch_eps_sigma(int nx, int ny, int nz, int nz_mat, int pitch, const T* eps,
                       const T* sig, T eps0, T dt, T dx, T* ca, T* cb, cudaStream_t st);
 
-// Fused z-marching step (fdtd_fused.cu). tile_x is the tile width in
-// threads (32: 128 cells), tile_y the rows per tile, zchunk the z planes per
-// block (0: automatic). Returns false when the tile shape is not supported.
-template <class T>
-bool launch_fused_step(const State<T>& s, const int* tdev, int toff, int tile_x,
-                       int tile_y, int zchunk, cudaStream_t st);
+// Fused step (fdtd_fused.cu): the interior box in one z-marching pass, the
+// shell by the split passes over a box list.
+struct FusedPlan {
+  int has_interior;
+  InteriorBox interior;
+  ShellBoxes shell;
+};
 
-// Planes per z chunk that launch_fused_step picks for zchunk == 0.
-int fused_auto_zchunk(int nx, int ny, int nz, int tile_y);
+// Interior box and shell boxes of a grid; zchunk 0 picks the z chunk.
+FusedPlan make_fused_plan(int nx, int ny, int nz, int npml, int tfsf_z, int tile_y, int zchunk);
+
+// Tile shapes the interior kernel is built for: 32 lanes wide, tile_y rows.
+bool fused_supported_tile(int tile_x, int tile_y, int elem_bytes);
+
+// Interior pass: reads the source set, writes the destination set.
+template <class T>
+bool launch_fused_interior(const State<T>& s, const FusedPlan& p, int tile_y, cudaStream_t st);
+
+// Split H pass (h_pass) or E pass over the shell boxes, from the State's
+// source pointers to its destination pointers.
+template <class T>
+void launch_shell_pass(const State<T>& s, const int* tdev, int toff, const ShellBoxes& bl,
+                       bool h_pass, cudaStream_t st);
 
 // Records an error message for fdtd_last_error(); returns code.
 int report_error(int code, const char* msg);

@@ -6,8 +6,10 @@
 // thread wrote it within a pass. It moves 80 B per FP32 cell-update
 // (H pass 36 B, E pass 44 B) against the 56 B minimum of a fused pass.
 // Each thread updates four consecutive x cells with vector loads and
-// stores; interior cells take the plain curl update, the rest (CPML faces,
-// domain edges, the injection plane) the per-cell h_cell / e_cell.
+// stores; interior vectors take the plain curl update, the rest (CPML
+// faces, domain edges, the injection plane) h_vec / e_vec. The same passes,
+// restricted to a list of boxes and run source -> destination, update the
+// shell of the fused step (fdtd_fused.cu).
 #include "fdtd_launch.h"
 #include "fdtd_vec.cuh"
 
@@ -15,122 +17,124 @@ namespace fdtd {
 
 __global__ void k_advance(int* t, int n) { *t += n; }
 
-// H pass: H^{n+1/2} = H^{n-1/2} - Db curl E^n, CPML and E-field injection,
-// in place (reads E only, writes the thread's own H and psi_H).
-// Block (32, 4): a warp covers 128 consecutive x cells of one row.
+// H pass on one vector: H^{n+1/2} = H^{n-1/2} - Db curl E^n, CPML and
+// E-field injection. Reads E and H from the source pointers and writes H
+// (and psi_H) to the destination pointers, so it serves both the in-place
+// step (source == destination) and the ping-pong shell of the fused step.
+// `lane` is the thread's position in a row segment of `width` lanes
+// (width * kVec consecutive x cells); every lane of the segment calls this
+// (the +x neighbour comes by shuffle), and only lanes with `act` update
+// and store their vector.
 template <class T>
-__global__ void __launch_bounds__(128) k_h_split(State<T> s, const int* __restrict__ tp, int toff) {
-  using M = R<T>;
-  const int lane = threadIdx.x;
-  const int x0 = (blockIdx.x * 32 + lane) * kVec;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int z = blockIdx.z;
-  const int t = *tp + toff;
+__device__ __forceinline__ void h_split_vec(const State<T>& s, int t, int z, int y, int x0,
+                                            int lane, int width, bool act) {
   const bool vin = x0 < s.pitch && y < s.ny;          // vector inside the row storage
   const long long P = s.plane, W = s.pitch;
   const long long i = (long long)z * P + (long long)y * W + x0;
-  T ex[kVec], ey[kVec], ez[kVec], exy[kVec], ezy[kVec], exz[kVec], eyz[kVec];
+  EVec<T> e;
   T hx[kVec], hy[kVec], hz[kVec];
   if (vin) {
-    ld4(ex, s.iex + i); ld4(ey, s.iey + i); ld4(ez, s.iez + i);
+    ld4(e.ex, s.iex + i); ld4(e.ey, s.iey + i); ld4(e.ez, s.iez + i);
     ld4(hx, s.ihx + i); ld4(hy, s.ihy + i); ld4(hz, s.ihz + i);
   } else {
-    zero4(ex); zero4(ey); zero4(ez); zero4(hx); zero4(hy); zero4(hz);
+    zero4(e.ex); zero4(e.ey); zero4(e.ez); zero4(hx); zero4(hy); zero4(hz);
   }
-  if (vin && y + 1 < s.ny) { ld4(exy, s.iex + i + W); ld4(ezy, s.iez + i + W); }
-  else { zero4(exy); zero4(ezy); }
-  if (vin && z + 1 < s.nz) { ld4(exz, s.iex + i + P); ld4(eyz, s.iey + i + P); }
-  else { zero4(exz); zero4(eyz); }
+  if (vin && y + 1 < s.ny) { ld4(e.exy, s.iex + i + W); ld4(e.ezy, s.iez + i + W); }
+  else { zero4(e.exy); zero4(e.ezy); }
+  if (vin && z + 1 < s.nz) { ld4(e.exz, s.iex + i + P); ld4(e.eyz, s.iey + i + P); }
+  else { zero4(e.exz); zero4(e.eyz); }
   // x+1 neighbour of the last cell: first cell of the next lane's vector
-  T ey_n = __shfl_down_sync(0xffffffffu, ey[0], 1);
-  T ez_n = __shfl_down_sync(0xffffffffu, ez[0], 1);
-  if (lane == 31) {
+  e.eyn = __shfl_down_sync(0xffffffffu, e.ey[0], 1, width);
+  e.ezn = __shfl_down_sync(0xffffffffu, e.ez[0], 1, width);
+  if (lane == width - 1) {
     const bool ok = vin && x0 + kVec < s.nx;
-    ey_n = ok ? s.iey[i + kVec] : T(0);
-    ez_n = ok ? s.iez[i + kVec] : T(0);
+    e.eyn = ok ? s.iey[i + kVec] : T(0);
+    e.ezn = ok ? s.iez[i + kVec] : T(0);
   }
-  if (!vin) return;
-  if (interior(s, z, y, x0, t)) {
-#pragma unroll
-    for (int j = 0; j < kVec; ++j) {
-      const T eyx = j + 1 < kVec ? ey[j + 1 < kVec ? j + 1 : j] : ey_n;
-      const T ezx = j + 1 < kVec ? ez[j + 1 < kVec ? j + 1 : j] : ez_n;
-      hx[j] = M::sub(hx[j], M::mul(s.db, M::sub(M::sub(ezy[j], ez[j]), M::sub(eyz[j], ey[j]))));
-      hy[j] = M::sub(hy[j], M::mul(s.db, M::sub(M::sub(exz[j], ex[j]), M::sub(ezx, ez[j]))));
-      hz[j] = M::sub(hz[j], M::mul(s.db, M::sub(M::sub(eyx, ey[j]), M::sub(exy[j], ex[j]))));
-    }
-  } else {
-#pragma unroll
-    for (int j = 0; j < kVec; ++j) {
-      const int x = x0 + j;
-      if (x >= s.nx) continue;
-      ENbr<T> e;
-      e.ex0 = ex[j]; e.exz = exz[j]; e.exy = exy[j];
-      e.ey0 = ey[j]; e.eyz = eyz[j]; e.eyx = j + 1 < kVec ? ey[j + 1 < kVec ? j + 1 : j] : ey_n;
-      e.ez0 = ez[j]; e.ezy = ezy[j]; e.ezx = j + 1 < kVec ? ez[j + 1 < kVec ? j + 1 : j] : ez_n;
-      h_cell(s, e, z, y, x, t, true, hx[j], hy[j], hz[j]);
-    }
-  }
+  if (!(act && vin)) return;
+  if (interior(s, z, y, x0, t)) h_vec_interior(s, e, hx, hy, hz);
+  else h_vec(s, e, z, y, x0, t, true, hx, hy, hz);
   st4(s.ohx + i, hx); st4(s.ohy + i, hy); st4(s.ohz + i, hz);
 }
 
-// E pass: E^{n+1} = Ca E^n + Cb curl H^{n+1/2}, CPML and H-field injection,
-// in place (reads H only, writes the thread's own E and psi_E).
+// E pass on one vector: E^{n+1} = Ca E^n + Cb curl H^{n+1/2}, CPML and
+// H-field injection. Reads H^{n+1/2} and E^n from the source pointers and
+// writes E (and psi_E) to the destination pointers.
 template <class T>
-__global__ void __launch_bounds__(128) k_e_split(State<T> s, const int* __restrict__ tp, int toff) {
-  using M = R<T>;
-  const int lane = threadIdx.x;
-  const int x0 = (blockIdx.x * 32 + lane) * kVec;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int z = blockIdx.z;
-  const int t = *tp + toff;
+__device__ __forceinline__ void e_split_vec(const State<T>& s, int t, int z, int y, int x0,
+                                            int lane, int width, bool act) {
   const bool vin = x0 < s.pitch && y < s.ny;
   const long long P = s.plane, W = s.pitch;
   const long long i = (long long)z * P + (long long)y * W + x0;
-  T hx[kVec], hy[kVec], hz[kVec], hxy[kVec], hzy[kVec], hxz[kVec], hyz[kVec];
+  HVec<T> h;
   T ex[kVec], ey[kVec], ez[kVec], ca[kVec], cb[kVec];
   if (vin) {
-    ld4(hx, s.ihx + i); ld4(hy, s.ihy + i); ld4(hz, s.ihz + i);
+    ld4(h.hx, s.ihx + i); ld4(h.hy, s.ihy + i); ld4(h.hz, s.ihz + i);
     ld4(ex, s.iex + i); ld4(ey, s.iey + i); ld4(ez, s.iez + i);
     ld4(ca, s.ca + i); ld4(cb, s.cb + i);
   } else {
-    zero4(hx); zero4(hy); zero4(hz); zero4(ex); zero4(ey); zero4(ez); zero4(ca); zero4(cb);
+    zero4(h.hx); zero4(h.hy); zero4(h.hz); zero4(ex); zero4(ey); zero4(ez); zero4(ca); zero4(cb);
   }
-  if (vin && y >= 1) { ld4(hxy, s.ihx + i - W); ld4(hzy, s.ihz + i - W); }
-  else { zero4(hxy); zero4(hzy); }
-  if (vin && z >= 1) { ld4(hxz, s.ihx + i - P); ld4(hyz, s.ihy + i - P); }
-  else { zero4(hxz); zero4(hyz); }
+  if (vin && y >= 1) { ld4(h.hxy, s.ihx + i - W); ld4(h.hzy, s.ihz + i - W); }
+  else { zero4(h.hxy); zero4(h.hzy); }
+  if (vin && z >= 1) { ld4(h.hxz, s.ihx + i - P); ld4(h.hyz, s.ihy + i - P); }
+  else { zero4(h.hxz); zero4(h.hyz); }
   // x-1 neighbour of the first cell: last cell of the previous lane's vector
-  T hy_p = __shfl_up_sync(0xffffffffu, hy[kVec - 1], 1);
-  T hz_p = __shfl_up_sync(0xffffffffu, hz[kVec - 1], 1);
+  h.hyp = __shfl_up_sync(0xffffffffu, h.hy[kVec - 1], 1, width);
+  h.hzp = __shfl_up_sync(0xffffffffu, h.hz[kVec - 1], 1, width);
   if (lane == 0) {
     const bool ok = vin && x0 >= 1;
-    hy_p = ok ? s.ihy[i - 1] : T(0);
-    hz_p = ok ? s.ihz[i - 1] : T(0);
+    h.hyp = ok ? s.ihy[i - 1] : T(0);
+    h.hzp = ok ? s.ihz[i - 1] : T(0);
   }
-  if (!vin) return;
-  if (interior(s, z, y, x0, t)) {
-#pragma unroll
-    for (int j = 0; j < kVec; ++j) {
-      const T hyx = j > 0 ? hy[j > 0 ? j - 1 : 0] : hy_p;
-      const T hzx = j > 0 ? hz[j > 0 ? j - 1 : 0] : hz_p;
-      ex[j] = M::add(M::mul(ex[j], ca[j]), M::mul(cb[j], M::sub(M::sub(hz[j], hzy[j]), M::sub(hy[j], hyz[j]))));
-      ey[j] = M::add(M::mul(ey[j], ca[j]), M::mul(cb[j], M::sub(M::sub(hx[j], hxz[j]), M::sub(hz[j], hzx))));
-      ez[j] = M::add(M::mul(ez[j], ca[j]), M::mul(cb[j], M::sub(M::sub(hy[j], hyx), M::sub(hx[j], hxy[j]))));
-    }
-  } else {
-#pragma unroll
-    for (int j = 0; j < kVec; ++j) {
-      const int x = x0 + j;
-      if (x >= s.nx) continue;
-      HNbr<T> h;
-      h.hx0 = hx[j]; h.hxz = hxz[j]; h.hxy = hxy[j];
-      h.hy0 = hy[j]; h.hyz = hyz[j]; h.hyx = j > 0 ? hy[j > 0 ? j - 1 : 0] : hy_p;
-      h.hz0 = hz[j]; h.hzy = hzy[j]; h.hzx = j > 0 ? hz[j > 0 ? j - 1 : 0] : hz_p;
-      e_cell(s, h, ca[j], cb[j], z, y, x, t, true, ex[j], ey[j], ez[j]);
-    }
-  }
+  if (!(act && vin)) return;
+  if (interior(s, z, y, x0, t)) e_vec_interior(h, ca, cb, ex, ey, ez);
+  else e_vec(s, h, ca, cb, z, y, x0, t, true, ex, ey, ez);
   st4(s.oex + i, ex); st4(s.oey + i, ey); st4(s.oez + i, ez);
+}
+
+// In-place split step over the whole grid. Block (32, 4): a warp covers
+// 128 consecutive x cells of one row; blockIdx.z is the plane.
+template <class T>
+__global__ void __launch_bounds__(128) k_h_split(State<T> s, const int* __restrict__ tp, int toff) {
+  const int x0 = (blockIdx.x * 32 + threadIdx.x) * kVec;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  h_split_vec(s, *tp + toff, (int)blockIdx.z, y, x0, (int)threadIdx.x, 32, true);
+}
+
+template <class T>
+__global__ void __launch_bounds__(128) k_e_split(State<T> s, const int* __restrict__ tp, int toff) {
+  const int x0 = (blockIdx.x * 32 + threadIdx.x) * kVec;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  e_split_vec(s, *tp + toff, (int)blockIdx.z, y, x0, (int)threadIdx.x, 32, true);
+}
+
+// The same passes over a list of boxes (the shell of the fused step), one
+// plane of one box tile per 128-thread block. A box tile is `width` lanes
+// (width * kVec x cells) by 128 / width rows.
+__device__ __forceinline__ const ShellBox& find_box(const ShellBoxes& bl, int bid) {
+  int k = 0;
+  while (k + 1 < bl.n && bid >= bl.b[k + 1].first) ++k;
+  return bl.b[k];
+}
+
+template <class T, bool kH>
+__global__ void __launch_bounds__(128) k_shell(State<T> s, const int* __restrict__ tp, int toff,
+                                               ShellBoxes bl) {
+  const int bid = blockIdx.x;
+  const ShellBox& b = find_box(bl, bid);
+  int local = bid - b.first;
+  const int bx = local % b.gx;
+  local /= b.gx;
+  const int by = local % b.gy;
+  const int bz = local / b.gy;
+  const int lane = threadIdx.x % b.width, row = threadIdx.x / b.width;
+  const int x0 = b.x0 + (bx * b.width + lane) * kVec;
+  const int y = b.y0 + by * (128 / b.width) + row;
+  const int z = b.z0 + bz;
+  const bool act = x0 < b.x1 && y < b.y1;
+  if (kH) h_split_vec(s, *tp + toff, z, y, x0, lane, b.width, act);
+  else e_split_vec(s, *tp + toff, z, y, x0, lane, b.width, act);
 }
 
 // ---------------------------------------------------------------------------
@@ -267,6 +271,14 @@ void launch_phasors(const State<T>& s, const int* tdev, int toff, cudaStream_t s
   k_phasors<T><<<grd, 256, 0, st>>>(s, tdev, toff);
 }
 
+template <class T>
+void launch_shell_pass(const State<T>& s, const int* tdev, int toff, const ShellBoxes& bl,
+                       bool h_pass, cudaStream_t st) {
+  if (bl.n == 0 || bl.total_blocks == 0) return;
+  if (h_pass) k_shell<T, true><<<bl.total_blocks, 128, 0, st>>>(s, tdev, toff, bl);
+  else k_shell<T, false><<<bl.total_blocks, 128, 0, st>>>(s, tdev, toff, bl);
+}
+
 void launch_advance(int* tdev, int n, cudaStream_t st) {
   k_advance<<<1, 1, 0, st>>>(tdev, n);
 }
@@ -280,6 +292,10 @@ void launch_eps_sigma(int nx, int ny, int nz, int nz_mat, int pitch, const T* ep
 
 template void launch_split_step<float>(const State<float>&, const int*, int, cudaStream_t);
 template void launch_split_step<double>(const State<double>&, const int*, int, cudaStream_t);
+template void launch_shell_pass<float>(const State<float>&, const int*, int, const ShellBoxes&,
+                                       bool, cudaStream_t);
+template void launch_shell_pass<double>(const State<double>&, const int*, int, const ShellBoxes&,
+                                        bool, cudaStream_t);
 template void launch_phasors<float>(const State<float>&, const int*, int, cudaStream_t);
 template void launch_phasors<double>(const State<double>&, const int*, int, cudaStream_t);
 template void launch_eps_sigma<float>(int, int, int, int, int, const float*, const float*, float,

@@ -32,6 +32,9 @@ WIDE = [
     (261, 45, 30, 14, 24, 16, 'float32'),
     (150, 61, 37, 20, 20, 20, 'float32'),
     (140, 33, 26, 12, 16, 10, 'float64'),
+    # injection plane at the lower / upper end of the fused interior z range
+    (300, 70, 40, 10, 12, 8, 'float32'),
+    (173, 53, 40, 28, 12, 8, 'float32'),
 ]
 
 
