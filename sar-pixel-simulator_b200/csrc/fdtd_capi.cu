@@ -77,6 +77,10 @@ struct fdtd_sim {
   int cur = 0;
   cudaStream_t own = nullptr;
   cudaStream_t stream = nullptr;
+  // second stream of the fused step: the shell H pass runs beside the
+  // interior pass (fork and join by events)
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
   bool have_abs = false, have_mat = false;
   std::vector<unsigned char> prof;       // 8 * npml values of the element type
   int kernel = FDTD_KERNEL_SPLIT;
@@ -200,8 +204,12 @@ int enqueue_steps(fdtd_sim* s, int n) {
       // interior and shell H pass read the source set only; the shell E
       // pass reads the destination H that both of them wrote
       State<T> st = make_state<T>(s, s->cur, nxt);
+      CK(cudaEventRecord(s->fork, s->stream));
+      CK(cudaStreamWaitEvent(s->side, s->fork, 0));
+      launch_shell_pass<T>(st, s->tdev, k, s->plan.shell, true, s->side);
       launch_fused_interior<T>(st, s->plan, s->tile_y, s->stream);
-      launch_shell_pass<T>(st, s->tdev, k, s->plan.shell, true, s->stream);
+      CK(cudaEventRecord(s->join, s->side));
+      CK(cudaStreamWaitEvent(s->stream, s->join, 0));
       State<T> se = st;
       se.ihx = (const T*)s->fld[nxt][3]; se.ihy = (const T*)s->fld[nxt][4]; se.ihz = (const T*)s->fld[nxt][5];
       launch_shell_pass<T>(se, s->tdev, k, s->plan.shell, false, s->stream);
@@ -365,6 +373,12 @@ int fdtd_create(const fdtd_geometry* geom, int device, fdtd_sim** out) {
     return fail(FDTD_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
   }
   s->stream = s->own;
+  if ((e = cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking)) != cudaSuccess ||
+      (e = cudaEventCreateWithFlags(&s->fork, cudaEventDisableTiming)) != cudaSuccess ||
+      (e = cudaEventCreateWithFlags(&s->join, cudaEventDisableTiming)) != cudaSuccess) {
+    fdtd_destroy(s);
+    return fail(FDTD_ERR_CUDA, "stream/event creation: %s", cudaGetErrorString(e));
+  }
   rc = fdtd_reset(s);
   if (rc != FDTD_OK) {
     fdtd_destroy(s);
@@ -379,7 +393,11 @@ int fdtd_destroy(fdtd_sim* s) {
   cudaSetDevice(s->device);
   if (s->own) cudaStreamSynchronize(s->own);
   for (auto& b : s->bufs) cudaFree(b.p);
+  if (s->side) cudaStreamSynchronize(s->side);
   for (auto e : s->ev) cudaEventDestroy(e);
+  if (s->fork) cudaEventDestroy(s->fork);
+  if (s->join) cudaEventDestroy(s->join);
+  if (s->side) cudaStreamDestroy(s->side);
   if (s->own) cudaStreamDestroy(s->own);
   delete s;
   cudaGetLastError();

@@ -7,7 +7,10 @@ measured entry it falls back to the built-in default; the autotuner in
 from . import _native
 
 
+DEFAULT_TILE = (32, 4)
+
+
 def choose(geom, kernel=None, tile=None):
-    k = _native.FDTD_KERNEL_SPLIT if kernel is None else int(kernel)
-    tx, ty = tile if tile is not None else (32, 8)
+    k = _native.FDTD_KERNEL_FUSED if kernel is None else int(kernel)
+    tx, ty = tile if tile is not None else DEFAULT_TILE
     return {'kernel': k, 'tile_x': int(tx), 'tile_y': int(ty)}
