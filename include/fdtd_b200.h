@@ -201,6 +201,15 @@ int fdtd_near2far(const void *ex_u, const void *ey_u, const void *hx_u,
                   int ntheta, const double *phis_deg, int nphi, double freq,
                   int device, double *out);
 
+/* Diagnostic (no counterpart in the reference): the CPML terms divide by
+ * the cell size with a correctly rounded reciprocal and one FMA correction
+ * (Markstein's method) instead of an IEEE division. This runs both on the
+ * device for every float bit pattern (FDTD_F32: 2^32 inputs) or for 2^30
+ * sampled doubles (FDTD_F64) with divisor `cell_size` rounded to the type,
+ * and returns how many inputs gave a result that differs in any bit. */
+int fdtd_check_cell_division(int dtype, double cell_size, int device, int64_t *tested,
+                             int64_t *mismatches);
+
 /* fdtd_near2far without any device allocation. This entry point has no
  * counterpart in the reference; it exists for callers that cannot call
  * cudaMalloc when they need a far field: code whose device memory is owned

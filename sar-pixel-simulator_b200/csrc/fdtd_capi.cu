@@ -125,6 +125,7 @@ State<T> make_state(const fdtd_sim* s, int src, int dst) {
   st.plane = s->plane;
   st.db = (T)g.db; st.dtm0 = (T)g.dtm0; st.dte0dx = (T)g.dte0dx;
   st.dx = (T)g.cell_size;
+  st.rdx = (T)1 / st.dx;   // IEEE division on the host: correctly rounded
   const T* pr = reinterpret_cast<const T*>(s->prof.data());
   if (!s->prof.empty())
     for (int k = 0; k < 8; ++k)

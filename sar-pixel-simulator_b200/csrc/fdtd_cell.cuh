@@ -73,8 +73,8 @@ __device__ __forceinline__ void h_cell(const State<T>& s, const ENbr<T>& e,
         const T b = s.prof[side ? BH_U : BH_D][q];
         const T c = s.prof[side ? CH_U : CH_D][q];
         const long long k = ((long long)q * ny + y) * s.pitch + x;
-        const T pyz = M::add(M::mul(b, s.ps.z[side][3][k]), M::div(M::mul(c, dex_z), s.dx));
-        const T pxz = M::add(M::mul(b, s.ps.z[side][2][k]), M::div(M::mul(c, dey_z), s.dx));
+        const T pyz = M::add(M::mul(b, s.ps.z[side][3][k]), div_dx(s, M::mul(c, dex_z)));
+        const T pxz = M::add(M::mul(b, s.ps.z[side][2][k]), div_dx(s, M::mul(c, dey_z)));
         if (wpsi) { s.pd.z[side][3][k] = pyz; s.pd.z[side][2][k] = pxz; }
         hy = M::sub(hy, M::mul(s.dtm0, pyz));
         hx = M::add(hx, M::mul(s.dtm0, pxz));
@@ -89,8 +89,8 @@ __device__ __forceinline__ void h_cell(const State<T>& s, const ENbr<T>& e,
         const T b = s.prof[side ? BH_U : BH_D][q];
         const T c = s.prof[side ? CH_U : CH_D][q];
         const long long k = ((long long)z * ny + y) * m + q;
-        const T pzx = M::add(M::mul(b, s.ps.x[side][3][k]), M::div(M::mul(c, dey_x), s.dx));
-        const T pyx = M::add(M::mul(b, s.ps.x[side][2][k]), M::div(M::mul(c, dez_x), s.dx));
+        const T pzx = M::add(M::mul(b, s.ps.x[side][3][k]), div_dx(s, M::mul(c, dey_x)));
+        const T pyx = M::add(M::mul(b, s.ps.x[side][2][k]), div_dx(s, M::mul(c, dez_x)));
         if (wpsi) { s.pd.x[side][3][k] = pzx; s.pd.x[side][2][k] = pyx; }
         hz = M::sub(hz, M::mul(s.dtm0, pzx));
         hy = M::add(hy, M::mul(s.dtm0, pyx));
@@ -105,8 +105,8 @@ __device__ __forceinline__ void h_cell(const State<T>& s, const ENbr<T>& e,
         const T b = s.prof[side ? BH_U : BH_D][q];
         const T c = s.prof[side ? CH_U : CH_D][q];
         const long long k = ((long long)z * m + q) * s.pitch + x;
-        const T pxy = M::add(M::mul(b, s.ps.y[side][2][k]), M::div(M::mul(c, dez_y), s.dx));
-        const T pzy = M::add(M::mul(b, s.ps.y[side][3][k]), M::div(M::mul(c, dex_y), s.dx));
+        const T pxy = M::add(M::mul(b, s.ps.y[side][2][k]), div_dx(s, M::mul(c, dez_y)));
+        const T pzy = M::add(M::mul(b, s.ps.y[side][3][k]), div_dx(s, M::mul(c, dex_y)));
         if (wpsi) { s.pd.y[side][2][k] = pxy; s.pd.y[side][3][k] = pzy; }
         hx = M::sub(hx, M::mul(s.dtm0, pxy));
         hz = M::add(hz, M::mul(s.dtm0, pzy));
@@ -150,8 +150,8 @@ __device__ __forceinline__ void e_cell(const State<T>& s, const HNbr<T>& h,
         const T b = s.prof[side ? BE_U : BE_D][q];
         const T c = s.prof[side ? CE_U : CE_D][q];
         const long long k = ((long long)q * ny + y) * s.pitch + x;
-        const T pyz = M::add(M::mul(b, s.ps.z[side][1][k]), M::div(M::mul(c, dhx_z), s.dx));
-        const T pxz = M::add(M::mul(b, s.ps.z[side][0][k]), M::div(M::mul(c, dhy_z), s.dx));
+        const T pyz = M::add(M::mul(b, s.ps.z[side][1][k]), div_dx(s, M::mul(c, dhx_z)));
+        const T pxz = M::add(M::mul(b, s.ps.z[side][0][k]), div_dx(s, M::mul(c, dhy_z)));
         if (wpsi) { s.pd.z[side][1][k] = pyz; s.pd.z[side][0][k] = pxz; }
         ey = M::add(ey, M::mul(cbdx, pyz));
         ex = M::sub(ex, M::mul(cbdx, pxz));
@@ -166,8 +166,8 @@ __device__ __forceinline__ void e_cell(const State<T>& s, const HNbr<T>& h,
         const T b = s.prof[side ? BE_U : BE_D][q];
         const T c = s.prof[side ? CE_U : CE_D][q];
         const long long k = ((long long)z * ny + y) * m + q;
-        const T pzx = M::add(M::mul(b, s.ps.x[side][1][k]), M::div(M::mul(c, dhy_x), s.dx));
-        const T pyx = M::add(M::mul(b, s.ps.x[side][0][k]), M::div(M::mul(c, dhz_x), s.dx));
+        const T pzx = M::add(M::mul(b, s.ps.x[side][1][k]), div_dx(s, M::mul(c, dhy_x)));
+        const T pyx = M::add(M::mul(b, s.ps.x[side][0][k]), div_dx(s, M::mul(c, dhz_x)));
         if (wpsi) { s.pd.x[side][1][k] = pzx; s.pd.x[side][0][k] = pyx; }
         ez = M::add(ez, M::mul(cbdx, pzx));
         ey = M::sub(ey, M::mul(cbdx, pyx));
@@ -182,8 +182,8 @@ __device__ __forceinline__ void e_cell(const State<T>& s, const HNbr<T>& h,
         const T b = s.prof[side ? BE_U : BE_D][q];
         const T c = s.prof[side ? CE_U : CE_D][q];
         const long long k = ((long long)z * m + q) * s.pitch + x;
-        const T pxy = M::add(M::mul(b, s.ps.y[side][0][k]), M::div(M::mul(c, dhz_y), s.dx));
-        const T pzy = M::add(M::mul(b, s.ps.y[side][1][k]), M::div(M::mul(c, dhx_y), s.dx));
+        const T pxy = M::add(M::mul(b, s.ps.y[side][0][k]), div_dx(s, M::mul(c, dhz_y)));
+        const T pzy = M::add(M::mul(b, s.ps.y[side][1][k]), div_dx(s, M::mul(c, dhx_y)));
         if (wpsi) { s.pd.y[side][0][k] = pxy; s.pd.y[side][1][k] = pzy; }
         ex = M::add(ex, M::mul(cbdx, pxy));
         ez = M::sub(ez, M::mul(cbdx, pzy));

@@ -15,6 +15,7 @@ constexpr int kMaxPml = 32;
 
 template <class T> struct R;
 template <> struct R<float> {
+  static __device__ __forceinline__ float fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
   static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
   static __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
   static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
@@ -22,6 +23,7 @@ template <> struct R<float> {
   static __device__ __forceinline__ float from_double(double a) { return __double2float_rn(a); }
 };
 template <> struct R<double> {
+  static __device__ __forceinline__ double fma(double a, double b, double c) { return __fma_rn(a, b, c); }
   static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
   static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
   static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
@@ -55,6 +57,7 @@ struct State {
   int pitch;
   long long plane;   // ny * pitch
   T db, dtm0, dte0dx, dx;
+  T rdx;   // 1 / dx correctly rounded (host IEEE division)
   T prof[8][kMaxPml];
   // field sets: src is read, dst is written (the same set for the in-place
   // split kernels; ping-pong sets for the fused kernel)
@@ -101,6 +104,32 @@ struct InteriorBox {
   int zchunk;
   int chunks0, chunks;   // chunks of the first range, of both ranges
 };
+
+// Correctly rounded u / d for d > 0, given r = RN(1/d): Markstein's FMA
+// correction (P. W. Markstein, "Computation of elementary functions on the
+// IBM RISC System/6000 processor", IBM J. Res. Develop. 34(1), 1990). With
+// r within half an ulp of 1/d and q0 = RN(u r) within one ulp of u/d, the
+// remainder u - d q0 is exact in one FMA and RN(q0 + r (u - d q0)) is the
+// correctly rounded quotient, as long as no step leaves the normal range.
+// |u| outside [2^-100, 2^100] (float; [2^-900, 2^900] double) takes the
+// IEEE division instead. Used for the CPML terms (c * dE) / dx, whose
+// divisor is the constant cell size.
+template <class T>
+__device__ __forceinline__ T div_const(T u, T d, T r) {
+  using M = R<T>;
+  const T lo = sizeof(T) == 4 ? T(7.8886090522101181e-31) : T(1.4708983551653345e-271);   // 2^-100, 2^-900
+  const T hi = sizeof(T) == 4 ? T(1.2676506002282294e+30) : T(6.7986211919640936e+270);   // 2^100, 2^900
+  const T a = u < T(0) ? -u : u;
+  if (a >= lo && a <= hi) {
+    const T q0 = M::mul(u, r);
+    const T rem = M::fma(-q0, d, u);
+    return M::fma(rem, r, q0);
+  }
+  return a == T(0) ? u : M::div(u, d);   // zeros keep their sign; tiny, huge, NaN: IEEE
+}
+
+template <class T>
+__device__ __forceinline__ T div_dx(const State<T>& s, T u) { return div_const(u, s.dx, s.rdx); }
 
 __global__ void k_advance(int* t, int n);
 

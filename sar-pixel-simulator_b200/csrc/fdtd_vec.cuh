@@ -156,8 +156,8 @@ __device__ __forceinline__ void h_vec(const State<T>& s, const EVec<T>& e, int z
 #pragma unroll
     for (int j = 0; j < kVec; ++j) {
       if (!inb[j]) continue;
-      p3[j] = M::add(M::mul(b, p3[j]), M::div(M::mul(c, dex_z[j]), s.dx));   // psi_Hyz
-      p2[j] = M::add(M::mul(b, p2[j]), M::div(M::mul(c, dey_z[j]), s.dx));   // psi_Hxz
+      p3[j] = M::add(M::mul(b, p3[j]), div_dx(s, M::mul(c, dex_z[j])));   // psi_Hyz
+      p2[j] = M::add(M::mul(b, p2[j]), div_dx(s, M::mul(c, dey_z[j])));   // psi_Hxz
       hy[j] = M::sub(hy[j], M::mul(s.dtm0, p3[j]));
       hx[j] = M::add(hx[j], M::mul(s.dtm0, p2[j]));
     }
@@ -174,8 +174,8 @@ __device__ __forceinline__ void h_vec(const State<T>& s, const EVec<T>& e, int z
       const T b = s.prof[side ? BH_U : BH_D][q];
       const T c = s.prof[side ? CH_U : CH_D][q];
       const long long k = ((long long)z * ny + y) * m + q;
-      const T pzx = M::add(M::mul(b, s.ps.x[side][3][k]), M::div(M::mul(c, dey_x[j]), s.dx));
-      const T pyx = M::add(M::mul(b, s.ps.x[side][2][k]), M::div(M::mul(c, dez_x[j]), s.dx));
+      const T pzx = M::add(M::mul(b, s.ps.x[side][3][k]), div_dx(s, M::mul(c, dey_x[j])));
+      const T pyx = M::add(M::mul(b, s.ps.x[side][2][k]), div_dx(s, M::mul(c, dez_x[j])));
       if (wpsi) { s.pd.x[side][3][k] = pzx; s.pd.x[side][2][k] = pyx; }
       hz[j] = M::sub(hz[j], M::mul(s.dtm0, pzx));
       hy[j] = M::add(hy[j], M::mul(s.dtm0, pyx));
@@ -194,8 +194,8 @@ __device__ __forceinline__ void h_vec(const State<T>& s, const EVec<T>& e, int z
 #pragma unroll
     for (int j = 0; j < kVec; ++j) {
       if (!inb[j]) continue;
-      p2[j] = M::add(M::mul(b, p2[j]), M::div(M::mul(c, dez_y[j]), s.dx));   // psi_Hxy
-      p3[j] = M::add(M::mul(b, p3[j]), M::div(M::mul(c, dex_y[j]), s.dx));   // psi_Hzy
+      p2[j] = M::add(M::mul(b, p2[j]), div_dx(s, M::mul(c, dez_y[j])));   // psi_Hxy
+      p3[j] = M::add(M::mul(b, p3[j]), div_dx(s, M::mul(c, dex_y[j])));   // psi_Hzy
       hx[j] = M::sub(hx[j], M::mul(s.dtm0, p2[j]));
       hz[j] = M::add(hz[j], M::mul(s.dtm0, p3[j]));
     }
@@ -260,8 +260,8 @@ __device__ __forceinline__ void e_vec(const State<T>& s, const HVec<T>& h, const
 #pragma unroll
     for (int j = 0; j < kVec; ++j) {
       if (!inb[j]) continue;
-      p1[j] = M::add(M::mul(b, p1[j]), M::div(M::mul(c, dhx_z[j]), s.dx));   // psi_Eyz
-      p0[j] = M::add(M::mul(b, p0[j]), M::div(M::mul(c, dhy_z[j]), s.dx));   // psi_Exz
+      p1[j] = M::add(M::mul(b, p1[j]), div_dx(s, M::mul(c, dhx_z[j])));   // psi_Eyz
+      p0[j] = M::add(M::mul(b, p0[j]), div_dx(s, M::mul(c, dhy_z[j])));   // psi_Exz
       ey[j] = M::add(ey[j], M::mul(cbdx[j], p1[j]));
       ex[j] = M::sub(ex[j], M::mul(cbdx[j], p0[j]));
     }
@@ -278,8 +278,8 @@ __device__ __forceinline__ void e_vec(const State<T>& s, const HVec<T>& h, const
       const T b = s.prof[side ? BE_U : BE_D][q];
       const T c = s.prof[side ? CE_U : CE_D][q];
       const long long k = ((long long)z * ny + y) * m + q;
-      const T pzx = M::add(M::mul(b, s.ps.x[side][1][k]), M::div(M::mul(c, dhy_x[j]), s.dx));
-      const T pyx = M::add(M::mul(b, s.ps.x[side][0][k]), M::div(M::mul(c, dhz_x[j]), s.dx));
+      const T pzx = M::add(M::mul(b, s.ps.x[side][1][k]), div_dx(s, M::mul(c, dhy_x[j])));
+      const T pyx = M::add(M::mul(b, s.ps.x[side][0][k]), div_dx(s, M::mul(c, dhz_x[j])));
       if (wpsi) { s.pd.x[side][1][k] = pzx; s.pd.x[side][0][k] = pyx; }
       ez[j] = M::add(ez[j], M::mul(cbdx[j], pzx));
       ey[j] = M::sub(ey[j], M::mul(cbdx[j], pyx));
@@ -298,8 +298,8 @@ __device__ __forceinline__ void e_vec(const State<T>& s, const HVec<T>& h, const
 #pragma unroll
     for (int j = 0; j < kVec; ++j) {
       if (!inb[j]) continue;
-      p0[j] = M::add(M::mul(b, p0[j]), M::div(M::mul(c, dhz_y[j]), s.dx));   // psi_Exy
-      p1[j] = M::add(M::mul(b, p1[j]), M::div(M::mul(c, dhx_y[j]), s.dx));   // psi_Ezy
+      p0[j] = M::add(M::mul(b, p0[j]), div_dx(s, M::mul(c, dhz_y[j])));   // psi_Exy
+      p1[j] = M::add(M::mul(b, p1[j]), div_dx(s, M::mul(c, dhx_y[j])));   // psi_Ezy
       ex[j] = M::add(ex[j], M::mul(cbdx[j], p0[j]));
       ez[j] = M::sub(ez[j], M::mul(cbdx[j], p1[j]));
     }

@@ -101,6 +101,8 @@ SIGNATURES = {
     'fdtd_get_field': [_P, _I, _P],
     'fdtd_set_field': [_P, _I, _P],
     'fdtd_near2far': [_P, _P, _P, _P, _I, _I, _I, _I, _D, _D, _P, _I, _P, _I, _D, _I, _P],
+    'fdtd_check_cell_division': [_I, _D, _I, ctypes.POINTER(ctypes.c_int64),
+                                 ctypes.POINTER(ctypes.c_int64)],
     'fdtd_near2far_noalloc': [_P, _P, _P, _P, _I, _I, _I, _I, _D, _D, _P, _I, _P, _I, _D, _I, _P],
 }
 
@@ -304,3 +306,12 @@ def near2far(ex_u, ey_u, hx_u, hy_u, nx, ny, nz, dx, r, thetas_deg, phis_deg, fr
                             float(dx), float(r), ptr(th), int(th.size), ptr(ph), int(ph.size),
                             float(freq), int(device), ptr(out)))
     return {'E_theta': out[0], 'E_phi': out[1], 'H_theta': out[2], 'H_phi': out[3]}
+
+
+def check_cell_division(dtype, cell_size, device=0):
+    """(tested, mismatches): the library's division by the cell size
+    against IEEE division on the device (fdtd_check_cell_division)."""
+    tested, bad = ctypes.c_int64(0), ctypes.c_int64(0)
+    check(lib.fdtd_check_cell_division(dtype_code(dtype), float(cell_size), int(device),
+                                       ctypes.byref(tested), ctypes.byref(bad)))
+    return tested.value, bad.value
