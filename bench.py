@@ -256,7 +256,9 @@ def run_ours(a):
         dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
     ms_max = float(ms_t.item())
     value = world * cells * a.steps / (ms_max / 1e3) / 1e6
-    launches_per_step = 3 if choice['kernel'] == _native.FDTD_KERNEL_SPLIT else 2
+    # split: H pass, E pass, phasors; fused: interior pass, shell H pass,
+    # shell E pass, phasors; plus one step-counter advance per run call
+    launches_per_step = 3 if choice['kernel'] == _native.FDTD_KERNEL_SPLIT else 4
     gpu_launches = launches_per_step * a.steps + 1
 
     # live per-kernel timing for the roofline (separate pass, same state)
