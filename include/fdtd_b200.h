@@ -201,6 +201,28 @@ int fdtd_near2far(const void *ex_u, const void *ey_u, const void *hx_u,
                   int ntheta, const double *phis_deg, int nphi, double freq,
                   int device, double *out);
 
+/* ---- batched sweep --------------------------------------------------------
+ * Several simulations (uneven grids, one device, one element type) advanced
+ * together: every time step runs the H pass, the E pass and the phasor pass
+ * of all members in one launch each, and chunks of steps are replayed from
+ * a captured CUDA graph. It replaces the loop over material models in
+ * run_experiment (experiment.py:61-84), where each model is a separate
+ * MainSimGpu.run (gpu/main_sim.py:74-115) and a separate time loop.
+ * The members stay ordinary handles: set their absorbers, materials and
+ * incident planes, run the batch, then read each member's phasors and
+ * fields as usual. Members must outlive the batch; a member's own calls are
+ * ordered after the batch's work. Each member advances nsteps from its own
+ * step index, using its current field set in place (the split step). */
+typedef struct fdtd_batch fdtd_batch;
+
+int fdtd_batch_create(fdtd_sim *const *sims, int n, fdtd_batch **out);
+int fdtd_batch_destroy(fdtd_batch *b);
+/* FDTD_OPT_GRAPH_CHUNK: steps per captured graph (0: no graph; default 64). */
+int fdtd_batch_set_option(fdtd_batch *b, int option, int value);
+int fdtd_batch_run(fdtd_batch *b, int nsteps);
+int fdtd_batch_synchronize(fdtd_batch *b);
+int fdtd_batch_get_stream(fdtd_batch *b, void **stream);
+
 /* Diagnostic (no counterpart in the reference): the CPML terms divide by
  * the cell size with a correctly rounded reciprocal and one FMA correction
  * (Markstein's method) instead of an IEEE division. This runs both on the

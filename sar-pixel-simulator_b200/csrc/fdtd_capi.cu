@@ -3,7 +3,9 @@
 // Owns all device memory of a simulation handle, builds the by-value kernel
 // state, and schedules the per-step kernels. Errors are reported as status
 // codes plus a per-thread message; nothing throws across the boundary.
+#include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -97,6 +99,26 @@ struct fdtd_sim {
   int ev_used = 0;
   double acc_ms[2] = {0, 0};
   int acc_n[2] = {0, 0};
+};
+
+// A batched sweep over member simulations (fdtd_batch_*). The members keep
+// their own device memory; the batch holds a device table of their States
+// and launches one kernel per phase for all of them.
+struct fdtd_batch {
+  std::vector<fdtd_sim*> sims;
+  int device = 0;
+  int dtype = FDTD_F32;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev = nullptr;
+  void* d_models = nullptr;   // BatchModel<T>[n]
+  int* d_start = nullptr;     // first step-kernel block of each model, n + 1 entries
+  int* d_start_ph = nullptr;  // first phasor block of each model, n + 1 entries
+  int blocks = 0, blocks_ph = 0;
+  std::vector<int> sig;       // each member's current field set when the table was built
+  bool table_ok = false;
+  int graph_chunk = 64;
+  cudaGraphExec_t gexec = nullptr;
+  int gexec_chunk = 0;
 };
 
 namespace {
@@ -754,3 +776,194 @@ extern "C" int fdtd_near2far(const void* ex_u, const void* ey_u, const void* hx_
     rc = fail(FDTD_ERR_CUDA, "near2far: %s", cudaGetErrorString(e));
   return rc;
 }
+
+// ---------------------------------------------------------------------------
+// batched sweep
+// ---------------------------------------------------------------------------
+namespace {
+
+template <class T>
+int batch_build_table(fdtd_batch* b) {
+  const int n = (int)b->sims.size();
+  std::vector<BatchModel<T>> tab(n);
+  std::vector<int> start(n + 1), start_ph(n + 1);
+  long long blk = 0, blk_ph = 0;
+  for (int m = 0; m < n; ++m) {
+    fdtd_sim* s = b->sims[m];
+    BatchModel<T>& bm = tab[m];
+    memset(&bm, 0, sizeof(bm));
+    bm.s = make_state<T>(s, s->cur, s->cur);
+    bm.tdev = s->tdev;
+    bm.gx = (s->g.nx + 127) / 128;
+    bm.gy = (s->g.ny + 3) / 4;
+    bm.ph_n = std::max(s->ny_ph * s->nx_ph, std::max(s->nz_ph * s->ny_ph, s->nz_ph * s->nx_ph));
+    start[m] = (int)blk;
+    start_ph[m] = (int)blk_ph;
+    blk += (long long)bm.gx * bm.gy * s->g.nz;
+    blk_ph += 6LL * ((bm.ph_n + 255) / 256);
+    if (blk > INT32_MAX || blk_ph > INT32_MAX) return fail(FDTD_ERR_INVALID, "batch too large");
+  }
+  start[n] = (int)blk;
+  start_ph[n] = (int)blk_ph;
+  CK(cudaMemcpy(b->d_models, tab.data(), sizeof(BatchModel<T>) * n, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(b->d_start, start.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(b->d_start_ph, start_ph.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
+  b->blocks = (int)blk;
+  b->blocks_ph = (int)blk_ph;
+  b->sig.resize(n);
+  for (int m = 0; m < n; ++m) b->sig[m] = b->sims[m]->cur;
+  b->table_ok = true;
+  if (b->gexec) { cudaGraphExecDestroy(b->gexec); b->gexec = nullptr; }
+  return FDTD_OK;
+}
+
+template <class T>
+void batch_enqueue(fdtd_batch* b, int nsteps) {
+  const int n = (int)b->sims.size();
+  const auto* bm = static_cast<const BatchModel<T>*>(b->d_models);
+  for (int k = 0; k < nsteps; ++k)
+    launch_batch_step<T>(bm, b->d_start, n, b->blocks, b->d_start_ph, b->blocks_ph, k, b->stream);
+  launch_batch_advance<T>(bm, n, nsteps, b->stream);
+}
+
+template <class T>
+int batch_run(fdtd_batch* b, int nsteps) {
+  bool stale = !b->table_ok;
+  for (size_t m = 0; m < b->sims.size(); ++m) stale = stale || b->sig[m] != b->sims[m]->cur;
+  if (stale) {
+    int rc = batch_build_table<T>(b);
+    if (rc) return rc;
+  }
+  // order after the members' own work
+  for (fdtd_sim* s : b->sims) {
+    CK(cudaEventRecord(b->ev, s->stream));
+    CK(cudaStreamWaitEvent(b->stream, b->ev, 0));
+  }
+  int left = nsteps;
+  const int chunk = b->graph_chunk;
+  if (chunk > 0 && left >= chunk) {
+    if (!b->gexec || b->gexec_chunk != chunk) {
+      if (b->gexec) { cudaGraphExecDestroy(b->gexec); b->gexec = nullptr; }
+      cudaGraph_t g = nullptr;
+      CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+      batch_enqueue<T>(b, chunk);
+      cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+      if (e != cudaSuccess) return fail(FDTD_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+      e = cudaGraphInstantiate(&b->gexec, g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) {
+        b->gexec = nullptr;
+        return fail(FDTD_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+      }
+      b->gexec_chunk = chunk;
+    }
+    while (left >= chunk) {
+      CK(cudaGraphLaunch(b->gexec, b->stream));
+      left -= chunk;
+    }
+  }
+  if (left > 0) batch_enqueue<T>(b, left);
+  CK(cudaGetLastError());
+  // members' later calls are ordered after the batch
+  CK(cudaEventRecord(b->ev, b->stream));
+  for (fdtd_sim* s : b->sims) {
+    CK(cudaStreamWaitEvent(s->stream, b->ev, 0));
+    s->t += nsteps;
+  }
+  return FDTD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fdtd_batch_create(fdtd_sim* const* sims, int n, fdtd_batch** out) {
+  if (!out) return fail(FDTD_ERR_INVALID, "null output handle");
+  *out = nullptr;
+  if (!sims || n < 1) return fail(FDTD_ERR_INVALID, "a batch needs at least one simulation");
+  for (int i = 0; i < n; ++i) {
+    if (!sims[i]) return fail(FDTD_ERR_INVALID, "null simulation %d", i);
+    if (sims[i]->device != sims[0]->device)
+      return fail(FDTD_ERR_INVALID, "simulation %d is on another device", i);
+    if (sims[i]->g.dtype != sims[0]->g.dtype)
+      return fail(FDTD_ERR_INVALID, "simulation %d has another element type", i);
+    for (int j = 0; j < i; ++j)
+      if (sims[j] == sims[i]) return fail(FDTD_ERR_INVALID, "simulation %d appears twice", i);
+  }
+  fdtd_batch* b = new fdtd_batch();
+  b->sims.assign(sims, sims + n);
+  b->device = sims[0]->device;
+  b->dtype = sims[0]->g.dtype;
+  cudaError_t e = cudaSetDevice(b->device);
+  const size_t msz = b->dtype == FDTD_F32 ? sizeof(BatchModel<float>) : sizeof(BatchModel<double>);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_models, msz * n);
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_start, sizeof(int) * (n + 1));
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_start_ph, sizeof(int) * (n + 1));
+  if (e != cudaSuccess) {
+    fdtd_batch_destroy(b);
+    cudaGetLastError();
+    return fail(FDTD_ERR_CUDA, "batch set-up: %s", cudaGetErrorString(e));
+  }
+  *out = b;
+  return FDTD_OK;
+}
+
+int fdtd_batch_destroy(fdtd_batch* b) {
+  if (!b) return FDTD_OK;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->gexec) cudaGraphExecDestroy(b->gexec);
+  if (b->d_models) cudaFree(b->d_models);
+  if (b->d_start) cudaFree(b->d_start);
+  if (b->d_start_ph) cudaFree(b->d_start_ph);
+  if (b->ev) cudaEventDestroy(b->ev);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+  cudaGetLastError();
+  return FDTD_OK;
+}
+
+int fdtd_batch_set_option(fdtd_batch* b, int option, int value) {
+  if (!b) return fail(FDTD_ERR_INVALID, "null batch handle");
+  if (option != FDTD_OPT_GRAPH_CHUNK) return fail(FDTD_ERR_INVALID, "unknown batch option %d", option);
+  if (value < 0) return fail(FDTD_ERR_INVALID, "bad graph chunk %d", value);
+  b->graph_chunk = value;
+  return FDTD_OK;
+}
+
+int fdtd_batch_run(fdtd_batch* b, int nsteps) {
+  if (!b) return fail(FDTD_ERR_INVALID, "null batch handle");
+  if (nsteps < 0) return fail(FDTD_ERR_INVALID, "negative step count");
+  for (size_t m = 0; m < b->sims.size(); ++m) {
+    fdtd_sim* s = b->sims[m];
+    if (!s->have_abs) return fail(FDTD_ERR_STATE, "member %zu: absorbers not set", m);
+    if (!s->have_mat) return fail(FDTD_ERR_STATE, "member %zu: materials not set", m);
+    if (s->t + nsteps > s->g.nt)
+      return fail(FDTD_ERR_INVALID, "member %zu: step %lld + %d exceeds size_t %d", m,
+                  (long long)s->t, nsteps, s->g.nt);
+    if (s->g.nt_inc > 0 && s->t < s->g.nt_inc && s->inc_nt < s->g.nt_inc)
+      return fail(FDTD_ERR_STATE, "member %zu: incident beam not set", m);
+  }
+  if (nsteps == 0) return FDTD_OK;
+  cudaError_t e = cudaSetDevice(b->device);
+  if (e != cudaSuccess) return fail(FDTD_ERR_CUDA, "cudaSetDevice: %s", cudaGetErrorString(e));
+  return b->dtype == FDTD_F32 ? batch_run<float>(b, nsteps) : batch_run<double>(b, nsteps);
+}
+
+int fdtd_batch_synchronize(fdtd_batch* b) {
+  if (!b) return fail(FDTD_ERR_INVALID, "null batch handle");
+  CK(cudaSetDevice(b->device));
+  CK(cudaStreamSynchronize(b->stream));
+  CK(cudaGetLastError());
+  return FDTD_OK;
+}
+
+int fdtd_batch_get_stream(fdtd_batch* b, void** stream) {
+  if (!b || !stream) return fail(FDTD_ERR_INVALID, "null argument");
+  *stream = (void*)b->stream;
+  return FDTD_OK;
+}
+
+}  // extern "C"

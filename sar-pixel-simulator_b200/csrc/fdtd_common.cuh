@@ -78,6 +78,17 @@ struct State {
   int kahan;
 };
 
+// One member of a batched sweep: its State (current field set, in place),
+// its step counter, and its tiling (gx x gy tiles of 128 x 4 cells per
+// plane; ph_n cells in its largest phasor plane).
+template <class T>
+struct BatchModel {
+  State<T> s;
+  int* tdev;
+  int gx, gy;
+  int ph_n;
+};
+
 // A box of the fused step's shell, swept by the split passes one plane per
 // block row: [x0, x1) x [y0, y1) x [z0, z1), x0 a multiple of 4. A tile is
 // `width` lanes (width * 4 x cells) by 128 / width rows; gx, gy tiles per

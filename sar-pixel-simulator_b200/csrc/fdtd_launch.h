@@ -16,6 +16,15 @@ void launch_phasors(const State<T>& s, const int* tdev, int toff, cudaStream_t s
 
 void launch_advance(int* tdev, int n, cudaStream_t st);
 
+// Batched sweep (fdtd_split.cu): one step of every model (H pass, E pass,
+// phasors, one launch each); `start` / `start_ph` hold each model's first
+// block (n + 1 entries, the last one the total). Then the step counters.
+template <class T>
+void launch_batch_step(const BatchModel<T>* bm, const int* start, int n, int blocks,
+                       const int* start_ph, int blocks_ph, int toff, cudaStream_t st);
+template <class T>
+void launch_batch_advance(const BatchModel<T>* bm, int n, int steps, cudaStream_t st);
+
 template <class T>
 void launch_eps_sigma(int nx, int ny, int nz, int nz_mat, int pitch, const T* eps,
                       const T* sig, T eps0, T dt, T dx, T* ca, T* cb, cudaStream_t st);

@@ -172,21 +172,18 @@ __device__ __forceinline__ double mean4(T a, T b, T c, T d) {
   return 0.25 * (double)M::add(M::add(M::add(a, b), c), d);
 }
 
-// One thread per phasor cell; blockIdx.y selects the plane pair member
-// 0 d, 1 u (z planes), 2 l, 3 r (x planes), 4 f, 5 b (y planes).
+// One phasor cell: plane group g = 0 d, 1 u (z planes), 2 l, 3 r (x
+// planes), 4 f, 5 b (y planes); idx runs over the group's plane.
 template <class T>
-__global__ void __launch_bounds__(256) k_phasors(State<T> s, const int* __restrict__ tp, int toff) {
-  const int g = blockIdx.y;
+__device__ __forceinline__ void phasor_cell(const State<T>& s, int g, int idx, int t) {
   const int m = s.npml;
   int d0, d1;
   if (g < 2) { d0 = s.ny_ph; d1 = s.nx_ph; }
   else if (g < 4) { d0 = s.nz_ph; d1 = s.ny_ph; }
   else { d0 = s.nz_ph; d1 = s.nx_ph; }
-  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= d0 * d1) return;
   const int a = idx / d1, b = idx - a * d1;
   if (a == 0 || b == 0) return;
-  const int t = *tp + toff;
   const double* ph = s.phase + 4 * (long long)t;
   const double cE = ph[0], sE = ph[1], cH = ph[2], sH = ph[3];
   const T* ex = s.oex; const T* ey = s.oey; const T* ez = s.oez;
@@ -218,6 +215,66 @@ __global__ void __launch_bounds__(256) k_phasors(State<T> s, const int* __restri
     ph_acc(s, base + 2, k, mean4(hx[i], hx[i - W], hx[i - P], hx[i - P - W]), cH, sH);
     ph_acc(s, base + 3, k, mean4(hz[i], hz[i - W], hz[i - 1], hz[i - W - 1]), cH, sH);
   }
+}
+
+// One thread per phasor cell; blockIdx.y selects the plane group.
+template <class T>
+__global__ void __launch_bounds__(256) k_phasors(State<T> s, const int* __restrict__ tp, int toff) {
+  phasor_cell(s, (int)blockIdx.y, (int)(blockIdx.x * blockDim.x + threadIdx.x), *tp + toff);
+}
+
+// ---------------------------------------------------------------------------
+// batched step: the split passes and the phasor pass of many simulations in
+// one launch each. Block b belongs to the model m with
+// start[m] <= b < start[m + 1]; the model's State lives in device memory.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int find_model(const int* __restrict__ start, int n, int bid) {
+  int lo = 0, hi = n - 1;   // last m with start[m] <= bid
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (start[mid] <= bid) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+template <class T, bool kH>
+__global__ void __launch_bounds__(128) k_batch_split(const BatchModel<T>* __restrict__ bm,
+                                                     const int* __restrict__ start, int n, int toff) {
+  const int bid = blockIdx.x;
+  const int mi = find_model(start, n, bid);
+  const BatchModel<T>& b = bm[mi];
+  int local = bid - start[mi];
+  const int bx = local % b.gx;
+  local /= b.gx;
+  const int by = local % b.gy;
+  const int z = local / b.gy;
+  const int lane = threadIdx.x & 31, row = threadIdx.x >> 5;
+  const int x0 = (bx * 32 + lane) * kVec;
+  const int y = by * 4 + row;
+  const int t = *b.tdev + toff;
+  if (kH) h_split_vec(b.s, t, z, y, x0, lane, 32, true);
+  else e_split_vec(b.s, t, z, y, x0, lane, 32, true);
+}
+
+template <class T>
+__global__ void __launch_bounds__(256) k_batch_phasors(const BatchModel<T>* __restrict__ bm,
+                                                       const int* __restrict__ start, int n,
+                                                       int toff) {
+  const int bid = blockIdx.x;
+  const int mi = find_model(start, n, bid);
+  const BatchModel<T>& b = bm[mi];
+  const int local = bid - start[mi];
+  const int per_group = (b.ph_n + 255) / 256;
+  const int g = local / per_group;
+  const int idx = (local - g * per_group) * 256 + threadIdx.x;
+  phasor_cell(b.s, g, idx, *b.tdev + toff);
+}
+
+template <class T>
+__global__ void k_batch_advance(const BatchModel<T>* __restrict__ bm, int n, int steps) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) *bm[i].tdev += steps;
 }
 
 // ---------------------------------------------------------------------------
@@ -272,6 +329,19 @@ void launch_phasors(const State<T>& s, const int* tdev, int toff, cudaStream_t s
 }
 
 template <class T>
+void launch_batch_step(const BatchModel<T>* bm, const int* start, int n, int blocks,
+                       const int* start_ph, int blocks_ph, int toff, cudaStream_t st) {
+  k_batch_split<T, true><<<blocks, 128, 0, st>>>(bm, start, n, toff);
+  k_batch_split<T, false><<<blocks, 128, 0, st>>>(bm, start, n, toff);
+  k_batch_phasors<T><<<blocks_ph, 256, 0, st>>>(bm, start_ph, n, toff);
+}
+
+template <class T>
+void launch_batch_advance(const BatchModel<T>* bm, int n, int steps, cudaStream_t st) {
+  k_batch_advance<T><<<(n + 127) / 128, 128, 0, st>>>(bm, n, steps);
+}
+
+template <class T>
 void launch_shell_pass(const State<T>& s, const int* tdev, int toff, const ShellBoxes& bl,
                        bool h_pass, cudaStream_t st) {
   if (bl.n == 0 || bl.total_blocks == 0) return;
@@ -296,6 +366,12 @@ template void launch_shell_pass<float>(const State<float>&, const int*, int, con
                                        bool, cudaStream_t);
 template void launch_shell_pass<double>(const State<double>&, const int*, int, const ShellBoxes&,
                                         bool, cudaStream_t);
+template void launch_batch_step<float>(const BatchModel<float>*, const int*, int, int, const int*,
+                                       int, int, cudaStream_t);
+template void launch_batch_step<double>(const BatchModel<double>*, const int*, int, int,
+                                        const int*, int, int, cudaStream_t);
+template void launch_batch_advance<float>(const BatchModel<float>*, int, int, cudaStream_t);
+template void launch_batch_advance<double>(const BatchModel<double>*, int, int, cudaStream_t);
 template void launch_phasors<float>(const State<float>&, const int*, int, cudaStream_t);
 template void launch_phasors<double>(const State<double>&, const int*, int, cudaStream_t);
 template void launch_eps_sigma<float>(int, int, int, int, int, const float*, const float*, float,

@@ -101,6 +101,12 @@ SIGNATURES = {
     'fdtd_get_field': [_P, _I, _P],
     'fdtd_set_field': [_P, _I, _P],
     'fdtd_near2far': [_P, _P, _P, _P, _I, _I, _I, _I, _D, _D, _P, _I, _P, _I, _D, _I, _P],
+    'fdtd_batch_create': [ctypes.POINTER(_P), _I, ctypes.POINTER(_P)],
+    'fdtd_batch_destroy': [_P],
+    'fdtd_batch_set_option': [_P, _I, _I],
+    'fdtd_batch_run': [_P, _I],
+    'fdtd_batch_synchronize': [_P],
+    'fdtd_batch_get_stream': [_P, ctypes.POINTER(_P)],
     'fdtd_check_cell_division': [_I, _D, _I, ctypes.POINTER(ctypes.c_int64),
                                  ctypes.POINTER(ctypes.c_int64)],
     'fdtd_near2far_noalloc': [_P, _P, _P, _P, _I, _I, _I, _I, _D, _D, _P, _I, _P, _I, _D, _I, _P],
@@ -315,3 +321,42 @@ def check_cell_division(dtype, cell_size, device=0):
     check(lib.fdtd_check_cell_division(dtype_code(dtype), float(cell_size), int(device),
                                        ctypes.byref(tested), ctypes.byref(bad)))
     return tested.value, bad.value
+
+
+class Batch:
+    """Several NativeSim members advanced together (fdtd_batch_*): one launch
+    per pass for all members each step, chunks of steps replayed from a
+    captured CUDA graph. Members keep their own state and readback calls."""
+
+    def __init__(self, sims, graph_chunk=None):
+        self.sims = list(sims)   # keeps the members alive while the batch exists
+        arr = (_P * len(self.sims))(*[s.h for s in self.sims])
+        self.h = _P()
+        check(lib.fdtd_batch_create(arr, len(self.sims), ctypes.byref(self.h)))
+        if graph_chunk is not None:
+            self.set_graph_chunk(graph_chunk)
+
+    def set_graph_chunk(self, steps):
+        check(lib.fdtd_batch_set_option(self.h, OPT_GRAPH_CHUNK, int(steps)))
+
+    def run(self, nsteps):
+        check(lib.fdtd_batch_run(self.h, int(nsteps)))
+
+    def synchronize(self):
+        check(lib.fdtd_batch_synchronize(self.h))
+
+    def stream(self):
+        p = _P()
+        check(lib.fdtd_batch_get_stream(self.h, ctypes.byref(p)))
+        return p.value or 0
+
+    def close(self):
+        if self.h:
+            lib.fdtd_batch_destroy(self.h)
+            self.h = _P()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,106 @@
+"""Batched sweep (fdtd_batch_*): members of uneven sizes advanced together,
+one launch per pass for all members, chunks replayed from a captured CUDA
+graph. Each member must end with the oracle's fields and phasors bit for
+bit, however the run is cut into calls and graph chunks."""
+import numpy as np
+import pytest
+
+from fdtdsarsim_b200 import _native
+from helpers import bits_equal, make_params, native_for, oracle_for, random_problem
+
+pytestmark = pytest.mark.gpu
+
+MODELS = [
+    # nx, ny, nz, tfsf_z, nt, ntp
+    (27, 25, 23, 14, 30, 20),
+    (41, 37, 29, 16, 30, 30),
+    (35, 31, 27, 20, 30, 12),     # injection plane inside the upper CPML
+    (150, 61, 37, 20, 30, 25),
+]
+
+
+def _members(models, seed, dtype='float32'):
+    out = []
+    for k, (nx, ny, nz, tfsf, nt, ntp) in enumerate(models):
+        pc = make_params(nx, ny, nz, tfsf, nt, ntp, dtype=dtype)
+        _, _, ca, cb, inc = random_problem(pc, seed + k)
+        orc = oracle_for(pc)
+        orc.run(ca, cb, inc, nt)
+        sim = native_for(pc)
+        sim.set_materials(ca, cb)
+        sim.set_incident(inc['ex'], inc['ey'], inc['hx'], inc['hy'])
+        out.append((orc, sim))
+    return out
+
+
+def _assert_member(orc, sim):
+    for c in _native.FIELD_NAMES:
+        assert bits_equal(sim.get_field(c), getattr(orc, c)), c
+    for k, name in enumerate(_native.PHASOR_NAMES):
+        assert bits_equal(sim.get_phasor(k), orc.ph[name]), name
+
+
+@pytest.mark.parametrize('chunk,calls', [(0, (30,)), (7, (30,)), (4, (3, 10, 17)), (64, (1, 29))])
+def test_batch_matches_oracle_for_every_member(chunk, calls):
+    members = _members(MODELS, seed=500)
+    batch = _native.Batch([s for _, s in members], graph_chunk=chunk)
+    for n in calls:
+        batch.run(n)
+    batch.synchronize()
+    for orc, sim in members:
+        assert sim.step_index() == 30
+        _assert_member(orc, sim)
+    batch.close()
+    for _, sim in members:
+        sim.close()
+
+
+def test_batch_float64_members():
+    members = _members(MODELS[:2], seed=520, dtype='float64')
+    batch = _native.Batch([s for _, s in members], graph_chunk=8)
+    batch.run(30)
+    for orc, sim in members:
+        _assert_member(orc, sim)
+    batch.close()
+
+
+def test_members_mix_own_steps_and_batch_steps():
+    """A member that ran fused steps on its own (its current field set
+    changed) joins the batch afterwards; the batch rebuilds its table."""
+    members = _members(MODELS, seed=540)
+    sims = [s for _, s in members]
+    sims[1].set_option(_native.OPT_KERNEL, _native.FDTD_KERNEL_FUSED)
+    sims[1].run(3)
+    sims[3].set_option(_native.OPT_KERNEL, _native.FDTD_KERNEL_FUSED)
+    sims[3].run(3)
+    batch = _native.Batch(sims, graph_chunk=5)
+    with pytest.raises(_native.FdtdError):
+        batch.run(28)   # members 1 and 3 would pass size_t
+    for s in (0, 2):
+        sims[s].run(3)
+    batch.run(20)
+    sims[1].run(7)
+    batch.run(0)
+    for s in (0, 2, 3):
+        sims[s].run(7)
+    for orc, sim in members:
+        assert sim.step_index() == 30
+        _assert_member(orc, sim)
+    batch.close()
+
+
+def test_batch_rejects_bad_members():
+    pc32 = make_params(27, 25, 23, 14, 10, 5)
+    pc64 = make_params(27, 25, 23, 14, 10, 5, dtype='float64')
+    a, b = native_for(pc32), native_for(pc64)
+    with pytest.raises(_native.FdtdError):
+        _native.Batch([a, b])
+    with pytest.raises(_native.FdtdError):
+        _native.Batch([a, a])
+    with pytest.raises(_native.FdtdError):
+        _native.Batch([])
+    batch = _native.Batch([a])
+    with pytest.raises(_native.FdtdError) as ei:
+        batch.run(1)   # materials not set
+    assert ei.value.code == _native.FDTD_ERR_STATE
+    batch.close()
