@@ -39,7 +39,9 @@ def parse():
     ap.add_argument('--steps', type=int, default=200)
     ap.add_argument('--warmup', type=int, default=5)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
-    ap.add_argument('--workload', default='plain_16x16', choices=['plain_16x16', 'plain_8x8'])
+    ap.add_argument('--workload', default='plain_16x16',
+                    choices=['plain_16x16', 'plain_8x8', 'batch64'])
+    ap.add_argument('--models', type=int, default=64, help='batch64: number of models')
     ap.add_argument('--kernel', default='auto', choices=['auto', 'split', 'fused'])
     ap.add_argument('--tile-y', type=int, default=None, help='fused kernel rows per tile')
     ap.add_argument('--zchunk', type=int, default=0, help='fused kernel z planes per block (0: auto)')
@@ -371,10 +373,131 @@ def run_reference(a):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# batched sweep: 64 uneven vegetation models, batched vs one after another
+# ---------------------------------------------------------------------------
+def batch_models(n, nsteps_inc, seed=4040, dtype='float32'):
+    """n seeded models of the batched configuration: x-y uniform in 2..8
+    wavelengths, depth 0.5..2 wavelengths, cell 0.03 wavelength, HH and VV
+    alternating, dielectric cylinders over flat soil. The material fraction
+    grows with the depth (0.4 at 0.5 wl, 0.7 from 1.25 wl) so that the
+    injection plane stays below the upper phasor plane."""
+    from fdtdsarsim_b200 import synthetic
+    from fdtdsarsim_b200.materials import compute_material_arrays
+    from fdtdsarsim_b200.parameters import set_geom_params
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        sx, sy = rng.uniform(2.0, 8.0, size=2)
+        depth = rng.uniform(0.5, 2.0)
+        mf = float(min(0.7, 0.4 + 0.4 * (depth - 0.5)))
+        pol = 'HH' if k % 2 == 0 else 'VV'
+        pc = synthetic.base_params(dtype, pol=pol, mf=mf, illum=sx)
+        set_geom_params(pc, sx, sy, depth, pc.geom_params.simulation_duration, 0.03, 'wavelength')
+        g = pc.geom_params
+        model = synthetic.vegetation_model(pc, rng, name=f'veg{k:02d}')
+        ca, cb = compute_material_arrays(pc, model)
+        g.size_t_inc = min(g.size_t_inc, nsteps_inc)
+        inc = {}
+        for comp, scale in (('ex', 1.0), ('ey', 1.0), ('hx', 1 / 376.73), ('hy', 1 / 376.73)):
+            inc[comp] = (scale * rng.standard_normal((g.size_t_inc, g.size_y, g.size_x))).astype(dtype)
+        out.append((pc, ca, cb, inc))
+    return out
+
+
+def run_batch(a):
+    import torch
+    torch.cuda.set_device(0)
+    from fdtdsarsim_b200 import _native, tuning
+    from fdtdsarsim_b200.absorbers import packed_profiles
+    from fdtdsarsim_b200.gpu.main_sim import native_geometry
+
+    models = batch_models(a.models, a.warmup + a.steps + 1, dtype=a.dtype)
+    cells = [pc.geom_params.size_x * pc.geom_params.size_y * pc.geom_params.size_z
+             for pc, _, _, _ in models]
+    total = int(sum(cells))
+    sims = []
+    for pc, ca, cb, inc in models:
+        geom = native_geometry(pc)
+        sim = _native.NativeSim(geom, 0)
+        sim.set_absorbers(packed_profiles(pc))
+        choice = tuning.choose(geom)
+        sim.set_option(_native.OPT_KERNEL, choice['kernel'])
+        sim.set_option(_native.OPT_TILE_X, choice['tile_x'])
+        sim.set_option(_native.OPT_TILE_Y, choice['tile_y'])
+        sim.set_materials(ca, cb)
+        sim.set_incident(inc['ex'], inc['ey'], inc['hx'], inc['hy'])
+        sims.append(sim)
+
+    def timed(stream, fn):
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    # batched: every member each step, one launch per pass, graph chunks
+    batch = _native.Batch(sims)
+    bstream = torch.cuda.ExternalStream(batch.stream())
+    batch.run(a.warmup)
+    batch.synchronize()
+    clocks = ClockSampler(0)
+    clocks.start()
+    ms_b = timed(bstream, lambda: batch.run(a.steps))
+    clk = clocks.stop()
+    batch.close()
+
+    # one after another: each model's own time loop (its default kernel), on
+    # one stream so the solves do not overlap
+    for s in sims:
+        s.reset()
+    seq = torch.cuda.Stream()
+    for s in sims:
+        s.set_stream(seq.cuda_stream)
+        s.run(a.warmup)
+    ms_s = timed(seq, lambda: [s.run(a.steps) for s in sims])
+    for s in sims:
+        s.close()
+
+    value = total * a.steps / (ms_b / 1e3) / 1e6
+    seq_value = total * a.steps / (ms_s / 1e3) / 1e6
+    peak, peak_kind = measured_peak_hbm()
+    achieved = total * BYTES_PER_CELL[a.dtype] * a.steps / (ms_b / 1e3) / 1e9
+    nx = [pc.geom_params.size_x for pc, _, _, _ in models]
+    nz = [pc.geom_params.size_z for pc, _, _, _ in models]
+    line = {
+        'metric': 'Mcell-updates/s', 'value': round(value, 1), 'unit': 'Mcell-updates/s',
+        'n_gpus': 1, 'steps': a.steps, 'warmup': a.warmup, 'ms_per_step': round(ms_b / a.steps, 4),
+        'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
+        'dtype': 'f32' if a.dtype == 'float32' else 'f64',
+        'data': 'synthetic (seeded vegetation models and incident planes of the named shapes)',
+        'config': {'workload': f'batch{a.models}: {a.models} vegetation models, x-y 2-8 wl, depth '
+                               f'0.5-2 wl, cell 0.03 wl, HH/VV, 5.4 GHz',
+                   'models': a.models, 'cells_total': total,
+                   'nx_range': [int(min(nx)), int(max(nx))], 'nz_range': [int(min(nz)), int(max(nz))],
+                   'l2': 'inputs larger than L2 (fields of all models)',
+                   'batched': 'split step of every model per launch, 64-step graph chunks'},
+        'sequential': {'value': round(seq_value, 1), 'ms_per_step': round(ms_s / a.steps, 4),
+                       'kernel': 'each model alone, its default kernel, one shared stream'},
+        'speedup_vs_sequential': round(ms_s / ms_b, 3),
+        'roofline': {'bound': 'hbm', 'achieved': round(achieved, 1), 'peak': peak, 'unit': 'GB/s',
+                     'frac': round(achieved / peak, 4), 'traffic': None, 'peak_source': peak_kind,
+                     'kernel': 'batch_split_step'},
+        'cpu_baseline': None, 'e2e': None,
+        'gpu_launches': 3 * a.steps + 1 + (a.steps + 63) // 64, 'clocks': clk,
+    }
+    print(json.dumps(line))
+
+
 def main():
     a = parse()
     if a.impl == 'reference':
         run_reference(a)
+    elif a.workload == 'batch64':
+        run_batch(a)
     else:
         run_ours(a)
 

@@ -794,8 +794,16 @@ int batch_build_table(fdtd_batch* b) {
     memset(&bm, 0, sizeof(bm));
     bm.s = make_state<T>(s, s->cur, s->cur);
     bm.tdev = s->tdev;
-    bm.gx = (s->g.nx + 127) / 128;
-    bm.gy = (s->g.ny + 3) / 4;
+    // row width with the least x padding (ties: the wider rows)
+    bm.width = 32;
+    long long best = 1LL << 62;
+    for (int w : {32, 16, 8}) {
+      const long long gx = (s->g.nx + 4 * w - 1) / (4 * w), gy = (s->g.ny + 128 / w - 1) / (128 / w);
+      const long long padded = gx * 4 * w * gy * (128 / w);
+      if (padded < best) { best = padded; bm.width = w; }
+    }
+    bm.gx = (s->g.nx + 4 * bm.width - 1) / (4 * bm.width);
+    bm.gy = (s->g.ny + 128 / bm.width - 1) / (128 / bm.width);
     bm.ph_n = std::max(s->ny_ph * s->nx_ph, std::max(s->nz_ph * s->ny_ph, s->nz_ph * s->nx_ph));
     start[m] = (int)blk;
     start_ph[m] = (int)blk_ph;

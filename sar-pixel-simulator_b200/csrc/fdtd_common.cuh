@@ -79,13 +79,14 @@ struct State {
 };
 
 // One member of a batched sweep: its State (current field set, in place),
-// its step counter, and its tiling (gx x gy tiles of 128 x 4 cells per
-// plane; ph_n cells in its largest phasor plane).
+// its step counter, and its tiling: 128-thread blocks of `width` lanes
+// (width * 4 x cells) by 128 / width rows, gx x gy of them per plane; ph_n
+// cells in its largest phasor plane.
 template <class T>
 struct BatchModel {
   State<T> s;
   int* tdev;
-  int gx, gy;
+  int width, gx, gy;
   int ph_n;
 };
 

@@ -249,12 +249,12 @@ __global__ void __launch_bounds__(128) k_batch_split(const BatchModel<T>* __rest
   local /= b.gx;
   const int by = local % b.gy;
   const int z = local / b.gy;
-  const int lane = threadIdx.x & 31, row = threadIdx.x >> 5;
-  const int x0 = (bx * 32 + lane) * kVec;
-  const int y = by * 4 + row;
+  const int lane = threadIdx.x % b.width, row = threadIdx.x / b.width;
+  const int x0 = (bx * b.width + lane) * kVec;
+  const int y = by * (128 / b.width) + row;
   const int t = *b.tdev + toff;
-  if (kH) h_split_vec(b.s, t, z, y, x0, lane, 32, true);
-  else e_split_vec(b.s, t, z, y, x0, lane, 32, true);
+  if (kH) h_split_vec(b.s, t, z, y, x0, lane, b.width, true);
+  else e_split_vec(b.s, t, z, y, x0, lane, b.width, true);
 }
 
 template <class T>
