@@ -201,6 +201,25 @@ int fdtd_near2far(const void *ex_u, const void *ey_u, const void *hx_u,
                   int ntheta, const double *phis_deg, int nphi, double freq,
                   int device, double *out);
 
+/* ---- gradient ---------------------------------------------------------------
+ * Reverse-mode derivative of an objective J of the four upper-plane phasors
+ * (ex_ph_u, ey_ph_u, hx_ph_u, hy_ph_u) with respect to Ca and Cb of every
+ * cell. No counterpart in the reference, which has no gradient.
+ * fdtd_grad_forward resets the simulation and runs all size_t steps,
+ * keeping the fields and CPML auxiliaries every `checkpoint_every` steps;
+ * the caller then reads the phasors, evaluates J and its derivative with
+ * respect to the real and imaginary part of each phasor cell, and passes
+ * them to fdtd_grad_backward (4 planes each, (ny_ph, nx_ph) float64, in
+ * the order above). The backward sweep recomputes each segment of steps
+ * from its checkpoint and runs the transposed step backwards through it.
+ * Outputs: dJ/dCa and dJ/dCb of the first nz_out planes, (nz_out, ny, nx)
+ * float64. The phasors are left as the forward solve produced them; the
+ * fields are not. Device memory: (size_t / checkpoint_every + checkpoint_every
+ * + 1) states of 6 fields plus the adjoint state. */
+int fdtd_grad_forward(fdtd_sim *s, int checkpoint_every);
+int fdtd_grad_backward(fdtd_sim *s, const double *dj_dre, const double *dj_dim, int nz_out,
+                       double *grad_ca, double *grad_cb);
+
 /* ---- batched sweep --------------------------------------------------------
  * Several simulations (uneven grids, one device, one element type) advanced
  * together: every time step runs the H pass, the E pass and the phasor pass

@@ -93,6 +93,19 @@ struct fdtd_sim {
   int plan_ok = 0, plan_tile_y = 0, plan_zchunk = 0;
   int graph_chunk = 0;
   int check_every = 0;
+  // gradient (fdtd_grad_*): checkpoints of the forward solve, the segment
+  // of recomputed states and the adjoint state; a state is the 6 fields
+  // followed by one CPML auxiliary set
+  int grad_every = 0, grad_ncp = 0, grad_seg_slots = 0;
+  bool grad_forward_done = false;
+  void* grad_cp = nullptr;
+  void* grad_seg = nullptr;
+  void* grad_lam = nullptr;
+  void* grad_lpsi = nullptr;
+  double* grad_ca = nullptr;
+  double* grad_cb = nullptr;
+  double* grad_gre = nullptr;
+  double* grad_gim = nullptr;
   // per-kernel event timing
   int timing = 0;
   std::vector<cudaEvent_t> ev;   // 3 per timed step: before step, after step, after phasors
@@ -134,6 +147,16 @@ int alloc(fdtd_sim* s, size_t bytes, void** out) {
   s->bufs.push_back({p, bytes});
   *out = p;
   return FDTD_OK;
+}
+
+void release(fdtd_sim* s, void* p) {
+  if (!p) return;
+  for (size_t i = 0; i < s->bufs.size(); ++i)
+    if (s->bufs[i].p == p) {
+      cudaFree(p);
+      s->bufs.erase(s->bufs.begin() + i);
+      return;
+    }
 }
 
 template <class T>
@@ -203,7 +226,7 @@ int collect_timing(fdtd_sim* s) {
 }
 
 template <class T>
-int enqueue_steps(fdtd_sim* s, int n) {
+int enqueue_steps(fdtd_sim* s, int n, bool phasors = true) {
   for (int k = 0; k < n; ++k) {
     if (s->timing && s->ev_used + 3 > 3 * 4096) {
       int rc = collect_timing(s);
@@ -239,12 +262,12 @@ int enqueue_steps(fdtd_sim* s, int n) {
       s->cur = nxt;
       mark(s, e1);
       State<T> sp = make_state<T>(s, s->cur, s->cur);
-      launch_phasors<T>(sp, s->tdev, k, s->stream);
+      if (phasors) launch_phasors<T>(sp, s->tdev, k, s->stream);
     } else {
       State<T> st = make_state<T>(s, s->cur, s->cur);
       launch_split_step<T>(st, s->tdev, k, s->stream);
       mark(s, e1);
-      launch_phasors<T>(st, s->tdev, k, s->stream);
+      if (phasors) launch_phasors<T>(st, s->tdev, k, s->stream);
     }
     mark(s, e2);
   }
@@ -972,6 +995,180 @@ int fdtd_batch_get_stream(fdtd_batch* b, void** stream) {
   if (!b || !stream) return fail(FDTD_ERR_INVALID, "null argument");
   *stream = (void*)b->stream;
   return FDTD_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// gradient of a far-field objective (adjoint sweep with checkpoints)
+// ---------------------------------------------------------------------------
+namespace {
+
+long long state_elems(const fdtd_sim* s) { return 6 * s->vol + s->psi_elems; }
+
+int save_state(fdtd_sim* s, void* slot) {
+  const size_t fb = (size_t)s->vol * s->esz;
+  unsigned char* d = static_cast<unsigned char*>(slot);
+  for (int c = 0; c < 6; ++c)
+    CK(cudaMemcpyAsync(d + c * fb, s->fld[s->cur][c], fb, cudaMemcpyDeviceToDevice, s->stream));
+  CK(cudaMemcpyAsync(d + 6 * fb, s->psi_base[s->cur], (size_t)s->psi_elems * s->esz,
+                     cudaMemcpyDeviceToDevice, s->stream));
+  return FDTD_OK;
+}
+
+int restore_state(fdtd_sim* s, const void* slot) {
+  const size_t fb = (size_t)s->vol * s->esz;
+  const unsigned char* d = static_cast<const unsigned char*>(slot);
+  for (int c = 0; c < 6; ++c)
+    CK(cudaMemcpyAsync(s->fld[s->cur][c], d + c * fb, fb, cudaMemcpyDeviceToDevice, s->stream));
+  CK(cudaMemcpyAsync(s->psi_base[s->cur], d + 6 * fb, (size_t)s->psi_elems * s->esz,
+                     cudaMemcpyDeviceToDevice, s->stream));
+  return FDTD_OK;
+}
+
+int set_step(fdtd_sim* s, int t) {
+  CK(cudaStreamSynchronize(s->stream));
+  const int h[4] = {t, 0, 0, 0};
+  CK(cudaMemcpy(s->tdev, h, sizeof(int), cudaMemcpyHostToDevice));
+  s->t = t;
+  return FDTD_OK;
+}
+
+template <class T>
+Psi<T> psi_view(const fdtd_sim* s, T* base) {
+  Psi<T> p;
+  for (int side = 0; side < 2; ++side)
+    for (int c = 0; c < 4; ++c) {
+      p.z[side][c] = base + s->poz[side][c];
+      p.x[side][c] = base + s->pox[side][c];
+      p.y[side][c] = base + s->poy[side][c];
+    }
+  return p;
+}
+
+template <class T>
+int grad_backward(fdtd_sim* s, int nz_out, double* out_ca, double* out_cb) {
+  const int nt = s->g.nt, every = s->grad_every;
+  const long long vol = s->vol, se = state_elems(s);
+  T* seg = static_cast<T*>(s->grad_seg);
+  T* lam = static_cast<T*>(s->grad_lam);
+  Adj<T> a;
+  a.lex = lam; a.ley = lam + vol; a.lez = lam + 2 * vol;
+  a.lhx = lam + 3 * vol; a.lhy = lam + 4 * vol; a.lhz = lam + 5 * vol;
+  a.lps = psi_view<T>(s, static_cast<T*>(s->grad_lpsi));
+  a.gca = s->grad_ca;
+  a.gcb = s->grad_cb;
+  a.g_re = s->grad_gre;
+  a.g_im = s->grad_gim;
+  a.nz_grad = s->g.nz;
+  for (int c = s->grad_ncp - 1; c >= 0; --c) {
+    const int z0 = c * every, n = std::min(every, nt - z0);
+    int rc;
+    if ((rc = restore_state(s, static_cast<T*>(s->grad_cp) + (size_t)c * se))) return rc;
+    if ((rc = set_step(s, z0))) return rc;
+    if ((rc = save_state(s, seg))) return rc;
+    for (int j = 1; j <= n; ++j) {   // recompute the segment, fields only
+      if ((rc = enqueue_steps<T>(s, 1, false))) return rc;
+      if ((rc = save_state(s, seg + (size_t)j * se))) return rc;
+    }
+    s->t = z0 + n;
+    for (int j = n - 1; j >= 0; --j) {
+      State<T> st = make_state<T>(s, s->cur, s->cur);
+      T* sn = seg + (size_t)j * se;
+      T* sn1 = seg + (size_t)(j + 1) * se;
+      st.iex = sn; st.iey = sn + vol; st.iez = sn + 2 * vol;
+      st.ihx = sn1 + 3 * vol; st.ihy = sn1 + 4 * vol; st.ihz = sn1 + 5 * vol;
+      st.ps = psi_view<T>(s, sn1 + 6 * vol);
+      launch_adjoint_step<T>(st, a, z0 + j, s->stream);
+    }
+    CK(cudaGetLastError());
+  }
+  // the first nz_out planes of the gradients, without the row padding
+  const size_t row = (size_t)s->g.nx * sizeof(double);
+  const size_t spitch = (size_t)s->pitch * sizeof(double);
+  if (out_ca)
+    CK(cudaMemcpy2DAsync(out_ca, row, s->grad_ca, spitch, row, (size_t)nz_out * s->g.ny,
+                         cudaMemcpyDeviceToHost, s->stream));
+  if (out_cb)
+    CK(cudaMemcpy2DAsync(out_cb, row, s->grad_cb, spitch, row, (size_t)nz_out * s->g.ny,
+                         cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return FDTD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fdtd_grad_forward(fdtd_sim* s, int checkpoint_every) {
+  int rc = check_sim(s);
+  if (rc) return rc;
+  if (checkpoint_every < 1) return fail(FDTD_ERR_INVALID, "checkpoint period must be >= 1");
+  if (!s->have_abs) return fail(FDTD_ERR_STATE, "absorbers not set (fdtd_set_absorbers)");
+  if (!s->have_mat) return fail(FDTD_ERR_STATE, "materials not set (fdtd_set_materials)");
+  if (s->g.nt_inc > 0 && s->inc_nt < s->g.nt_inc)
+    return fail(FDTD_ERR_STATE, "incident beam not set (fdtd_set_incident)");
+  const int nt = s->g.nt;
+  const int ncp = (nt + checkpoint_every - 1) / checkpoint_every;
+  const size_t sb = (size_t)state_elems(s) * s->esz;
+  if (s->grad_cp == nullptr || s->grad_ncp != ncp) {
+    release(s, s->grad_cp);
+    s->grad_cp = nullptr;
+    if ((rc = alloc(s, sb * ncp, &s->grad_cp))) return rc;
+  }
+  s->grad_every = checkpoint_every;
+  s->grad_ncp = ncp;
+  s->grad_forward_done = false;
+  if ((rc = fdtd_reset(s))) return rc;
+  for (int c = 0; c < ncp; ++c) {
+    if ((rc = save_state(s, static_cast<unsigned char*>(s->grad_cp) + c * sb))) return rc;
+    const int n = std::min(checkpoint_every, nt - c * checkpoint_every);
+    rc = s->g.dtype == FDTD_F32 ? enqueue_steps<float>(s, n) : enqueue_steps<double>(s, n);
+    if (rc) return rc;
+    s->t += n;
+  }
+  CK(cudaStreamSynchronize(s->stream));
+  s->grad_forward_done = true;
+  return FDTD_OK;
+}
+
+int fdtd_grad_backward(fdtd_sim* s, const double* dj_dre, const double* dj_dim, int nz_out,
+                       double* grad_ca, double* grad_cb) {
+  int rc = check_sim(s);
+  if (rc) return rc;
+  if (!dj_dre || !dj_dim) return fail(FDTD_ERR_INVALID, "null phasor gradient");
+  if (nz_out < 0 || nz_out > s->g.nz) return fail(FDTD_ERR_INVALID, "bad nz_out %d", nz_out);
+  if (!s->grad_forward_done || s->t != s->g.nt)
+    return fail(FDTD_ERR_STATE, "run fdtd_grad_forward first (and no steps after it)");
+  const size_t sb = (size_t)state_elems(s) * s->esz;
+  const int slots = s->grad_every + 1;
+  if (s->grad_seg == nullptr || s->grad_seg_slots != slots) {
+    release(s, s->grad_seg);
+    s->grad_seg = nullptr;
+    if ((rc = alloc(s, sb * slots, &s->grad_seg))) return rc;
+    s->grad_seg_slots = slots;
+  }
+  const size_t fb = (size_t)s->vol * s->esz;
+  const size_t gb = (size_t)s->vol * sizeof(double);
+  const size_t pb = (size_t)4 * s->ny_ph * s->nx_ph * sizeof(double);
+  if (!s->grad_lam) {
+    if ((rc = alloc(s, 6 * fb, &s->grad_lam))) return rc;
+    if ((rc = alloc(s, (size_t)s->psi_elems * s->esz, &s->grad_lpsi))) return rc;
+    if ((rc = alloc(s, gb, (void**)&s->grad_ca))) return rc;
+    if ((rc = alloc(s, gb, (void**)&s->grad_cb))) return rc;
+    if ((rc = alloc(s, pb, (void**)&s->grad_gre))) return rc;
+    if ((rc = alloc(s, pb, (void**)&s->grad_gim))) return rc;
+  }
+  CK(cudaMemsetAsync(s->grad_lam, 0, 6 * fb, s->stream));
+  CK(cudaMemsetAsync(s->grad_lpsi, 0, (size_t)s->psi_elems * s->esz, s->stream));
+  CK(cudaMemsetAsync(s->grad_ca, 0, gb, s->stream));
+  CK(cudaMemsetAsync(s->grad_cb, 0, gb, s->stream));
+  CK(cudaMemcpyAsync(s->grad_gre, dj_dre, pb, cudaMemcpyHostToDevice, s->stream));
+  CK(cudaMemcpyAsync(s->grad_gim, dj_dim, pb, cudaMemcpyHostToDevice, s->stream));
+  rc = s->g.dtype == FDTD_F32 ? grad_backward<float>(s, nz_out, grad_ca, grad_cb)
+                              : grad_backward<double>(s, nz_out, grad_ca, grad_cb);
+  s->grad_forward_done = false;
+  return rc;
 }
 
 }  // extern "C"

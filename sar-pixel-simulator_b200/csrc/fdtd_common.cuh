@@ -78,6 +78,23 @@ struct State {
   int kahan;
 };
 
+// Adjoint state of one simulation (fdtd_adjoint.cu): the adjoint fields,
+// the adjoint CPML auxiliaries (same layout as Psi), the gradient
+// accumulators with respect to Ca and Cb (float64, planes z < nz_grad), and
+// dJ/d(Re p), dJ/d(Im p) of the four upper-plane phasors (ex, ey, hx, hy;
+// (ny_ph, nx_ph) each, float64).
+template <class T>
+struct Adj {
+  T* lex; T* ley; T* lez;
+  T* lhx; T* lhy; T* lhz;
+  Psi<T> lps;
+  double* gca;
+  double* gcb;
+  const double* g_re;
+  const double* g_im;
+  int nz_grad;
+};
+
 // One member of a batched sweep: its State (current field set, in place),
 // its step counter, and its tiling: 128-thread blocks of `width` lanes
 // (width * 4 x cells) by 128 / width rows, gx x gy of them per plane; ph_n

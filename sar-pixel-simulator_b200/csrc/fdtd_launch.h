@@ -53,6 +53,12 @@ template <class T>
 void launch_shell_pass(const State<T>& s, const int* tdev, int toff, const ShellBoxes& bl,
                        bool h_pass, cudaStream_t st);
 
+// One transposed step (fdtd_adjoint.cu): s holds E^n in its source E
+// pointers, H^{n+1/2} in its source H pointers and the CPML auxiliaries
+// after the step in ps; t is the step index n.
+template <class T>
+void launch_adjoint_step(const State<T>& s, const Adj<T>& a, int t, cudaStream_t st);
+
 // Records an error message for fdtd_last_error(); returns code.
 int report_error(int code, const char* msg);
 

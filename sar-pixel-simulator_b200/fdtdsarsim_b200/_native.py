@@ -101,6 +101,8 @@ SIGNATURES = {
     'fdtd_get_field': [_P, _I, _P],
     'fdtd_set_field': [_P, _I, _P],
     'fdtd_near2far': [_P, _P, _P, _P, _I, _I, _I, _I, _D, _D, _P, _I, _P, _I, _D, _I, _P],
+    'fdtd_grad_forward': [_P, _I],
+    'fdtd_grad_backward': [_P, _P, _P, _I, _P, _P],
     'fdtd_batch_create': [ctypes.POINTER(_P), _I, ctypes.POINTER(_P)],
     'fdtd_batch_destroy': [_P],
     'fdtd_batch_set_option': [_P, _I, _I],
@@ -285,6 +287,26 @@ class NativeSim:
         k = FIELD_NAMES.index(comp) if isinstance(comp, str) else int(comp)
         a = self._arr(arr, (g.nz, g.ny, g.nx))
         check(lib.fdtd_set_field(self.h, k, ptr(a)))
+
+    def grad_forward(self, checkpoint_every):
+        """Reset and run all size_t steps keeping checkpoints
+        (fdtd_grad_forward)."""
+        check(lib.fdtd_grad_forward(self.h, int(checkpoint_every)))
+
+    def grad_backward(self, dj_dre, dj_dim, nz_out):
+        """dJ/dCa, dJ/dCb of the first nz_out planes from dJ/d(Re, Im) of the
+        four upper-plane phasors, each (4, ny_ph, nx_ph) float64
+        (fdtd_grad_backward)."""
+        g = self.geom
+        shape = (4, g.ny - 2 * g.npml, g.nx - 2 * g.npml)
+        re = np.ascontiguousarray(dj_dre, dtype=np.float64)
+        im = np.ascontiguousarray(dj_dim, dtype=np.float64)
+        if re.shape != shape or im.shape != shape:
+            raise ValueError(f'phasor gradients must have shape {shape}')
+        gca = np.empty((int(nz_out), g.ny, g.nx), np.float64)
+        gcb = np.empty_like(gca)
+        check(lib.fdtd_grad_backward(self.h, ptr(re), ptr(im), int(nz_out), ptr(gca), ptr(gcb)))
+        return gca, gcb
 
     def get_fields(self):
         return {c: self.get_field(c) for c in FIELD_NAMES}
