@@ -115,7 +115,7 @@ def test_autograd_function_returns_the_runner_gradient():
     ts = torch.tensor(sig, dtype=torch.float64, requires_grad=True)
     P = backscatter_power(te, ts, run)
     (2.0 * P).backward()
-    assert float(P) == J
+    assert float(P.detach()) == J
     assert np.array_equal(te.grad.numpy(), 2.0 * ge)
     assert np.array_equal(ts.grad.numpy(), 2.0 * gs)
     run.close()
