@@ -40,7 +40,8 @@ def parse():
     ap.add_argument('--warmup', type=int, default=5)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--workload', default='plain_16x16',
-                    choices=['plain_16x16', 'plain_8x8', 'batch64'])
+                    choices=['plain_16x16', 'plain_8x8', 'batch64', 'adjoint_4x4'])
+    ap.add_argument('--fd-cells', type=int, default=32, help='adjoint_4x4: cells checked by FD')
     ap.add_argument('--models', type=int, default=64, help='batch64: number of models')
     ap.add_argument('--kernel', default='auto', choices=['auto', 'split', 'fused'])
     ap.add_argument('--tile-y', type=int, default=None, help='fused kernel rows per tile')
@@ -68,11 +69,11 @@ def build_workload(name, dtype, nsteps_inc, seed=2024):
     ca, cb = compute_material_arrays(pc, model)
     # The timed window covers steps t < size_t_inc of a full solve, so every
     # timed step injects, as the first 1372 steps of the real solve do. Only
-    # the planes of the steps that run are synthesised.
-    g.size_t_inc = min(g.size_t_inc, nsteps_inc)
-    inc = {}
-    for comp, scale in (('ex', 1.0), ('ey', 1.0), ('hx', 1 / 376.73), ('hy', 1 / 376.73)):
-        inc[comp] = (scale * rng.standard_normal((g.size_t_inc, g.size_y, g.size_x))).astype(dtype)
+    # the planes of the steps that run are synthesised (a tapered plane wave
+    # with the geometry's frequency, polarisation and angle).
+    n = min(g.size_t_inc, nsteps_inc)
+    inc = synthetic.plane_wave_incident(pc, n, dtype)
+    g.size_t_inc = n
     return pc, ca, cb, inc
 
 
@@ -88,7 +89,7 @@ def workload_desc(pc, name):
         'npml': g.size_pml,
         'materials': 'synthetic seeded (snowpack of ice spheres over rough soil)'
         if name == 'plain_16x16' else 'synthetic seeded (rough lognormal soil)',
-        'incident': 'synthetic seeded planes, injected every timed step',
+        'incident': 'tapered plane wave (geometry frequency, polarisation, angle), injected every timed step',
         'l2': 'inputs larger than L2 (fields alone 2.8 GB)',
     }
 
@@ -214,17 +215,19 @@ def run_ours(a):
     geom = native_geometry(pc)
     kernel = {'auto': None, 'split': _native.FDTD_KERNEL_SPLIT,
               'fused': _native.FDTD_KERNEL_FUSED}[a.kernel]
-    choice = tuning.choose(geom, kernel=kernel,
-                           tile=None if a.tile_y is None else (32, a.tile_y))
+    tuned = None
+    if kernel is None and a.tile_y is None:
+        # measure the candidates on this geometry (a few steps each)
+        choice, tuned = tuning.autotune(geom, local, save=False)
+    else:
+        choice = tuning.choose(geom, kernel=kernel,
+                               tile=None if a.tile_y is None else (32, a.tile_y))
+        choice['zchunk'] = a.zchunk
 
     def new_sim():
         sim = _native.NativeSim(geom, local)
         sim.set_absorbers(packed_profiles(pc))
-        sim.set_option(_native.OPT_KERNEL, choice['kernel'])
-        if choice['kernel'] == _native.FDTD_KERNEL_FUSED:
-            sim.set_option(_native.OPT_TILE_X, choice['tile_x'])
-            sim.set_option(_native.OPT_TILE_Y, choice['tile_y'])
-            sim.set_option(_native.OPT_ZCHUNK, a.zchunk)
+        tuning.apply(sim, choice)
         return sim
 
     sim = new_sim()
@@ -332,11 +335,15 @@ def run_ours(a):
             'ms_per_step': round(ms_max / a.steps, 4), 'higher_is_better': True,
             'scaling': 'weak', 'vs_baseline': None,
             'dtype': 'f32' if a.dtype == 'float32' else 'f64',
-            'data': 'synthetic (seeded materials and incident planes of the named shapes)',
+            'data': 'synthetic (seeded materials of the named shapes, tapered plane-wave incident planes)',
             'config': dict(workload_desc(pc, a.workload),
                            parallelism=f'replicas x{world}' if world > 1 else 'single GPU',
                            kernel=kname, tile=[choice['tile_x'], choice['tile_y']]
-                           if choice['kernel'] == _native.FDTD_KERNEL_FUSED else None),
+                           if choice['kernel'] == _native.FDTD_KERNEL_FUSED else None,
+                           zchunk=choice.get('zchunk', 0),
+                           autotuned=None if tuned is None else
+                           [{'ms': t, 'kernel': 'fused' if c['kernel'] else 'split',
+                             'tile_y': c['tile_y'], 'zchunk': c['zchunk']} for t, c in tuned]),
             'roofline': roofline, 'cpu_baseline': base, 'e2e': e2e,
             'gpu_launches': gpu_launches, 'clocks': clk,
         }
@@ -364,7 +371,7 @@ def run_reference(a):
         'ms_per_step': round(cells / (base['value'] * 1e6) * 1e3, 2), 'higher_is_better': True,
         'scaling': 'weak', 'vs_baseline': None,
         'dtype': 'f32' if a.dtype == 'float32' else 'f64',
-        'data': 'synthetic (seeded materials and incident planes of the named shapes)',
+        'data': 'synthetic (seeded materials of the named shapes, tapered plane-wave incident planes)',
         'config': workload_desc(pc, a.workload),
         'cpu_baseline': base,
         'e2e': {'value': round(base['value'], 2), 'unit': 'Mcell-updates/s',
@@ -397,10 +404,9 @@ def batch_models(n, nsteps_inc, seed=4040, dtype='float32'):
         g = pc.geom_params
         model = synthetic.vegetation_model(pc, rng, name=f'veg{k:02d}')
         ca, cb = compute_material_arrays(pc, model)
-        g.size_t_inc = min(g.size_t_inc, nsteps_inc)
-        inc = {}
-        for comp, scale in (('ex', 1.0), ('ey', 1.0), ('hx', 1 / 376.73), ('hy', 1 / 376.73)):
-            inc[comp] = (scale * rng.standard_normal((g.size_t_inc, g.size_y, g.size_x))).astype(dtype)
+        n = min(g.size_t_inc, nsteps_inc)
+        inc = synthetic.plane_wave_incident(pc, n, dtype)
+        g.size_t_inc = n
         out.append((pc, ca, cb, inc))
     return out
 
@@ -473,7 +479,7 @@ def run_batch(a):
         'n_gpus': 1, 'steps': a.steps, 'warmup': a.warmup, 'ms_per_step': round(ms_b / a.steps, 4),
         'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
         'dtype': 'f32' if a.dtype == 'float32' else 'f64',
-        'data': 'synthetic (seeded vegetation models and incident planes of the named shapes)',
+        'data': 'synthetic (seeded vegetation models, tapered plane-wave incident planes)',
         'config': {'workload': f'batch{a.models}: {a.models} vegetation models, x-y 2-8 wl, depth '
                                f'0.5-2 wl, cell 0.03 wl, HH/VV, 5.4 GHz',
                    'models': a.models, 'cells_total': total,
@@ -492,12 +498,103 @@ def run_batch(a):
     print(json.dumps(line))
 
 
+# ---------------------------------------------------------------------------
+# adjoint: cost of the gradient against one forward solve, and its accuracy
+# ---------------------------------------------------------------------------
+def run_adjoint(a):
+    import torch
+    torch.cuda.set_device(0)
+    from fdtdsarsim_b200 import synthetic
+    from fdtdsarsim_b200.adjoint import BackscatterGradient
+
+    def problem(dtype):
+        pc = synthetic.config_params('adjoint_4x4', dtype)
+        g = pc.geom_params
+        rng = np.random.default_rng(5050)
+        model = synthetic.uniform_rough_soil(pc, rng)
+        return pc, model, synthetic.plane_wave_incident(pc, g.size_t_inc, dtype)
+
+    pc, model, inc = problem('float32')
+    g = pc.geom_params
+    eps = model.relative_permittivity.astype(np.float64)
+    sig = model.conductivity.astype(np.float64)
+    from fdtdsarsim_b200 import tuning
+    from fdtdsarsim_b200.gpu.main_sim import native_geometry
+    tuned, _ = tuning.autotune(native_geometry(pc), 0)   # cached for the runners below
+    run = BackscatterGradient(pc, inc, checkpoint_every=64)
+    run.value(eps, sig)   # warm-up
+    run.value_and_grad(eps, sig)
+
+    def wall(fn, reps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            out = fn()
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) / reps, out
+    t_fwd, J = wall(lambda: run.value(eps, sig), 3)
+    t_adj, (J2, ge, gs) = wall(lambda: run.value_and_grad(eps, sig), 3)
+
+    # float64 adjoint and central differences of float64 forward solves
+    pc64, _, inc64 = problem('float64')
+    inc64 = {k: v.astype(np.float64) for k, v in inc.items()}
+    run64 = BackscatterGradient(pc64, inc64, checkpoint_every=64)
+    J64, ge64, gs64 = run64.value_and_grad(eps, sig)
+    rng = np.random.default_rng(7)
+    mask = np.abs(ge64) > 1e-3 * np.abs(ge64).max()
+    cells = np.argwhere(mask)
+    picks = cells[rng.choice(len(cells), size=min(a.fd_cells, len(cells)), replace=False)]
+    err32, err64 = [], []
+    for z, y, x in picks:
+        for base, g32, g64, is_eps in ((eps, ge, ge64, True), (sig, gs, gs64, False)):
+            if base[z, y, x] == 0:
+                continue   # sigma 0 (air): no relative step
+            h = 1e-3 * base[z, y, x]
+            b1, b2 = base.copy(), base.copy()
+            b1[z, y, x] += h
+            b2[z, y, x] -= h
+            if is_eps:
+                fd = (run64.value(b1, sig) - run64.value(b2, sig)) / (2 * h)
+            else:
+                fd = (run64.value(eps, b1) - run64.value(eps, b2)) / (2 * h)
+            err32.append(abs(g32[z, y, x] - fd) / abs(fd))
+            err64.append(abs(g64[z, y, x] - fd) / abs(fd))
+    finite = bool(np.isfinite(ge).all() and np.isfinite(gs).all())
+    norm_rel = float(np.linalg.norm(ge - ge64) / np.linalg.norm(ge64)) if finite else None
+    cells_total = g.size_x * g.size_y * g.size_z
+    line = {
+        'metric': 'adjoint gradient time / forward solve time', 'value': round(t_adj / t_fwd, 3),
+        'unit': 'ratio', 'higher_is_better': False, 'n_gpus': 1,
+        'dtype': 'f32', 'data': 'synthetic (seeded rough soil, eps_r U(5,12), sigma U(0.005,0.05); '
+                                'tapered plane-wave incident planes)',
+        'config': {'workload': f'adjoint_4x4: {g.size_z}x{g.size_y}x{g.size_x} cells, nt {g.size_t}, '
+                               f'HH backscatter power at theta -20 deg, checkpoint every 64',
+                   'cells': cells_total, 'size_t': g.size_t},
+        'forward_s': round(t_fwd, 4), 'gradient_s': round(t_adj, 4),
+        'forward_mcell_updates_per_s': round(cells_total * g.size_t / t_fwd / 1e6, 1),
+        'power': J, 'power_f64': J64,
+        'fd_check': {'cells': int(len(picks)), 'params': ['eps_r', 'sigma'], 'step': '1e-3 relative',
+                     'fd_solver': 'float64 forward solves',
+                     'max_rel_err_f32_adjoint': float(max(err32)),
+                     'median_rel_err_f32_adjoint': float(np.median(err32)),
+                     'max_rel_err_f64_adjoint': float(max(err64))},
+        'f32_vs_f64_adjoint_rel_l2': norm_rel, 'gradients_finite': finite,
+        'nonfinite_f32': int((~np.isfinite(ge)).sum() + (~np.isfinite(gs)).sum()),
+        'kernel': tuned,
+    }
+    run.close()
+    run64.close()
+    print(json.dumps(line))
+
+
 def main():
     a = parse()
     if a.impl == 'reference':
         run_reference(a)
     elif a.workload == 'batch64':
         run_batch(a)
+    elif a.workload == 'adjoint_4x4':
+        run_adjoint(a)
     else:
         run_ours(a)
 

@@ -14,15 +14,18 @@
 // onto the neighbour that owned the term.
 //
 // Every kernel is written in gather form (each thread writes only its own
-// cell), in the order of the reverse sweep of step n:
-//   1. k_adj_phasor_e: lambda_E on the upper phasor plane += dJ/dE^{n+1}
-//   2. k_adj_e_to_h:   lambda_H += (E update and E CPML)^T lambda_E
-//   3. k_adj_e_own:    gradients; psi_E adjoint; lambda_E = Ca lambda_E
-//   4. k_adj_phasor_h: lambda_H on the two planes += dJ/dH^{n+1/2}
-//   5. k_adj_h_to_e:   lambda_E += (H update and H CPML)^T lambda_H
-//   6. k_adj_h_own:    psi_H adjoint
-// Kernel 2 reads lambda_E and the E adjoint auxiliaries of neighbours
-// before kernel 3 overwrites them; kernel 5 likewise before kernel 6.
+// cell). The reverse sweep of step n is, in order:
+//   a. lambda_E on the upper phasor plane += dJ/dE^{n+1}
+//   b. lambda_H += (E update and E CPML)^T lambda_E
+//   c. gradients; psi_E adjoint; lambda_E = Ca lambda_E
+//   d. lambda_H on the two planes += dJ/dH^{n+1/2}
+//   e. lambda_E += (H update and H CPML)^T lambda_H
+//   f. psi_H adjoint
+// b reads lambda_E and the E auxiliaries' adjoint of neighbours before c
+// overwrites them; e reads lambda_H and the H auxiliaries' adjoint of
+// neighbours before f overwrites them. Two kernels per step do all six:
+// k_adj_k1 = f of step n + 1, b, d; k_adj_k2 = c, e, a of step n - 1; only
+// the first backward step needs a on its own (k_adj_phasor_e).
 #include "fdtd_launch.h"
 
 namespace fdtd {
@@ -109,44 +112,58 @@ __device__ __forceinline__ double ph_g(const Adj<T>& a, int comp, int ia, int ib
   return a.g_re[k] * c + a.g_im[k] * sn;
 }
 
+// phasor E source of step t at cell (z, y, x): (d ex, d ey)
 template <class T>
-__global__ void k_adj_phasor_e(const __grid_constant__ State<T> s, Adj<T> a, int t) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
-  if (x >= s.nx) return;
-  const int m = s.npml, pz = s.nz - m - 1;
+__device__ __forceinline__ void phasor_e_src(const State<T>& s, const Adj<T>& a, int t, int z, int y,
+                                             int x, T& dex, T& dey) {
+  dex = T(0);
+  dey = T(0);
+  const int m = s.npml;
+  if (z != s.nz - m - 1) return;
   const double* ph = s.phase + 4 * (long long)t;
   const double c = ph[0], sn = ph[1];
   const int ia = y - m, ib = x - m;
-  const long long i = idx(s, pz, y, x);
   const double gx = ph_g(a, 0, ia, ib, s.ny_ph, s.nx_ph, c, sn) + ph_g(a, 0, ia, ib + 1, s.ny_ph, s.nx_ph, c, sn);
   const double gy = ph_g(a, 1, ia, ib, s.ny_ph, s.nx_ph, c, sn) + ph_g(a, 1, ia + 1, ib, s.ny_ph, s.nx_ph, c, sn);
-  if (gx != 0.0) a.lex[i] += (T)(0.5 * gx);
-  if (gy != 0.0) a.ley[i] += (T)(0.5 * gy);
+  dex = (T)(0.5 * gx);
+  dey = (T)(0.5 * gy);
 }
 
+// phasor H source of step t at cell (z, y, x): (d hx, d hy), planes pz - 1, pz
 template <class T>
-__global__ void k_adj_phasor_h(const __grid_constant__ State<T> s, Adj<T> a, int t) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
-  if (x >= s.nx) return;
+__device__ __forceinline__ void phasor_h_src(const State<T>& s, const Adj<T>& a, int t, int z, int y,
+                                             int x, T& dhx, T& dhy) {
+  dhx = T(0);
+  dhy = T(0);
   const int m = s.npml, pz = s.nz - m - 1;
+  if (z != pz && z != pz - 1) return;
   const double* ph = s.phase + 4 * (long long)t;
   const double c = ph[2], sn = ph[3];
   const int ia = y - m, ib = x - m;
   const double gx = ph_g(a, 2, ia, ib, s.ny_ph, s.nx_ph, c, sn) + ph_g(a, 2, ia + 1, ib, s.ny_ph, s.nx_ph, c, sn);
   const double gy = ph_g(a, 3, ia, ib, s.ny_ph, s.nx_ph, c, sn) + ph_g(a, 3, ia, ib + 1, s.ny_ph, s.nx_ph, c, sn);
-  if (gx == 0.0 && gy == 0.0) return;
-  for (int zz = pz - 1; zz <= pz; ++zz) {
-    const long long i = idx(s, zz, y, x);
-    a.lhx[i] += (T)(0.25 * gx);
-    a.lhy[i] += (T)(0.25 * gy);
-  }
+  dhx = (T)(0.25 * gx);
+  dhy = (T)(0.25 * gy);
+}
+
+// standalone E source of the first backward step (the later ones are added
+// by k_adj_k2 of the step after them)
+template <class T>
+__global__ void k_adj_phasor_e(const __grid_constant__ State<T> s, Adj<T> a, int t) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+  if (x >= s.nx) return;
+  const int z = s.nz - s.npml - 1;
+  T dex, dey;
+  phasor_e_src(s, a, t, z, y, x, dex, dey);
+  const long long i = idx(s, z, y, x);
+  if (re_x(s, z, y, x)) a.lex[i] += dex;
+  if (re_y(s, z, y, x)) a.ley[i] += dey;
 }
 
 // ---- 2: lambda_H += (E update + E CPML)^T lambda_E ----------------------------
 template <class T>
-__global__ void __launch_bounds__(128) k_adj_e_to_h(const __grid_constant__ State<T> s, Adj<T> a) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y, z = blockIdx.z;
-  if (x >= s.nx) return;
+__device__ __forceinline__ void e_to_h_terms(const State<T>& s, const Adj<T>& a, int z, int y, int x,
+                                             T& out_hx, T& out_hy, T& out_hz) {
   const int nx = s.nx, ny = s.ny, nz = s.nz, m = s.npml;
   // F = Cb lambda_E on each component's update range
   auto Fx = [&](int zz, int yy, int xx) -> T {
@@ -210,18 +227,17 @@ __global__ void __launch_bounds__(128) k_adj_e_to_h(const __grid_constant__ Stat
   // y faces: Exy uses hz(c) - hz(c - y), Ezy uses hx(c) - hx(c - y)
   dhz += face_term(2, 0, z, y, x) - face_term(2, 0, z, y + 1, x);
   dhx += face_term(2, 1, z, y, x) - face_term(2, 1, z, y + 1, x);
-  const long long i = idx(s, z, y, x);
-  a.lhx[i] += dhx;
-  a.lhy[i] += dhy;
-  a.lhz[i] += dhz;
+  out_hx = dhx;
+  out_hy = dhy;
+  out_hz = dhz;
 }
 
-// ---- 3: gradients, E auxiliaries' adjoint, lambda_E = Ca lambda_E ---------
+// ---- 3: gradients, E auxiliaries' adjoint, Ca lambda_E --------------------
 // s.iex.. hold E^n, s.ihx.. H^{n+1/2}, s.ps the auxiliaries after the step.
+// Returns Ca lambda_E of the cell (zero outside the update ranges).
 template <class T>
-__global__ void __launch_bounds__(128) k_adj_e_own(const __grid_constant__ State<T> s, Adj<T> a) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y, z = blockIdx.z;
-  if (x >= s.nx) return;
+__device__ __forceinline__ void e_own_part(const State<T>& s, const Adj<T>& a, int z, int y, int x,
+                                           T& out_x, T& out_y, T& out_z) {
   const int nx = s.nx, ny = s.ny, nz = s.nz, m = s.npml;
   const long long P = s.plane, W = s.pitch;
   const long long i = idx(s, z, y, x);
@@ -229,15 +245,16 @@ __global__ void __launch_bounds__(128) k_adj_e_own(const __grid_constant__ State
   const T cb = s.cb[i], ca = s.ca[i];
   double gca = 0.0, gcb = 0.0;
   const T* hx = s.ihx; const T* hy = s.ihy; const T* hz = s.ihz;
-  if (re_x(s, z, y, x)) {
+  const bool grad = z < a.nz_grad;   // gradients only over the requested planes
+  if (grad && re_x(s, z, y, x)) {
     gca += (double)lx * (double)s.iex[i];
     gcb += (double)lx * (double)((hz[i] - hz[i - W]) - (hy[i] - hy[i - P]));
   }
-  if (re_y(s, z, y, x)) {
+  if (grad && re_y(s, z, y, x)) {
     gca += (double)ly * (double)s.iey[i];
     gcb += (double)ly * (double)((hx[i] - hx[i - P]) - (hz[i] - hz[i - 1]));
   }
-  if (re_z(s, z, y, x)) {
+  if (grad && re_z(s, z, y, x)) {
     gca += (double)lz * (double)s.iez[i];
     gcb += (double)lz * (double)((hy[i] - hy[i - 1]) - (hx[i] - hx[i - W]));
   }
@@ -248,7 +265,7 @@ __global__ void __launch_bounds__(128) k_adj_e_own(const __grid_constant__ State
       const T b = s.prof[side ? BE_U : BE_D][q];
       T* p1 = a.lps.z[side][1];
       T* p0 = a.lps.z[side][0];
-      gcb += (double)s.dx * ((double)s.ps.z[side][1][k] * ly - (double)s.ps.z[side][0][k] * lx);
+      if (grad) gcb += (double)s.dx * ((double)s.ps.z[side][1][k] * ly - (double)s.ps.z[side][0][k] * lx);
       p1[k] = b * (p1[k] + cb * s.dx * ly);
       p0[k] = b * (p0[k] - cb * s.dx * lx);
     }
@@ -257,7 +274,7 @@ __global__ void __launch_bounds__(128) k_adj_e_own(const __grid_constant__ State
       const T b = s.prof[side ? BE_U : BE_D][q];
       T* p1 = a.lps.x[side][1];
       T* p0 = a.lps.x[side][0];
-      gcb += (double)s.dx * ((double)s.ps.x[side][1][k] * lz - (double)s.ps.x[side][0][k] * ly);
+      if (grad) gcb += (double)s.dx * ((double)s.ps.x[side][1][k] * lz - (double)s.ps.x[side][0][k] * ly);
       p1[k] = b * (p1[k] + cb * s.dx * lz);
       p0[k] = b * (p0[k] - cb * s.dx * ly);
     }
@@ -266,25 +283,34 @@ __global__ void __launch_bounds__(128) k_adj_e_own(const __grid_constant__ State
       const T b = s.prof[side ? BE_U : BE_D][q];
       T* p0 = a.lps.y[side][0];
       T* p1 = a.lps.y[side][1];
-      gcb += (double)s.dx * ((double)s.ps.y[side][0][k] * lx - (double)s.ps.y[side][1][k] * lz);
+      if (grad) gcb += (double)s.dx * ((double)s.ps.y[side][0][k] * lx - (double)s.ps.y[side][1][k] * lz);
       p0[k] = b * (p0[k] + cb * s.dx * lx);
       p1[k] = b * (p1[k] - cb * s.dx * lz);
     }
   }
-  if (z < a.nz_grad) {
+  if (grad) {
     a.gca[i] += gca;
     a.gcb[i] += gcb;
   }
-  if (re_x(s, z, y, x)) a.lex[i] = ca * lx;
-  if (re_y(s, z, y, x)) a.ley[i] = ca * ly;
-  if (re_z(s, z, y, x)) a.lez[i] = ca * lz;
+  // A component outside its main-update range is updated in the forward
+  // step only by CPML corrections and injection terms that read other such
+  // components (the edge sub-systems, e.g. ey, ez, hx on x = 0), or not at
+  // all. With an incident beam that vanishes on those edges (as the
+  // reference's does) it stays exactly zero, so no parameter reaches J
+  // through it, and nothing in range reads it back in the transposed step.
+  // Its exact adjoint, fed by the interior's, grows exponentially like the
+  // forward sub-system would if driven; it is held at zero instead (here,
+  // and by the range tests where adjoints are accumulated), which leaves
+  // every gradient unchanged and keeps the sweep finite.
+  out_x = re_x(s, z, y, x) ? ca * lx : T(0);
+  out_y = re_y(s, z, y, x) ? ca * ly : T(0);
+  out_z = re_z(s, z, y, x) ? ca * lz : T(0);
 }
 
 // ---- 5: lambda_E += (H update + H CPML)^T lambda_H ----------------------------
 template <class T>
-__global__ void __launch_bounds__(128) k_adj_h_to_e(const __grid_constant__ State<T> s, Adj<T> a) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y, z = blockIdx.z;
-  if (x >= s.nx) return;
+__device__ __forceinline__ void h_to_e_terms(const State<T>& s, const Adj<T>& a, int z, int y, int x,
+                                             T& out_x, T& out_y, T& out_z) {
   const int nx = s.nx, ny = s.ny, nz = s.nz, m = s.npml;
   const T db = s.db;
   auto Gx = [&](int zz, int yy, int xx) -> T {
@@ -343,20 +369,17 @@ __global__ void __launch_bounds__(128) k_adj_h_to_e(const __grid_constant__ Stat
   dez += face_term(1, 2, z, y, x - 1) - face_term(1, 2, z, y, x);
   dez += face_term(2, 2, z, y - 1, x) - face_term(2, 2, z, y, x);
   dex += face_term(2, 3, z, y - 1, x) - face_term(2, 3, z, y, x);
-  const long long i = idx(s, z, y, x);
-  a.lex[i] += dex;
-  a.ley[i] += dey;
-  a.lez[i] += dez;
+  out_x = dex;
+  out_y = dey;
+  out_z = dez;
 }
 
-// ---- 6: H auxiliaries' adjoint ---------------------------------------------------
+// ---- 6: H auxiliaries' adjoint, from the cell's lambda_H (lhx, lhy, lhz) --
 template <class T>
-__global__ void __launch_bounds__(128) k_adj_h_own(const __grid_constant__ State<T> s, Adj<T> a) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y, z = blockIdx.z;
-  if (x >= s.nx || !box(s, z, y, x)) return;
+__device__ __forceinline__ void h_own_part(const State<T>& s, const Adj<T>& a, int z, int y, int x,
+                                           T lhx, T lhy, T lhz) {
+  if (!box(s, z, y, x)) return;
   const int nx = s.nx, ny = s.ny, nz = s.nz, m = s.npml;
-  const long long i = idx(s, z, y, x);
-  const T lhx = a.lhx[i], lhy = a.lhy[i], lhz = a.lhz[i];
   int side, q;
   if (h_face(z, nz, m, side, q)) {
     const long long k = kz(s, q, y, x);
@@ -384,20 +407,61 @@ __global__ void __launch_bounds__(128) k_adj_h_own(const __grid_constant__ State
   }
 }
 
+// ---- the two kernels of one backward step ------------------------------------
+// K1 (step n): the H auxiliaries' adjoint of step n + 1 (skipped for the
+// first backward step), then lambda_H += (E step)^T lambda_E + the H phasor
+// source of step n.
 template <class T>
-void launch_adjoint_step(const State<T>& s, const Adj<T>& a, int t, cudaStream_t st) {
-  const dim3 blk(128, 1, 1);
-  const dim3 grd((s.nx + 127) / 128, s.ny, s.nz);
-  const dim3 gpl((s.nx + 127) / 128, s.ny, 1);
-  k_adj_phasor_e<T><<<gpl, blk, 0, st>>>(s, a, t);
-  k_adj_e_to_h<T><<<grd, blk, 0, st>>>(s, a);
-  k_adj_e_own<T><<<grd, blk, 0, st>>>(s, a);
-  k_adj_phasor_h<T><<<gpl, blk, 0, st>>>(s, a, t);
-  k_adj_h_to_e<T><<<grd, blk, 0, st>>>(s, a);
-  k_adj_h_own<T><<<grd, blk, 0, st>>>(s, a);
+__global__ void __launch_bounds__(128) k_adj_k1(const __grid_constant__ State<T> s, Adj<T> a, int t,
+                                                int first) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y, z = blockIdx.z;
+  if (x >= s.nx) return;
+  const long long i = idx(s, z, y, x);
+  const T lhx = a.lhx[i], lhy = a.lhy[i], lhz = a.lhz[i];
+  if (!first) h_own_part(s, a, z, y, x, lhx, lhy, lhz);
+  T dhx, dhy, dhz, phx, phy;
+  e_to_h_terms(s, a, z, y, x, dhx, dhy, dhz);
+  phasor_h_src(s, a, t, z, y, x, phx, phy);
+  // components outside their update range keep a zero adjoint (e_own_part)
+  a.lhx[i] = rh_x(s, z, y, x) ? lhx + dhx + phx : T(0);
+  a.lhy[i] = rh_y(s, z, y, x) ? lhy + dhy + phy : T(0);
+  a.lhz[i] = rh_z(s, z, y, x) ? lhz + dhz : T(0);
 }
 
-template void launch_adjoint_step<float>(const State<float>&, const Adj<float>&, int, cudaStream_t);
-template void launch_adjoint_step<double>(const State<double>&, const Adj<double>&, int, cudaStream_t);
+// K2 (step n): gradients and the E auxiliaries' adjoint, then
+// lambda_E = Ca lambda_E + (H step)^T lambda_H + the E phasor source of
+// step n - 1 (t_prev < 0: none).
+template <class T>
+__global__ void __launch_bounds__(128) k_adj_k2(const __grid_constant__ State<T> s, Adj<T> a,
+                                                int t_prev) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y, z = blockIdx.z;
+  if (x >= s.nx) return;
+  const long long i = idx(s, z, y, x);
+  T ex, ey, ez, dex, dey, dez, pex = T(0), pey = T(0);
+  e_own_part(s, a, z, y, x, ex, ey, ez);
+  h_to_e_terms(s, a, z, y, x, dex, dey, dez);
+  if (t_prev >= 0) phasor_e_src(s, a, t_prev, z, y, x, pex, pey);
+  a.lex[i] = re_x(s, z, y, x) ? ex + dex + pex : T(0);
+  a.ley[i] = re_y(s, z, y, x) ? ey + dey + pey : T(0);
+  a.lez[i] = re_z(s, z, y, x) ? ez + dez : T(0);
+}
+
+template <class T>
+void launch_adjoint_first(const State<T>& s, const Adj<T>& a, int t, cudaStream_t st) {
+  k_adj_phasor_e<T><<<dim3((s.nx + 127) / 128, s.ny, 1), 128, 0, st>>>(s, a, t);
+}
+
+template <class T>
+void launch_adjoint_step(const State<T>& s, const Adj<T>& a, int t, bool first, cudaStream_t st) {
+  const dim3 grd((s.nx + 127) / 128, s.ny, s.nz);
+  k_adj_k1<T><<<grd, 128, 0, st>>>(s, a, t, first ? 1 : 0);
+  k_adj_k2<T><<<grd, 128, 0, st>>>(s, a, t - 1);
+}
+
+template void launch_adjoint_first<float>(const State<float>&, const Adj<float>&, int, cudaStream_t);
+template void launch_adjoint_first<double>(const State<double>&, const Adj<double>&, int, cudaStream_t);
+template void launch_adjoint_step<float>(const State<float>&, const Adj<float>&, int, bool, cudaStream_t);
+template void launch_adjoint_step<double>(const State<double>&, const Adj<double>&, int, bool,
+                                          cudaStream_t);
 
 }  // namespace fdtd

@@ -1060,29 +1060,80 @@ int grad_backward(fdtd_sim* s, int nz_out, double* out_ca, double* out_cb) {
   a.gcb = s->grad_cb;
   a.g_re = s->grad_gre;
   a.g_im = s->grad_gim;
-  a.nz_grad = s->g.nz;
-  for (int c = s->grad_ncp - 1; c >= 0; --c) {
-    const int z0 = c * every, n = std::min(every, nt - z0);
-    int rc;
-    if ((rc = restore_state(s, static_cast<T*>(s->grad_cp) + (size_t)c * se))) return rc;
-    if ((rc = set_step(s, z0))) return rc;
-    if ((rc = save_state(s, seg))) return rc;
-    for (int j = 1; j <= n; ++j) {   // recompute the segment, fields only
-      if ((rc = enqueue_steps<T>(s, 1, false))) return rc;
-      if ((rc = save_state(s, seg + (size_t)j * se))) return rc;
+  a.nz_grad = nz_out;
+  ShellBoxes whole;
+  memset(&whole, 0, sizeof(whole));
+  add_shell_box(whole, 0, s->g.nx, 0, s->g.ny, 0, s->g.nz);
+  // Segments are recomputed on the side stream into two alternating slot
+  // buffers while the main stream sweeps the previous segment backwards.
+  // The recompute reads the step index as toff with a zero counter
+  // (tdev[2]), so it needs no counter updates between segments.
+  const size_t buf = (size_t)every * se;   // slots 1..every of one buffer
+  const int* zero_t = s->tdev + 2;
+  cudaEvent_t start = nullptr, rec_done[2] = {nullptr, nullptr}, adj_done[2] = {nullptr, nullptr};
+  auto cleanup = [&]() {
+    for (cudaEvent_t e : {start, rec_done[0], rec_done[1], adj_done[0], adj_done[1]})
+      if (e) cudaEventDestroy(e);
+  };
+  for (cudaEvent_t* e : {&start, &rec_done[0], &rec_done[1], &adj_done[0], &adj_done[1]})
+    if (cudaEventCreateWithFlags(e, cudaEventDisableTiming) != cudaSuccess) {
+      cleanup();
+      return fail(FDTD_ERR_CUDA, "event creation failed");
     }
-    s->t = z0 + n;
+  CK(cudaEventRecord(start, s->stream));
+  CK(cudaStreamWaitEvent(s->side, start, 0));
+  bool first = true;
+  for (int idx = 0; idx < s->grad_ncp; ++idx) {
+    const int c = s->grad_ncp - 1 - idx, bsel = idx & 1;
+    const int z0 = c * every, n = std::min(every, nt - z0);
+    T* cp = static_cast<T*>(s->grad_cp) + (size_t)c * se;
+    T* base = seg + bsel * buf - se;   // slot j (j >= 1) at base + j * se
+    // state j of the segment (step z0 + j): the checkpoint, then the slots
+    auto slot = [&](int j) -> T* { return j == 0 ? cp : base + (size_t)j * se; };
+    // recompute the segment, state j - 1 -> state j, fields only: the split
+    // passes run source -> destination, so nothing is copied
+    if (idx >= 2) CK(cudaStreamWaitEvent(s->side, adj_done[bsel], 0));
+    for (int j = 1; j <= n; ++j) {
+      T* src = slot(j - 1);
+      T* dst = slot(j);
+      State<T> st = make_state<T>(s, s->cur, s->cur);
+      st.iex = src; st.iey = src + vol; st.iez = src + 2 * vol;
+      st.ihx = src + 3 * vol; st.ihy = src + 4 * vol; st.ihz = src + 5 * vol;
+      st.oex = dst; st.oey = dst + vol; st.oez = dst + 2 * vol;
+      st.ohx = dst + 3 * vol; st.ohy = dst + 4 * vol; st.ohz = dst + 5 * vol;
+      st.ps = psi_view<T>(s, src + 6 * vol);
+      st.pd = psi_view<T>(s, dst + 6 * vol);
+      launch_shell_pass<T>(st, zero_t, z0 + j - 1, whole, true, s->side);
+      State<T> se2 = st;
+      se2.ihx = dst + 3 * vol; se2.ihy = dst + 4 * vol; se2.ihz = dst + 5 * vol;
+      launch_shell_pass<T>(se2, zero_t, z0 + j - 1, whole, false, s->side);
+    }
+    CK(cudaEventRecord(rec_done[bsel], s->side));
+    CK(cudaStreamWaitEvent(s->stream, rec_done[bsel], 0));
     for (int j = n - 1; j >= 0; --j) {
       State<T> st = make_state<T>(s, s->cur, s->cur);
-      T* sn = seg + (size_t)j * se;
-      T* sn1 = seg + (size_t)(j + 1) * se;
+      T* sn = slot(j);
+      T* sn1 = slot(j + 1);
       st.iex = sn; st.iey = sn + vol; st.iez = sn + 2 * vol;
       st.ihx = sn1 + 3 * vol; st.ihy = sn1 + 4 * vol; st.ihz = sn1 + 5 * vol;
       st.ps = psi_view<T>(s, sn1 + 6 * vol);
-      launch_adjoint_step<T>(st, a, z0 + j, s->stream);
+      if (first) launch_adjoint_first<T>(st, a, z0 + j, s->stream);
+      launch_adjoint_step<T>(st, a, z0 + j, first, s->stream);
+      first = false;
     }
-    CK(cudaGetLastError());
+    CK(cudaEventRecord(adj_done[bsel], s->stream));
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+      cleanup();
+      return fail(FDTD_ERR_CUDA, "adjoint sweep: %s", cudaGetErrorString(e));
+    }
   }
+  cudaError_t e = cudaStreamSynchronize(s->side);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  cleanup();
+  if (e != cudaSuccess) return fail(FDTD_ERR_CUDA, "adjoint sweep: %s", cudaGetErrorString(e));
+  int rc = set_step(s, nt);   // the fields still hold the forward solve's last state
+  if (rc) return rc;
   // the first nz_out planes of the gradients, without the row padding
   const size_t row = (size_t)s->g.nx * sizeof(double);
   const size_t spitch = (size_t)s->pitch * sizeof(double);
@@ -1141,7 +1192,7 @@ int fdtd_grad_backward(fdtd_sim* s, const double* dj_dre, const double* dj_dim, 
   if (!s->grad_forward_done || s->t != s->g.nt)
     return fail(FDTD_ERR_STATE, "run fdtd_grad_forward first (and no steps after it)");
   const size_t sb = (size_t)state_elems(s) * s->esz;
-  const int slots = s->grad_every + 1;
+  const int slots = 2 * s->grad_every;   // two buffers of states 1..every
   if (s->grad_seg == nullptr || s->grad_seg_slots != slots) {
     release(s, s->grad_seg);
     s->grad_seg = nullptr;

@@ -150,18 +150,6 @@ void launch_interior_ty(const State<T>& s, const InteriorBox& ib, cudaStream_t s
   k_fused_interior<T, TY><<<grd, blk, 0, st>>>(s, ib);
 }
 
-void add_box(ShellBoxes& bl, int x0, int x1, int y0, int y1, int z0, int z1) {
-  if (x0 >= x1 || y0 >= y1 || z0 >= z1) return;
-  ShellBox& b = bl.b[bl.n++];
-  b.x0 = x0; b.x1 = x1; b.y0 = y0; b.y1 = y1; b.z0 = z0; b.z1 = z1;
-  b.width = x1 - x0 >= 64 ? kLanes : 8;   // strips narrower than 64 cells: 32-cell tiles
-  b.gx = (x1 - x0 + b.width * kVec - 1) / (b.width * kVec);
-  const int rows = 128 / b.width;
-  b.gy = (y1 - y0 + rows - 1) / rows;
-  b.first = bl.total_blocks;
-  bl.total_blocks += b.gx * b.gy * (z1 - z0);
-}
-
 }  // namespace
 
 bool fused_supported_tile(int tile_x, int tile_y, int elem_bytes) {
@@ -196,7 +184,7 @@ FusedPlan make_fused_plan(int nx, int ny, int nz, int npml, int tfsf_z, int tile
   p.has_interior = m >= 1 && ib.xa < ib.xb && ib.ya < ib.yb && nzr > 0;
   ShellBoxes& bl = p.shell;
   if (!p.has_interior) {
-    add_box(bl, 0, nx, 0, ny, 0, nz);
+    add_shell_box(bl, 0, nx, 0, ny, 0, nz);
     return p;
   }
   int planes = 0;
@@ -225,15 +213,15 @@ FusedPlan make_fused_plan(int nx, int ny, int nz, int npml, int tfsf_z, int tile
   // interior range the y strips (whole rows) and the x strips
   int zc = 0;
   for (int k = 0; k < nzr; ++k) {
-    add_box(bl, 0, nx, 0, ny, zc, ib.z0[k]);
+    add_shell_box(bl, 0, nx, 0, ny, zc, ib.z0[k]);
     zc = ib.z1[k];
   }
-  add_box(bl, 0, nx, 0, ny, zc, nz);
+  add_shell_box(bl, 0, nx, 0, ny, zc, nz);
   for (int k = 0; k < nzr; ++k) {
-    add_box(bl, 0, nx, 0, ib.ya, ib.z0[k], ib.z1[k]);
-    add_box(bl, 0, nx, ib.yb, ny, ib.z0[k], ib.z1[k]);
-    add_box(bl, 0, ib.xa, ib.ya, ib.yb, ib.z0[k], ib.z1[k]);
-    add_box(bl, ib.xb, nx, ib.ya, ib.yb, ib.z0[k], ib.z1[k]);
+    add_shell_box(bl, 0, nx, 0, ib.ya, ib.z0[k], ib.z1[k]);
+    add_shell_box(bl, 0, nx, ib.yb, ny, ib.z0[k], ib.z1[k]);
+    add_shell_box(bl, 0, ib.xa, ib.ya, ib.yb, ib.z0[k], ib.z1[k]);
+    add_shell_box(bl, ib.xb, nx, ib.ya, ib.yb, ib.z0[k], ib.z1[k]);
   }
   return p;
 }

@@ -47,6 +47,10 @@ bool fused_supported_tile(int tile_x, int tile_y, int elem_bytes);
 template <class T>
 bool launch_fused_interior(const State<T>& s, const FusedPlan& p, int tile_y, cudaStream_t st);
 
+// Appends the box [x0, x1) x [y0, y1) x [z0, z1) to a box list, with the
+// row width (32, 16 or 8 lanes) that pads x the least.
+void add_shell_box(ShellBoxes& bl, int x0, int x1, int y0, int y1, int z0, int z1);
+
 // Split H pass (h_pass) or E pass over the shell boxes, from the State's
 // source pointers to its destination pointers.
 template <class T>
@@ -55,9 +59,13 @@ void launch_shell_pass(const State<T>& s, const int* tdev, int toff, const Shell
 
 // One transposed step (fdtd_adjoint.cu): s holds E^n in its source E
 // pointers, H^{n+1/2} in its source H pointers and the CPML auxiliaries
-// after the step in ps; t is the step index n.
+// after the step in ps; t is the step index n; `first` marks the first
+// step of the backward sweep (t = size_t - 1), which launch_adjoint_first
+// (the E phasor source of that step) must precede.
 template <class T>
-void launch_adjoint_step(const State<T>& s, const Adj<T>& a, int t, cudaStream_t st);
+void launch_adjoint_first(const State<T>& s, const Adj<T>& a, int t, cudaStream_t st);
+template <class T>
+void launch_adjoint_step(const State<T>& s, const Adj<T>& a, int t, bool first, cudaStream_t st);
 
 // Records an error message for fdtd_last_error(); returns code.
 int report_error(int code, const char* msg);

@@ -10,6 +10,8 @@
 // faces, domain edges, the injection plane) h_vec / e_vec. The same passes,
 // restricted to a list of boxes and run source -> destination, update the
 // shell of the fused step (fdtd_fused.cu).
+#include <cstring>
+
 #include "fdtd_launch.h"
 #include "fdtd_vec.cuh"
 
@@ -93,24 +95,8 @@ __device__ __forceinline__ void e_split_vec(const State<T>& s, int t, int z, int
   st4(s.oex + i, ex); st4(s.oey + i, ey); st4(s.oez + i, ez);
 }
 
-// In-place split step over the whole grid. Block (32, 4): a warp covers
-// 128 consecutive x cells of one row; blockIdx.z is the plane.
-template <class T>
-__global__ void __launch_bounds__(128) k_h_split(State<T> s, const int* __restrict__ tp, int toff) {
-  const int x0 = (blockIdx.x * 32 + threadIdx.x) * kVec;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  h_split_vec(s, *tp + toff, (int)blockIdx.z, y, x0, (int)threadIdx.x, 32, true);
-}
-
-template <class T>
-__global__ void __launch_bounds__(128) k_e_split(State<T> s, const int* __restrict__ tp, int toff) {
-  const int x0 = (blockIdx.x * 32 + threadIdx.x) * kVec;
-  const int y = blockIdx.y * blockDim.y + threadIdx.y;
-  e_split_vec(s, *tp + toff, (int)blockIdx.z, y, x0, (int)threadIdx.x, 32, true);
-}
-
-// The same passes over a list of boxes (the shell of the fused step), one
-// plane of one box tile per 128-thread block. A box tile is `width` lanes
+// The passes over a list of boxes (the whole grid for the split step, the
+// shell of the fused step), one plane of one box tile per 128-thread block. A box tile is `width` lanes
 // (width * kVec x cells) by 128 / width rows.
 __device__ __forceinline__ const ShellBox& find_box(const ShellBoxes& bl, int bid) {
   int k = 0;
@@ -311,12 +297,30 @@ __global__ void k_eps_sigma(int nx, int ny, int nz, int nz_mat, int pitch,
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
+void add_shell_box(ShellBoxes& bl, int x0, int x1, int y0, int y1, int z0, int z1) {
+  if (x0 >= x1 || y0 >= y1 || z0 >= z1 || bl.n >= kMaxShellBoxes) return;
+  ShellBox& b = bl.b[bl.n++];
+  b.x0 = x0; b.x1 = x1; b.y0 = y0; b.y1 = y1; b.z0 = z0; b.z1 = z1;
+  // row width with the least x padding (ties: the wider rows)
+  long long best = -1;
+  for (int w : {32, 16, 8}) {
+    const long long gx = (x1 - x0 + 4 * w - 1) / (4 * w), gy = (y1 - y0 + 128 / w - 1) / (128 / w);
+    const long long padded = gx * 4 * w * gy * (128 / w);
+    if (best < 0 || padded < best) { best = padded; b.width = w; }
+  }
+  b.gx = (x1 - x0 + b.width * kVec - 1) / (b.width * kVec);
+  b.gy = (y1 - y0 + 128 / b.width - 1) / (128 / b.width);
+  b.first = bl.total_blocks;
+  bl.total_blocks += b.gx * b.gy * (z1 - z0);
+}
+
 template <class T>
 void launch_split_step(const State<T>& s, const int* tdev, int toff, cudaStream_t st) {
-  const dim3 blk(32, 4, 1);
-  const dim3 grd((s.nx + 32 * kVec - 1) / (32 * kVec), (s.ny + 3) / 4, s.nz);
-  k_h_split<T><<<grd, blk, 0, st>>>(s, tdev, toff);
-  k_e_split<T><<<grd, blk, 0, st>>>(s, tdev, toff);
+  ShellBoxes whole;
+  memset(&whole, 0, sizeof(whole));
+  add_shell_box(whole, 0, s.nx, 0, s.ny, 0, s.nz);
+  launch_shell_pass<T>(s, tdev, toff, whole, true, st);
+  launch_shell_pass<T>(s, tdev, toff, whole, false, st);
 }
 
 template <class T>

@@ -118,10 +118,11 @@ class BackscatterGradient:
         self.params = params
         g = params.geom_params
         self.every = int(checkpoint_every)
-        self.sim = _native.NativeSim(native_geometry(params), device)
+        from . import tuning
+        geom = native_geometry(params)
+        self.sim = _native.NativeSim(geom, device)
         self.sim.set_absorbers(packed_profiles(params))
-        if kernel is not None:
-            self.sim.set_option(_native.OPT_KERNEL, int(kernel))
+        tuning.apply(self.sim, tuning.choose(geom, kernel=kernel, device=device))
         self.sim.set_incident(incident['ex'], incident['ey'], incident['hx'], incident['hy'])
         theta = -params.inc_beam_params.theta_angle if theta_deg is None else theta_deg
         pol = params.inc_beam_params.polarization if pol is None else pol

@@ -76,11 +76,8 @@ class MainSimGpu:
 
     def _configure(self, kernel, tile):
         from .. import tuning
-        choice = tuning.choose(self.geom, kernel=kernel, tile=tile)
-        self.native.set_option(_native.OPT_KERNEL, choice['kernel'])
-        if choice['kernel'] == _native.FDTD_KERNEL_FUSED:
-            self.native.set_option(_native.OPT_TILE_X, choice['tile_x'])
-            self.native.set_option(_native.OPT_TILE_Y, choice['tile_y'])
+        choice = tuning.choose(self.geom, kernel=kernel, tile=tile, device=self.gpu_num)
+        tuning.apply(self.native, choice)
         self.kernel_choice = choice
 
     # -- incident beam ----------------------------------------------------
