@@ -150,8 +150,8 @@ __device__ __forceinline__ void phasor_h_src(const State<T>& s, const Adj<T>& a,
 // by k_adj_k2 of the step after them)
 template <class T>
 __global__ void k_adj_phasor_e(const __grid_constant__ State<T> s, Adj<T> a, int t) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
-  if (x >= s.nx) return;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= s.nx || y >= s.ny) return;
   const int z = s.nz - s.npml - 1;
   T dex, dey;
   phasor_e_src(s, a, t, z, y, x, dex, dey);
@@ -414,13 +414,28 @@ __device__ __forceinline__ void h_own_part(const State<T>& s, const Adj<T>& a, i
 template <class T>
 __global__ void __launch_bounds__(128) k_adj_k1(const __grid_constant__ State<T> s, Adj<T> a, int t,
                                                 int first) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y, z = blockIdx.z;
-  if (x >= s.nx) return;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  if (x >= s.nx || y >= s.ny) return;
   const long long i = idx(s, z, y, x);
   const T lhx = a.lhx[i], lhy = a.lhy[i], lhz = a.lhz[i];
-  if (!first) h_own_part(s, a, z, y, x, lhx, lhy, lhz);
+  const int m = s.npml;
   T dhx, dhy, dhz, phx, phy;
-  e_to_h_terms(s, a, z, y, x, dhx, dhy, dhz);
+  if (z >= m && z < s.nz - m - 1 && y >= m && y < s.ny - m - 1 && x >= m && x < s.nx - m - 1) {
+    // the cell and its +x, +y, +z neighbours are away from every CPML face
+    // and domain edge: the plain transposed curl
+    const long long P = s.plane, W = s.pitch;
+    const T fx = s.cb[i] * a.lex[i], fy = s.cb[i] * a.ley[i], fz = s.cb[i] * a.lez[i];
+    const T fy_z = s.cb[i + P] * a.ley[i + P], fx_z = s.cb[i + P] * a.lex[i + P];
+    const T fz_y = s.cb[i + W] * a.lez[i + W], fx_y = s.cb[i + W] * a.lex[i + W];
+    const T fz_x = s.cb[i + 1] * a.lez[i + 1], fy_x = s.cb[i + 1] * a.ley[i + 1];
+    dhx = (fy - fy_z) - (fz - fz_y);
+    dhy = (fz - fz_x) - (fx - fx_z);
+    dhz = (fx - fx_y) - (fy - fy_x);
+  } else {
+    if (!first) h_own_part(s, a, z, y, x, lhx, lhy, lhz);
+    e_to_h_terms(s, a, z, y, x, dhx, dhy, dhz);
+  }
   phasor_h_src(s, a, t, z, y, x, phx, phy);
   // components outside their update range keep a zero adjoint (e_own_part)
   a.lhx[i] = rh_x(s, z, y, x) ? lhx + dhx + phx : T(0);
@@ -434,28 +449,57 @@ __global__ void __launch_bounds__(128) k_adj_k1(const __grid_constant__ State<T>
 template <class T>
 __global__ void __launch_bounds__(128) k_adj_k2(const __grid_constant__ State<T> s, Adj<T> a,
                                                 int t_prev) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y, z = blockIdx.z;
-  if (x >= s.nx) return;
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int z = blockIdx.z;
+  if (x >= s.nx || y >= s.ny) return;
   const long long i = idx(s, z, y, x);
+  const int m = s.npml;
   T ex, ey, ez, dex, dey, dez, pex = T(0), pey = T(0);
-  e_own_part(s, a, z, y, x, ex, ey, ez);
-  h_to_e_terms(s, a, z, y, x, dex, dey, dez);
+  if (z >= m && z < s.nz - m && y >= m && y < s.ny - m && x >= m && x < s.nx - m) {
+    // the cell and its -x, -y, -z neighbours are away from every CPML face
+    // and domain edge
+    const long long P = s.plane, W = s.pitch;
+    const T lx = a.lex[i], ly = a.ley[i], lz = a.lez[i];
+    if (z < a.nz_grad) {
+      const T* hx = s.ihx; const T* hy = s.ihy; const T* hz = s.ihz;
+      a.gca[i] += (double)lx * (double)s.iex[i] + (double)ly * (double)s.iey[i] +
+                  (double)lz * (double)s.iez[i];
+      a.gcb[i] += (double)lx * (double)((hz[i] - hz[i - W]) - (hy[i] - hy[i - P])) +
+                  (double)ly * (double)((hx[i] - hx[i - P]) - (hz[i] - hz[i - 1])) +
+                  (double)lz * (double)((hy[i] - hy[i - 1]) - (hx[i] - hx[i - W]));
+    }
+    const T ca = s.ca[i], db = s.db;
+    ex = ca * lx;
+    ey = ca * ly;
+    ez = ca * lz;
+    const T gx = db * a.lhx[i], gy = db * a.lhy[i], gz = db * a.lhz[i];
+    const T gy_z = db * a.lhy[i - P], gx_z = db * a.lhx[i - P];
+    const T gz_y = db * a.lhz[i - W], gx_y = db * a.lhx[i - W];
+    const T gz_x = db * a.lhz[i - 1], gy_x = db * a.lhy[i - 1];
+    dex = (gy - gy_z) - (gz - gz_y);
+    dey = (gz - gz_x) - (gx - gx_z);
+    dez = (gx - gx_y) - (gy - gy_x);
+  } else {
+    e_own_part(s, a, z, y, x, ex, ey, ez);
+    h_to_e_terms(s, a, z, y, x, dex, dey, dez);
+  }
   if (t_prev >= 0) phasor_e_src(s, a, t_prev, z, y, x, pex, pey);
   a.lex[i] = re_x(s, z, y, x) ? ex + dex + pex : T(0);
   a.ley[i] = re_y(s, z, y, x) ? ey + dey + pey : T(0);
   a.lez[i] = re_z(s, z, y, x) ? ez + dez : T(0);
 }
 
+// 32 x 4 cells per block: little x padding on grids a few hundred cells wide
 template <class T>
 void launch_adjoint_first(const State<T>& s, const Adj<T>& a, int t, cudaStream_t st) {
-  k_adj_phasor_e<T><<<dim3((s.nx + 127) / 128, s.ny, 1), 128, 0, st>>>(s, a, t);
+  k_adj_phasor_e<T><<<dim3((s.nx + 31) / 32, (s.ny + 3) / 4, 1), dim3(32, 4, 1), 0, st>>>(s, a, t);
 }
 
 template <class T>
 void launch_adjoint_step(const State<T>& s, const Adj<T>& a, int t, bool first, cudaStream_t st) {
-  const dim3 grd((s.nx + 127) / 128, s.ny, s.nz);
-  k_adj_k1<T><<<grd, 128, 0, st>>>(s, a, t, first ? 1 : 0);
-  k_adj_k2<T><<<grd, 128, 0, st>>>(s, a, t - 1);
+  const dim3 grd((s.nx + 31) / 32, (s.ny + 3) / 4, s.nz), blk(32, 4, 1);
+  k_adj_k1<T><<<grd, blk, 0, st>>>(s, a, t, first ? 1 : 0);
+  k_adj_k2<T><<<grd, blk, 0, st>>>(s, a, t - 1);
 }
 
 template void launch_adjoint_first<float>(const State<float>&, const Adj<float>&, int, cudaStream_t);
