@@ -49,7 +49,7 @@ def parse():
     ap.add_argument('--dtype', default='float32', choices=['float32', 'float64'])
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-cpu-baseline', action='store_true')
-    ap.add_argument('--cpu-steps', type=int, default=2)
+    ap.add_argument('--cpu-steps', type=int, default=4)
     return ap.parse_args()
 
 
@@ -171,23 +171,38 @@ def committed_traffic(kernel_name, workload):
 # CPU baseline (the oracle: CPU restatement of the reference's algorithm)
 # ---------------------------------------------------------------------------
 def cpu_baseline(pc, ca, cb, inc, steps):
+    """The oracle (CPU restatement of the reference's step) on the host: the
+    C restatement on every host core when it is built (make -C oracle), else
+    the numpy oracle on one core. `steps` full-grid steps after one untimed
+    step (first touch of every array)."""
     sys.path.insert(0, os.path.join(ROOT, 'oracle'))
     import fdtd_oracle as O
     from fdtdsarsim_b200.absorbers import cpml_profiles
     g = pc.geom_params
-    sim = O.OracleSim(g.size_x, g.size_y, g.size_z, g.size_pml, g.tfsf_z, g.cell_size,
-                      g.timestep, pc.inc_beam_params.frequency, pc.processing_params.datatype,
-                      cpml_profiles(pc))
+    args = (g.size_x, g.size_y, g.size_z, g.size_pml, g.tfsf_z, g.cell_size, g.timestep,
+            pc.inc_beam_params.frequency, pc.processing_params.datatype, cpml_profiles(pc))
+    try:
+        import fdtd_oracle_c as OC
+        if not OC.available():
+            subprocess.run(['make', '-C', os.path.join(ROOT, 'oracle')], check=True,
+                           capture_output=True)
+        cores = os.cpu_count() or 1
+        sim = OC.COracleSim(*args, nthreads=cores)
+        what = f'C oracle, {cores} threads'
+    except Exception:   # no compiler on the host: the numpy oracle
+        cores = 1
+        sim = O.OracleSim(*args)
+        what = 'numpy oracle, one thread'
     sim.step(ca, cb, inc)  # first-touch of every array, untimed
     t0 = time.perf_counter()
     for _ in range(steps):
         sim.step(ca, cb, inc)
     dt = time.perf_counter() - t0
     cells = g.size_x * g.size_y * g.size_z
-    return {'value': cells * steps / dt / 1e6, 'unit': 'Mcell-updates/s', 'cores': 1,
+    return {'value': cells * steps / dt / 1e6, 'unit': 'Mcell-updates/s', 'cores': cores,
             'kind': 'port',
             'sample': f'{steps} time steps of the full {g.size_z}x{g.size_y}x{g.size_x} grid '
-                      f'(numpy oracle, one thread), after one untimed step'}
+                      f'({what}), after one untimed step'}
 
 
 # ---------------------------------------------------------------------------
