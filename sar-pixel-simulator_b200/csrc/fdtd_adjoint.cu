@@ -27,6 +27,7 @@
 // k_adj_k1 = f of step n + 1, b, d; k_adj_k2 = c, e, a of step n - 1; only
 // the first backward step needs a on its own (k_adj_phasor_e).
 #include "fdtd_launch.h"
+#include "fdtd_vec.cuh"
 
 namespace fdtd {
 
@@ -160,137 +161,465 @@ __global__ void k_adj_phasor_e(const __grid_constant__ State<T> s, Adj<T> a, int
   if (re_y(s, z, y, x)) a.ley[i] += dey;
 }
 
-// ---- 2: lambda_H += (E update + E CPML)^T lambda_E ----------------------------
+// ---- vector form ------------------------------------------------------------
+// A thread owns four consecutive x cells of one row (x0 a multiple of 4;
+// the pitch is a multiple of 32 elements, so the four cells are one aligned
+// vector in every (.., pitch)-strided array, as in the forward step). z- and
+// y-face auxiliaries have coefficients uniform over the vector; x-face
+// auxiliaries ((z, y, npml) layout) run per cell.
+
+// main-update ranges of the E components of the vector's cells
 template <class T>
-__device__ __forceinline__ void e_to_h_terms(const State<T>& s, const Adj<T>& a, int z, int y, int x,
-                                             T& out_hx, T& out_hy, T& out_hz) {
-  const int nx = s.nx, ny = s.ny, nz = s.nz, m = s.npml;
-  // F = Cb lambda_E on each component's update range
-  auto Fx = [&](int zz, int yy, int xx) -> T {
-    if (zz >= nz || yy >= ny || xx >= nx || !re_x(s, zz, yy, xx)) return T(0);
-    const long long j = idx(s, zz, yy, xx);
-    return s.cb[j] * a.lex[j];
-  };
-  auto Fy = [&](int zz, int yy, int xx) -> T {
-    if (zz >= nz || yy >= ny || xx >= nx || !re_y(s, zz, yy, xx)) return T(0);
-    const long long j = idx(s, zz, yy, xx);
-    return s.cb[j] * a.ley[j];
-  };
-  auto Fz = [&](int zz, int yy, int xx) -> T {
-    if (zz >= nz || yy >= ny || xx >= nx || !re_z(s, zz, yy, xx)) return T(0);
-    const long long j = idx(s, zz, yy, xx);
-    return s.cb[j] * a.lez[j];
-  };
-  const T fx = Fx(z, y, x), fy = Fy(z, y, x), fz = Fz(z, y, x);
-  T dhx = (fy - Fy(z + 1, y, x)) - (fz - Fz(z, y + 1, x));
-  T dhy = (fz - Fz(z, y, x + 1)) - (fx - Fx(z + 1, y, x));
-  T dhz = (fx - Fx(z, y + 1, x)) - (fy - Fy(z, y, x + 1));
-  const T rdx = T(1) / s.dx;
-  // E-face auxiliaries at (zz, yy, xx): coefficient c/dx times their total
-  // adjoint, for the face normal to `axis`, auxiliary slot `slot`
-  auto face_term = [&](int axis, int slot, int zz, int yy, int xx) -> T {
-    if (zz >= nz || yy >= ny || xx >= nx || !box(s, zz, yy, xx)) return T(0);
-    int side, q;
-    long long k;
-    const T* lp;
-    const T* lc;
-    T sign;
-    if (axis == 0) {
-      if (!e_face(zz, nz, m, side, q)) return T(0);
-      k = kz(s, q, yy, xx);
-      lp = a.lps.z[side][slot];
-      lc = slot == 1 ? a.ley : a.lex;
-      sign = slot == 1 ? T(1) : T(-1);
-    } else if (axis == 1) {
-      if (!e_face(xx, nx, m, side, q)) return T(0);
-      k = kx(s, zz, yy, q);
-      lp = a.lps.x[side][slot];
-      lc = slot == 1 ? a.lez : a.ley;
-      sign = slot == 1 ? T(1) : T(-1);
-    } else {
-      if (!e_face(yy, ny, m, side, q)) return T(0);
-      k = ky(s, zz, q, xx);
-      lp = a.lps.y[side][slot];
-      lc = slot == 0 ? a.lex : a.lez;
-      sign = slot == 0 ? T(1) : T(-1);
-    }
-    const long long j = idx(s, zz, yy, xx);
-    const T c = s.prof[side ? CE_U : CE_D][q];
-    return c * rdx * (lp[k] + sign * s.cb[j] * s.dx * lc[j]);
-  };
-  // z faces: Eyz uses hx(c) - hx(c - z), Exz uses hy(c) - hy(c - z)
-  dhx += face_term(0, 1, z, y, x) - face_term(0, 1, z + 1, y, x);
-  dhy += face_term(0, 0, z, y, x) - face_term(0, 0, z + 1, y, x);
-  // x faces: Ezx uses hy(c) - hy(c - x), Eyx uses hz(c) - hz(c - x)
-  dhy += face_term(1, 1, z, y, x) - face_term(1, 1, z, y, x + 1);
-  dhz += face_term(1, 0, z, y, x) - face_term(1, 0, z, y, x + 1);
-  // y faces: Exy uses hz(c) - hz(c - y), Ezy uses hx(c) - hx(c - y)
-  dhz += face_term(2, 0, z, y, x) - face_term(2, 0, z, y + 1, x);
-  dhx += face_term(2, 1, z, y, x) - face_term(2, 1, z, y + 1, x);
-  out_hx = dhx;
-  out_hy = dhy;
-  out_hz = dhz;
+__device__ __forceinline__ void e_ranges(const State<T>& s, int z, int y, int x0, bool (&rx)[kVec],
+                                         bool (&ry)[kVec], bool (&rz)[kVec]) {
+  const bool zi = z >= 1 && z < s.nz - 1, yi = y >= 1 && y < s.ny - 1;
+  const bool zb = z >= 0 && z < s.nz - 1, yb = y >= 0 && y < s.ny - 1;
+#pragma unroll
+  for (int j = 0; j < kVec; ++j) {
+    const int x = x0 + j;
+    const bool xb = x < s.nx - 1, xi = x >= 1 && x < s.nx - 1;
+    rx[j] = zi && yi && xb;
+    ry[j] = zi && yb && xi;
+    rz[j] = zb && yi && xi;
+  }
 }
 
-// ---- 3: gradients, E auxiliaries' adjoint, Ca lambda_E --------------------
-// s.iex.. hold E^n, s.ihx.. H^{n+1/2}, s.ps the auxiliaries after the step.
-// Returns Ca lambda_E of the cell (zero outside the update ranges).
+// and of the H components
 template <class T>
-__device__ __forceinline__ void e_own_part(const State<T>& s, const Adj<T>& a, int z, int y, int x,
-                                           T& out_x, T& out_y, T& out_z) {
+__device__ __forceinline__ void h_ranges(const State<T>& s, int z, int y, int x0, bool (&rx)[kVec],
+                                         bool (&ry)[kVec], bool (&rz)[kVec]) {
+  const bool zi = z >= 1 && z < s.nz - 1, yi = y >= 1 && y < s.ny - 1;
+  const bool zb = z >= 0 && z < s.nz - 1, yb = y >= 0 && y < s.ny - 1;
+#pragma unroll
+  for (int j = 0; j < kVec; ++j) {
+    const int x = x0 + j;
+    const bool xb = x < s.nx - 1, xi = x >= 1 && x < s.nx - 1;
+    rx[j] = zb && yb && xi;
+    ry[j] = zb && yi && xb;
+    rz[j] = zi && yb && xb;
+  }
+}
+
+// F = Cb lambda_E of one component where `r` holds
+template <class T>
+__device__ __forceinline__ void masked_prod(T (&f)[kVec], const T (&cb)[kVec], const T (&l)[kVec],
+                                            const bool (&r)[kVec]) {
+#pragma unroll
+  for (int j = 0; j < kVec; ++j) f[j] = r[j] ? cb[j] * l[j] : T(0);
+}
+
+// E-face auxiliaries of plane zz (z faces) or row yy (y faces): c/dx times
+// their total adjoint lambda_psi + sign Cb dx lambda_E, zero off the faces
+// and outside the box. With F = Cb lambda_E of the two components involved.
+// z faces: t0 Exz (F = fx, sign -), t1 Eyz (fy, +).
+template <class T>
+__device__ __forceinline__ void e_zface(const State<T>& s, const Adj<T>& a, int zz, int y, int x0,
+                                        const T (&fx)[kVec], const T (&fy)[kVec], T (&t0)[kVec],
+                                        T (&t1)[kVec]) {
+  zero4(t0);
+  zero4(t1);
+  int side, q;
+  if (zz >= s.nz - 1 || y >= s.ny - 1 || !e_face(zz, s.nz, s.npml, side, q)) return;
+  const long long k = kz(s, q, y, x0);
+  const T c = s.prof[side ? CE_U : CE_D][q] * s.rdx;
+  T p0[kVec], p1[kVec];
+  ld4(p0, a.lps.z[side][0] + k);
+  ld4(p1, a.lps.z[side][1] + k);
+#pragma unroll
+  for (int j = 0; j < kVec; ++j) {
+    if (x0 + j >= s.nx - 1) continue;
+    t0[j] = c * (p0[j] - s.dx * fx[j]);
+    t1[j] = c * (p1[j] + s.dx * fy[j]);
+  }
+}
+
+// y faces: t0 Exy (F = fx, sign +), t1 Ezy (fz, -).
+template <class T>
+__device__ __forceinline__ void e_yface(const State<T>& s, const Adj<T>& a, int z, int yy, int x0,
+                                        const T (&fx)[kVec], const T (&fz)[kVec], T (&t0)[kVec],
+                                        T (&t1)[kVec]) {
+  zero4(t0);
+  zero4(t1);
+  int side, q;
+  if (z >= s.nz - 1 || yy >= s.ny - 1 || !e_face(yy, s.ny, s.npml, side, q)) return;
+  const long long k = ky(s, z, q, x0);
+  const T c = s.prof[side ? CE_U : CE_D][q] * s.rdx;
+  T p0[kVec], p1[kVec];
+  ld4(p0, a.lps.y[side][0] + k);
+  ld4(p1, a.lps.y[side][1] + k);
+#pragma unroll
+  for (int j = 0; j < kVec; ++j) {
+    if (x0 + j >= s.nx - 1) continue;
+    t0[j] = c * (p0[j] + s.dx * fx[j]);
+    t1[j] = c * (p1[j] - s.dx * fz[j]);
+  }
+}
+
+// H-face auxiliaries: c/dx times lambda_psi + sign dtm0 lambda_H.
+// z faces: t2 Hxz (lhx, +), t3 Hyz (lhy, -).
+template <class T>
+__device__ __forceinline__ void h_zface(const State<T>& s, const Adj<T>& a, int zz, int y, int x0,
+                                        const T (&lx)[kVec], const T (&ly)[kVec], T (&t2)[kVec],
+                                        T (&t3)[kVec]) {
+  zero4(t2);
+  zero4(t3);
+  int side, q;
+  if (zz < 0 || zz >= s.nz - 1 || y >= s.ny - 1 || !h_face(zz, s.nz, s.npml, side, q)) return;
+  const long long k = kz(s, q, y, x0);
+  const T c = s.prof[side ? CH_U : CH_D][q] * s.rdx;
+  T p2[kVec], p3[kVec];
+  ld4(p2, a.lps.z[side][2] + k);
+  ld4(p3, a.lps.z[side][3] + k);
+#pragma unroll
+  for (int j = 0; j < kVec; ++j) {
+    if (x0 + j >= s.nx - 1) continue;
+    t2[j] = c * (p2[j] + s.dtm0 * lx[j]);
+    t3[j] = c * (p3[j] - s.dtm0 * ly[j]);
+  }
+}
+
+// y faces: t2 Hxy (lhx, -), t3 Hzy (lhz, +).
+template <class T>
+__device__ __forceinline__ void h_yface(const State<T>& s, const Adj<T>& a, int z, int yy, int x0,
+                                        const T (&lx)[kVec], const T (&lz)[kVec], T (&t2)[kVec],
+                                        T (&t3)[kVec]) {
+  zero4(t2);
+  zero4(t3);
+  int side, q;
+  if (yy < 0 || z >= s.nz - 1 || yy >= s.ny - 1 || !h_face(yy, s.ny, s.npml, side, q)) return;
+  const long long k = ky(s, z, q, x0);
+  const T c = s.prof[side ? CH_U : CH_D][q] * s.rdx;
+  T p2[kVec], p3[kVec];
+  ld4(p2, a.lps.y[side][2] + k);
+  ld4(p3, a.lps.y[side][3] + k);
+#pragma unroll
+  for (int j = 0; j < kVec; ++j) {
+    if (x0 + j >= s.nx - 1) continue;
+    t2[j] = c * (p2[j] - s.dtm0 * lx[j]);
+    t3[j] = c * (p3[j] + s.dtm0 * lz[j]);
+  }
+}
+
+// H auxiliaries' adjoint (f) of the vector, from its lambda_H:
+// lambda_psi = bh (lambda_psi + sign dtm0 lambda_H) on every H face.
+template <class T>
+__device__ __forceinline__ void h_own_vec(const State<T>& s, const Adj<T>& a, int z, int y, int x0,
+                                          const T (&lhx)[kVec], const T (&lhy)[kVec],
+                                          const T (&lhz)[kVec]) {
   const int nx = s.nx, ny = s.ny, nz = s.nz, m = s.npml;
-  const long long P = s.plane, W = s.pitch;
-  const long long i = idx(s, z, y, x);
-  const T lx = a.lex[i], ly = a.ley[i], lz = a.lez[i];
-  const T cb = s.cb[i], ca = s.ca[i];
-  double gca = 0.0, gcb = 0.0;
-  const T* hx = s.ihx; const T* hy = s.ihy; const T* hz = s.ihz;
-  const bool grad = z < a.nz_grad;   // gradients only over the requested planes
-  if (grad && re_x(s, z, y, x)) {
-    gca += (double)lx * (double)s.iex[i];
-    gcb += (double)lx * (double)((hz[i] - hz[i - W]) - (hy[i] - hy[i - P]));
-  }
-  if (grad && re_y(s, z, y, x)) {
-    gca += (double)ly * (double)s.iey[i];
-    gcb += (double)ly * (double)((hx[i] - hx[i - P]) - (hz[i] - hz[i - 1]));
-  }
-  if (grad && re_z(s, z, y, x)) {
-    gca += (double)lz * (double)s.iez[i];
-    gcb += (double)lz * (double)((hy[i] - hy[i - 1]) - (hx[i] - hx[i - W]));
-  }
-  if (box(s, z, y, x)) {
-    int side, q;
-    if (e_face(z, nz, m, side, q)) {
-      const long long k = kz(s, q, y, x);
-      const T b = s.prof[side ? BE_U : BE_D][q];
-      T* p1 = a.lps.z[side][1];
-      T* p0 = a.lps.z[side][0];
-      if (grad) gcb += (double)s.dx * ((double)s.ps.z[side][1][k] * ly - (double)s.ps.z[side][0][k] * lx);
-      p1[k] = b * (p1[k] + cb * s.dx * ly);
-      p0[k] = b * (p0[k] - cb * s.dx * lx);
+  if (z >= nz - 1 || y >= ny - 1) return;
+  int side, q;
+  if (h_face(z, nz, m, side, q)) {
+    const long long k = kz(s, q, y, x0);
+    const T b = s.prof[side ? BH_U : BH_D][q];
+    T p2[kVec], p3[kVec];
+    ld4(p2, a.lps.z[side][2] + k);
+    ld4(p3, a.lps.z[side][3] + k);
+#pragma unroll
+    for (int j = 0; j < kVec; ++j) {
+      if (x0 + j >= nx - 1) continue;
+      p3[j] = b * (p3[j] - s.dtm0 * lhy[j]);
+      p2[j] = b * (p2[j] + s.dtm0 * lhx[j]);
     }
-    if (e_face(x, nx, m, side, q)) {
+    st4(a.lps.z[side][2] + k, p2);
+    st4(a.lps.z[side][3] + k, p3);
+  }
+  if (x0 < m - 1 || x0 + kVec - 1 >= nx - m) {
+#pragma unroll
+    for (int j = 0; j < kVec; ++j) {
+      const int x = x0 + j;
+      if (x >= nx - 1 || !h_face(x, nx, m, side, q)) continue;
       const long long k = kx(s, z, y, q);
-      const T b = s.prof[side ? BE_U : BE_D][q];
-      T* p1 = a.lps.x[side][1];
-      T* p0 = a.lps.x[side][0];
-      if (grad) gcb += (double)s.dx * ((double)s.ps.x[side][1][k] * lz - (double)s.ps.x[side][0][k] * ly);
-      p1[k] = b * (p1[k] + cb * s.dx * lz);
-      p0[k] = b * (p0[k] - cb * s.dx * ly);
+      const T b = s.prof[side ? BH_U : BH_D][q];
+      T* p3 = a.lps.x[side][3];
+      T* p2 = a.lps.x[side][2];
+      p3[k] = b * (p3[k] - s.dtm0 * lhz[j]);
+      p2[k] = b * (p2[k] + s.dtm0 * lhy[j]);
     }
-    if (e_face(y, ny, m, side, q)) {
-      const long long k = ky(s, z, q, x);
-      const T b = s.prof[side ? BE_U : BE_D][q];
-      T* p0 = a.lps.y[side][0];
-      T* p1 = a.lps.y[side][1];
-      if (grad) gcb += (double)s.dx * ((double)s.ps.y[side][0][k] * lx - (double)s.ps.y[side][1][k] * lz);
-      p0[k] = b * (p0[k] + cb * s.dx * lx);
-      p1[k] = b * (p1[k] - cb * s.dx * lz);
+  }
+  if (h_face(y, ny, m, side, q)) {
+    const long long k = ky(s, z, q, x0);
+    const T b = s.prof[side ? BH_U : BH_D][q];
+    T p2[kVec], p3[kVec];
+    ld4(p2, a.lps.y[side][2] + k);
+    ld4(p3, a.lps.y[side][3] + k);
+#pragma unroll
+    for (int j = 0; j < kVec; ++j) {
+      if (x0 + j >= nx - 1) continue;
+      p2[j] = b * (p2[j] - s.dtm0 * lhx[j]);
+      p3[j] = b * (p3[j] + s.dtm0 * lhz[j]);
+    }
+    st4(a.lps.y[side][2] + k, p2);
+    st4(a.lps.y[side][3] + k, p3);
+  }
+}
+
+// (b) lambda_H increments of the vector: the transposed curl of
+// F = Cb lambda_E (backward differences of F: the forward E update of the
+// cell and of its +x, +y, +z neighbours reads H of this cell) and the E-face
+// auxiliaries of the cell and of those neighbours. `fast`: the vector and
+// every neighbour it reads lie away from every CPML face and domain edge.
+template <class T, bool kFast>
+__device__ __forceinline__ void e_to_h_vec(const State<T>& s, const Adj<T>& a, int z, int y, int x0,
+                                           T (&dhx)[kVec], T (&dhy)[kVec], T (&dhz)[kVec]) {
+  const int nx = s.nx, ny = s.ny, nz = s.nz, m = s.npml;
+  const long long P = s.plane, W = s.pitch, i = idx(s, z, y, x0);
+  T cb[kVec], l0[kVec], l1[kVec], l2[kVec];
+  T fx[kVec], fy[kVec], fz[kVec];       // cell
+  T fxz[kVec], fyz[kVec];               // z + 1
+  T fxy[kVec], fzy[kVec];               // y + 1
+  T fyn = T(0), fzn = T(0);             // x0 + 4
+  ld4(cb, s.cb + i);
+  ld4(l0, a.lex + i);
+  ld4(l1, a.ley + i);
+  ld4(l2, a.lez + i);
+  if constexpr (kFast) {
+#pragma unroll
+    for (int j = 0; j < kVec; ++j) {
+      fx[j] = cb[j] * l0[j];
+      fy[j] = cb[j] * l1[j];
+      fz[j] = cb[j] * l2[j];
+    }
+    ld4(cb, s.cb + i + P);
+    ld4(l0, a.lex + i + P);
+    ld4(l1, a.ley + i + P);
+#pragma unroll
+    for (int j = 0; j < kVec; ++j) {
+      fxz[j] = cb[j] * l0[j];
+      fyz[j] = cb[j] * l1[j];
+    }
+    ld4(cb, s.cb + i + W);
+    ld4(l0, a.lex + i + W);
+    ld4(l2, a.lez + i + W);
+#pragma unroll
+    for (int j = 0; j < kVec; ++j) {
+      fxy[j] = cb[j] * l0[j];
+      fzy[j] = cb[j] * l2[j];
+    }
+    const T cbn = s.cb[i + kVec];
+    fyn = cbn * a.ley[i + kVec];
+    fzn = cbn * a.lez[i + kVec];
+  } else {
+    bool rx[kVec], ry[kVec], rz[kVec];
+    e_ranges(s, z, y, x0, rx, ry, rz);
+    masked_prod(fx, cb, l0, rx);
+    masked_prod(fy, cb, l1, ry);
+    masked_prod(fz, cb, l2, rz);
+    zero4(fxz);
+    zero4(fyz);
+    if (z + 1 < nz - 1) {
+      e_ranges(s, z + 1, y, x0, rx, ry, rz);
+      ld4(cb, s.cb + i + P);
+      ld4(l0, a.lex + i + P);
+      ld4(l1, a.ley + i + P);
+      masked_prod(fxz, cb, l0, rx);
+      masked_prod(fyz, cb, l1, ry);
+    }
+    zero4(fxy);
+    zero4(fzy);
+    if (y + 1 < ny - 1) {
+      e_ranges(s, z, y + 1, x0, rx, ry, rz);
+      ld4(cb, s.cb + i + W);
+      ld4(l0, a.lex + i + W);
+      ld4(l2, a.lez + i + W);
+      masked_prod(fxy, cb, l0, rx);
+      masked_prod(fzy, cb, l2, rz);
+    }
+    if (x0 + kVec < nx - 1) {   // the cell x0 + 4 is inside the x ranges
+      const T cbn = s.cb[i + kVec];
+      if (z >= 1 && z < nz - 1 && y < ny - 1) fyn = cbn * a.ley[i + kVec];
+      if (z < nz - 1 && y >= 1 && y < ny - 1) fzn = cbn * a.lez[i + kVec];
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < kVec; ++j) {
+    const T fy_x = j + 1 < kVec ? fy[j + 1 < kVec ? j + 1 : j] : fyn;
+    const T fz_x = j + 1 < kVec ? fz[j + 1 < kVec ? j + 1 : j] : fzn;
+    dhx[j] = (fy[j] - fyz[j]) - (fz[j] - fzy[j]);
+    dhy[j] = (fz[j] - fz_x) - (fx[j] - fxz[j]);
+    dhz[j] = (fx[j] - fxy[j]) - (fy[j] - fy_x);
+  }
+  if constexpr (!kFast) {
+    T t0[kVec], t1[kVec], u0[kVec], u1[kVec];
+    // z faces of the cell and of z + 1: Eyz reads hx(c) - hx(c - z), Exz hy
+    e_zface(s, a, z, y, x0, fx, fy, t0, t1);
+    e_zface(s, a, z + 1, y, x0, fxz, fyz, u0, u1);
+#pragma unroll
+    for (int j = 0; j < kVec; ++j) {
+      dhx[j] += t1[j] - u1[j];
+      dhy[j] += t0[j] - u0[j];
+    }
+    // y faces of the cell and of y + 1: Exy reads hz(c) - hz(c - y), Ezy hx
+    e_yface(s, a, z, y, x0, fx, fz, t0, t1);
+    e_yface(s, a, z, y + 1, x0, fxy, fzy, u0, u1);
+#pragma unroll
+    for (int j = 0; j < kVec; ++j) {
+      dhz[j] += t0[j] - u0[j];
+      dhx[j] += t1[j] - u1[j];
+    }
+    // x faces of x0 .. x0 + 4: Ezx reads hy(c) - hy(c - x), Eyx hz
+    if (x0 < m || x0 + kVec >= nx - m) {
+      T xt0[kVec + 1], xt1[kVec + 1];
+#pragma unroll
+      for (int p = 0; p <= kVec; ++p) {
+        const int xx = x0 + p;
+        const T fyv = p < kVec ? fy[p < kVec ? p : 0] : fyn;
+        const T fzv = p < kVec ? fz[p < kVec ? p : 0] : fzn;
+        xt0[p] = T(0);
+        xt1[p] = T(0);
+        int side, q;
+        if (z < nz - 1 && y < ny - 1 && xx < nx - 1 && e_face(xx, nx, m, side, q)) {
+          const long long k = kx(s, z, y, q);
+          const T c = s.prof[side ? CE_U : CE_D][q] * s.rdx;
+          xt0[p] = c * (a.lps.x[side][0][k] - s.dx * fyv);
+          xt1[p] = c * (a.lps.x[side][1][k] + s.dx * fzv);
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < kVec; ++j) {
+        dhy[j] += xt1[j] - xt1[j + 1];
+        dhz[j] += xt0[j] - xt0[j + 1];
+      }
+    }
+  }
+}
+
+// (c) gradients and the E auxiliaries' adjoint of the vector; returns
+// Ca lambda_E (zero outside the update ranges). s.iex.. hold E^n, s.ihx..
+// H^{n+1/2}, s.ps the auxiliaries after the step.
+template <class T, bool kFast>
+__device__ __forceinline__ void e_own_vec(const State<T>& s, const Adj<T>& a, int z, int y, int x0,
+                                          T (&ox)[kVec], T (&oy)[kVec], T (&oz)[kVec]) {
+  const int nx = s.nx, ny = s.ny, nz = s.nz, m = s.npml;
+  const long long P = s.plane, W = s.pitch, i = idx(s, z, y, x0);
+  T lx[kVec], ly[kVec], lz[kVec], ca[kVec], cb[kVec];
+  ld4(lx, a.lex + i);
+  ld4(ly, a.ley + i);
+  ld4(lz, a.lez + i);
+  ld4(ca, s.ca + i);
+  ld4(cb, s.cb + i);
+  bool rx[kVec], ry[kVec], rz[kVec];
+  if constexpr (kFast) {
+#pragma unroll
+    for (int j = 0; j < kVec; ++j) rx[j] = ry[j] = rz[j] = true;
+  } else {
+    e_ranges(s, z, y, x0, rx, ry, rz);
+  }
+  const bool grad = z < a.nz_grad;   // gradients only over the requested planes
+  double gca[kVec], gcb[kVec];
+  if (grad) {
+    T e[kVec], h0[kVec], h1[kVec], h2[kVec], hn0[kVec], hn1[kVec];
+    ld4(e, s.iex + i);
+#pragma unroll
+    for (int j = 0; j < kVec; ++j) gca[j] = rx[j] ? (double)lx[j] * (double)e[j] : 0.0;
+    ld4(e, s.iey + i);
+#pragma unroll
+    for (int j = 0; j < kVec; ++j) gca[j] += ry[j] ? (double)ly[j] * (double)e[j] : 0.0;
+    ld4(e, s.iez + i);
+#pragma unroll
+    for (int j = 0; j < kVec; ++j) gca[j] += rz[j] ? (double)lz[j] * (double)e[j] : 0.0;
+    ld4(h0, s.ihx + i);
+    ld4(h1, s.ihy + i);
+    ld4(h2, s.ihz + i);
+    // ex: (hz - hz(y-1)) - (hy - hy(z-1))
+    if (kFast || (z >= 1 && y >= 1)) {
+      ld4(hn0, s.ihz + i - W);
+      ld4(hn1, s.ihy + i - P);
+    } else {
+      zero4(hn0);
+      zero4(hn1);
+    }
+#pragma unroll
+    for (int j = 0; j < kVec; ++j)
+      gcb[j] = rx[j] ? (double)lx[j] * (double)((h2[j] - hn0[j]) - (h1[j] - hn1[j])) : 0.0;
+    // ey: (hx - hx(z-1)) - (hz - hz(x-1))
+    const T hzp = (kFast || (x0 >= 1 && z >= 1)) ? s.ihz[i - 1] : T(0);
+    if (kFast || z >= 1) ld4(hn0, s.ihx + i - P); else zero4(hn0);
+#pragma unroll
+    for (int j = 0; j < kVec; ++j) {
+      const T hz_x = j > 0 ? h2[j > 0 ? j - 1 : 0] : hzp;
+      gcb[j] += ry[j] ? (double)ly[j] * (double)((h0[j] - hn0[j]) - (h2[j] - hz_x)) : 0.0;
+    }
+    // ez: (hy - hy(x-1)) - (hx - hx(y-1))
+    const T hyp = (kFast || (x0 >= 1 && y >= 1)) ? s.ihy[i - 1] : T(0);
+    if (kFast || y >= 1) ld4(hn0, s.ihx + i - W); else zero4(hn0);
+#pragma unroll
+    for (int j = 0; j < kVec; ++j) {
+      const T hy_x = j > 0 ? h1[j > 0 ? j - 1 : 0] : hyp;
+      gcb[j] += rz[j] ? (double)lz[j] * (double)((h1[j] - hy_x) - (h0[j] - hn0[j])) : 0.0;
+    }
+  }
+  if constexpr (!kFast) {
+    if (z < nz - 1 && y < ny - 1) {
+      const T dx = s.dx;
+      int side, q;
+      if (e_face(z, nz, m, side, q)) {
+        const long long k = kz(s, q, y, x0);
+        const T b = s.prof[side ? BE_U : BE_D][q];
+        T p0[kVec], p1[kVec], s0[kVec], s1[kVec];
+        ld4(p0, a.lps.z[side][0] + k);
+        ld4(p1, a.lps.z[side][1] + k);
+        if (grad) {
+          ld4(s0, s.ps.z[side][0] + k);
+          ld4(s1, s.ps.z[side][1] + k);
+        }
+#pragma unroll
+        for (int j = 0; j < kVec; ++j) {
+          if (x0 + j >= nx - 1) continue;
+          if (grad) gcb[j] += (double)dx * ((double)s1[j] * ly[j] - (double)s0[j] * lx[j]);
+          p1[j] = b * (p1[j] + cb[j] * dx * ly[j]);
+          p0[j] = b * (p0[j] - cb[j] * dx * lx[j]);
+        }
+        st4(a.lps.z[side][0] + k, p0);
+        st4(a.lps.z[side][1] + k, p1);
+      }
+      if (x0 < m || x0 + kVec - 1 >= nx - m) {
+#pragma unroll
+        for (int j = 0; j < kVec; ++j) {
+          const int x = x0 + j;
+          if (x >= nx - 1 || !e_face(x, nx, m, side, q)) continue;
+          const long long k = kx(s, z, y, q);
+          const T b = s.prof[side ? BE_U : BE_D][q];
+          T* p1 = a.lps.x[side][1];
+          T* p0 = a.lps.x[side][0];
+          if (grad)
+            gcb[j] += (double)dx * ((double)s.ps.x[side][1][k] * lz[j] - (double)s.ps.x[side][0][k] * ly[j]);
+          p1[k] = b * (p1[k] + cb[j] * dx * lz[j]);
+          p0[k] = b * (p0[k] - cb[j] * dx * ly[j]);
+        }
+      }
+      if (e_face(y, ny, m, side, q)) {
+        const long long k = ky(s, z, q, x0);
+        const T b = s.prof[side ? BE_U : BE_D][q];
+        T p0[kVec], p1[kVec], s0[kVec], s1[kVec];
+        ld4(p0, a.lps.y[side][0] + k);
+        ld4(p1, a.lps.y[side][1] + k);
+        if (grad) {
+          ld4(s0, s.ps.y[side][0] + k);
+          ld4(s1, s.ps.y[side][1] + k);
+        }
+#pragma unroll
+        for (int j = 0; j < kVec; ++j) {
+          if (x0 + j >= nx - 1) continue;
+          if (grad) gcb[j] += (double)dx * ((double)s0[j] * lx[j] - (double)s1[j] * lz[j]);
+          p0[j] = b * (p0[j] + cb[j] * dx * lx[j]);
+          p1[j] = b * (p1[j] - cb[j] * dx * lz[j]);
+        }
+        st4(a.lps.y[side][0] + k, p0);
+        st4(a.lps.y[side][1] + k, p1);
+      }
     }
   }
   if (grad) {
-    a.gca[i] += gca;
-    a.gcb[i] += gcb;
+    double g[kVec];
+    ld4(g, a.gca + i);
+#pragma unroll
+    for (int j = 0; j < kVec; ++j) g[j] += gca[j];
+    st4(a.gca + i, g);
+    ld4(g, a.gcb + i);
+#pragma unroll
+    for (int j = 0; j < kVec; ++j) g[j] += gcb[j];
+    st4(a.gcb + i, g);
   }
   // A component outside its main-update range is updated in the forward
   // step only by CPML corrections and injection terms that read other such
@@ -299,148 +628,161 @@ __device__ __forceinline__ void e_own_part(const State<T>& s, const Adj<T>& a, i
   // reference's does) it stays exactly zero, so no parameter reaches J
   // through it, and nothing in range reads it back in the transposed step.
   // Its exact adjoint, fed by the interior's, grows exponentially like the
-  // forward sub-system would if driven; it is held at zero instead (here,
-  // and by the range tests where adjoints are accumulated), which leaves
-  // every gradient unchanged and keeps the sweep finite.
-  out_x = re_x(s, z, y, x) ? ca * lx : T(0);
-  out_y = re_y(s, z, y, x) ? ca * ly : T(0);
-  out_z = re_z(s, z, y, x) ? ca * lz : T(0);
+  // forward sub-system would if driven; it is held at zero instead (here
+  // and in k_adj_k1), which leaves every gradient unchanged and keeps the
+  // sweep finite. Every reader below relies on that: adjoint fields are
+  // exactly zero outside their update ranges.
+#pragma unroll
+  for (int j = 0; j < kVec; ++j) {
+    ox[j] = rx[j] ? ca[j] * lx[j] : T(0);
+    oy[j] = ry[j] ? ca[j] * ly[j] : T(0);
+    oz[j] = rz[j] ? ca[j] * lz[j] : T(0);
+  }
 }
 
-// ---- 5: lambda_E += (H update + H CPML)^T lambda_H ----------------------------
-template <class T>
-__device__ __forceinline__ void h_to_e_terms(const State<T>& s, const Adj<T>& a, int z, int y, int x,
-                                             T& out_x, T& out_y, T& out_z) {
+// (e) lambda_E increments of the vector: the transposed curl of
+// G = Db lambda_H (forward differences: the forward H update of the cell
+// and of its -x, -y, -z neighbours reads E of this cell) and the H-face
+// auxiliaries of the cell and of those neighbours.
+template <class T, bool kFast>
+__device__ __forceinline__ void h_to_e_vec(const State<T>& s, const Adj<T>& a, int z, int y, int x0,
+                                           T (&dex)[kVec], T (&dey)[kVec], T (&dez)[kVec]) {
   const int nx = s.nx, ny = s.ny, nz = s.nz, m = s.npml;
+  const long long P = s.plane, W = s.pitch, i = idx(s, z, y, x0);
+  T hx[kVec], hy[kVec], hz[kVec];       // lambda_H of the cell
+  T hxz[kVec], hyz[kVec];               // z - 1
+  T hxy[kVec], hzy[kVec];               // y - 1
+  ld4(hx, a.lhx + i);
+  ld4(hy, a.lhy + i);
+  ld4(hz, a.lhz + i);
+  if (kFast || z >= 1) {
+    ld4(hxz, a.lhx + i - P);
+    ld4(hyz, a.lhy + i - P);
+  } else {
+    zero4(hxz);
+    zero4(hyz);
+  }
+  if (kFast || y >= 1) {
+    ld4(hxy, a.lhx + i - W);
+    ld4(hzy, a.lhz + i - W);
+  } else {
+    zero4(hxy);
+    zero4(hzy);
+  }
+  T hyp = T(0), hzp = T(0);             // x0 - 1
+  if (kFast || x0 >= 1) {
+    hyp = a.lhy[i - 1];
+    hzp = a.lhz[i - 1];
+  }
   const T db = s.db;
-  auto Gx = [&](int zz, int yy, int xx) -> T {
-    if (zz < 0 || yy < 0 || xx < 0 || !rh_x(s, zz, yy, xx)) return T(0);
-    return db * a.lhx[idx(s, zz, yy, xx)];
-  };
-  auto Gy = [&](int zz, int yy, int xx) -> T {
-    if (zz < 0 || yy < 0 || xx < 0 || !rh_y(s, zz, yy, xx)) return T(0);
-    return db * a.lhy[idx(s, zz, yy, xx)];
-  };
-  auto Gz = [&](int zz, int yy, int xx) -> T {
-    if (zz < 0 || yy < 0 || xx < 0 || !rh_z(s, zz, yy, xx)) return T(0);
-    return db * a.lhz[idx(s, zz, yy, xx)];
-  };
-  const T gx = Gx(z, y, x), gy = Gy(z, y, x), gz = Gz(z, y, x);
-  T dex = (gy - Gy(z - 1, y, x)) - (gz - Gz(z, y - 1, x));
-  T dey = (gz - Gz(z, y, x - 1)) - (gx - Gx(z - 1, y, x));
-  T dez = (gx - Gx(z, y - 1, x)) - (gy - Gy(z, y, x - 1));
-  const T rdx = T(1) / s.dx;
-  // H-face auxiliaries: their total adjoint times c/dx. slot/comp: z faces
-  // 3 Hyz (hy, -) -> ex, 2 Hxz (hx, +) -> ey; x faces 3 Hzx (hz, -) -> ey,
-  // 2 Hyx (hy, +) -> ez; y faces 2 Hxy (hx, -) -> ez, 3 Hzy (hz, +) -> ex.
-  auto face_term = [&](int axis, int slot, int zz, int yy, int xx) -> T {
-    if (!box(s, zz, yy, xx)) return T(0);
-    int side, q;
-    long long k;
-    const T* lp;
-    const T* lc;
-    T sign;
-    if (axis == 0) {
-      if (!h_face(zz, nz, m, side, q)) return T(0);
-      k = kz(s, q, yy, xx);
-      lp = a.lps.z[side][slot];
-      lc = slot == 3 ? a.lhy : a.lhx;
-      sign = slot == 3 ? T(-1) : T(1);
-    } else if (axis == 1) {
-      if (!h_face(xx, nx, m, side, q)) return T(0);
-      k = kx(s, zz, yy, q);
-      lp = a.lps.x[side][slot];
-      lc = slot == 3 ? a.lhz : a.lhy;
-      sign = slot == 3 ? T(-1) : T(1);
-    } else {
-      if (!h_face(yy, ny, m, side, q)) return T(0);
-      k = ky(s, zz, q, xx);
-      lp = a.lps.y[side][slot];
-      lc = slot == 2 ? a.lhx : a.lhz;
-      sign = slot == 2 ? T(-1) : T(1);
+#pragma unroll
+  for (int j = 0; j < kVec; ++j) {
+    const T hy_x = j > 0 ? hy[j > 0 ? j - 1 : 0] : hyp;
+    const T hz_x = j > 0 ? hz[j > 0 ? j - 1 : 0] : hzp;
+    dex[j] = db * ((hy[j] - hyz[j]) - (hz[j] - hzy[j]));
+    dey[j] = db * ((hz[j] - hz_x) - (hx[j] - hxz[j]));
+    dez[j] = db * ((hx[j] - hxy[j]) - (hy[j] - hy_x));
+  }
+  if constexpr (!kFast) {
+    T t2[kVec], t3[kVec], u2[kVec], u3[kVec];
+    // z faces of z - 1 and of the cell: Hyz reads ex(c + z) - ex(c), Hxz ey
+    h_zface(s, a, z - 1, y, x0, hxz, hyz, t2, t3);
+    h_zface(s, a, z, y, x0, hx, hy, u2, u3);
+#pragma unroll
+    for (int j = 0; j < kVec; ++j) {
+      dex[j] += t3[j] - u3[j];
+      dey[j] += t2[j] - u2[j];
     }
-    const T c = s.prof[side ? CH_U : CH_D][q];
-    return c * rdx * (lp[k] + sign * s.dtm0 * lc[idx(s, zz, yy, xx)]);
-  };
-  // the auxiliary at c' uses e(c' + n) - e(c'): e(c) gets +term(c - n) - term(c)
-  dex += face_term(0, 3, z - 1, y, x) - face_term(0, 3, z, y, x);
-  dey += face_term(0, 2, z - 1, y, x) - face_term(0, 2, z, y, x);
-  dey += face_term(1, 3, z, y, x - 1) - face_term(1, 3, z, y, x);
-  dez += face_term(1, 2, z, y, x - 1) - face_term(1, 2, z, y, x);
-  dez += face_term(2, 2, z, y - 1, x) - face_term(2, 2, z, y, x);
-  dex += face_term(2, 3, z, y - 1, x) - face_term(2, 3, z, y, x);
-  out_x = dex;
-  out_y = dey;
-  out_z = dez;
-}
-
-// ---- 6: H auxiliaries' adjoint, from the cell's lambda_H (lhx, lhy, lhz) --
-template <class T>
-__device__ __forceinline__ void h_own_part(const State<T>& s, const Adj<T>& a, int z, int y, int x,
-                                           T lhx, T lhy, T lhz) {
-  if (!box(s, z, y, x)) return;
-  const int nx = s.nx, ny = s.ny, nz = s.nz, m = s.npml;
-  int side, q;
-  if (h_face(z, nz, m, side, q)) {
-    const long long k = kz(s, q, y, x);
-    const T b = s.prof[side ? BH_U : BH_D][q];
-    T* p3 = a.lps.z[side][3];
-    T* p2 = a.lps.z[side][2];
-    p3[k] = b * (p3[k] - s.dtm0 * lhy);
-    p2[k] = b * (p2[k] + s.dtm0 * lhx);
-  }
-  if (h_face(x, nx, m, side, q)) {
-    const long long k = kx(s, z, y, q);
-    const T b = s.prof[side ? BH_U : BH_D][q];
-    T* p3 = a.lps.x[side][3];
-    T* p2 = a.lps.x[side][2];
-    p3[k] = b * (p3[k] - s.dtm0 * lhz);
-    p2[k] = b * (p2[k] + s.dtm0 * lhy);
-  }
-  if (h_face(y, ny, m, side, q)) {
-    const long long k = ky(s, z, q, x);
-    const T b = s.prof[side ? BH_U : BH_D][q];
-    T* p2 = a.lps.y[side][2];
-    T* p3 = a.lps.y[side][3];
-    p2[k] = b * (p2[k] - s.dtm0 * lhx);
-    p3[k] = b * (p3[k] + s.dtm0 * lhz);
+    // y faces of y - 1 and of the cell: Hxy reads ez(c + y) - ez(c), Hzy ex
+    h_yface(s, a, z, y - 1, x0, hxy, hzy, t2, t3);
+    h_yface(s, a, z, y, x0, hx, hz, u2, u3);
+#pragma unroll
+    for (int j = 0; j < kVec; ++j) {
+      dez[j] += t2[j] - u2[j];
+      dex[j] += t3[j] - u3[j];
+    }
+    // x faces of x0 - 1 .. x0 + 3: Hzx reads ey(c + x) - ey(c), Hyx ez
+    if (x0 < m || x0 + kVec - 1 >= nx - m) {
+      T xt2[kVec + 1], xt3[kVec + 1];
+#pragma unroll
+      for (int p = 0; p <= kVec; ++p) {
+        const int xx = x0 - 1 + p;
+        const T lyv = p > 0 ? hy[p > 0 ? p - 1 : 0] : hyp;
+        const T lzv = p > 0 ? hz[p > 0 ? p - 1 : 0] : hzp;
+        xt2[p] = T(0);
+        xt3[p] = T(0);
+        int side, q;
+        if (xx >= 0 && z < nz - 1 && y < ny - 1 && xx < nx - 1 && h_face(xx, nx, m, side, q)) {
+          const long long k = kx(s, z, y, q);
+          const T c = s.prof[side ? CH_U : CH_D][q] * s.rdx;
+          xt2[p] = c * (a.lps.x[side][2][k] + s.dtm0 * lyv);
+          xt3[p] = c * (a.lps.x[side][3][k] - s.dtm0 * lzv);
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < kVec; ++j) {
+        dey[j] += xt3[j] - xt3[j + 1];
+        dez[j] += xt2[j] - xt2[j + 1];
+      }
+    }
   }
 }
 
 // ---- the two kernels of one backward step ------------------------------------
+// Blocks of (lanes, 128 / lanes) threads, each thread four x cells; grid
+// (x tiles, y tiles, nz).
+template <class T>
+__device__ __forceinline__ bool vec_cell(const State<T>& s, int& z, int& y, int& x0) {
+  x0 = kVec * (blockIdx.x * blockDim.x + threadIdx.x);
+  y = blockIdx.y * blockDim.y + threadIdx.y;
+  z = blockIdx.z;
+  return x0 < s.nx && y < s.ny;
+}
+
 // K1 (step n): the H auxiliaries' adjoint of step n + 1 (skipped for the
 // first backward step), then lambda_H += (E step)^T lambda_E + the H phasor
 // source of step n.
 template <class T>
 __global__ void __launch_bounds__(128) k_adj_k1(const __grid_constant__ State<T> s, Adj<T> a, int t,
                                                 int first) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int z = blockIdx.z;
-  if (x >= s.nx || y >= s.ny) return;
-  const long long i = idx(s, z, y, x);
-  const T lhx = a.lhx[i], lhy = a.lhy[i], lhz = a.lhz[i];
+  int z, y, x0;
+  if (!vec_cell(s, z, y, x0)) return;
   const int m = s.npml;
-  T dhx, dhy, dhz, phx, phy;
-  if (z >= m && z < s.nz - m - 1 && y >= m && y < s.ny - m - 1 && x >= m && x < s.nx - m - 1) {
-    // the cell and its +x, +y, +z neighbours are away from every CPML face
-    // and domain edge: the plain transposed curl
-    const long long P = s.plane, W = s.pitch;
-    const T fx = s.cb[i] * a.lex[i], fy = s.cb[i] * a.ley[i], fz = s.cb[i] * a.lez[i];
-    const T fy_z = s.cb[i + P] * a.ley[i + P], fx_z = s.cb[i + P] * a.lex[i + P];
-    const T fz_y = s.cb[i + W] * a.lez[i + W], fx_y = s.cb[i + W] * a.lex[i + W];
-    const T fz_x = s.cb[i + 1] * a.lez[i + 1], fy_x = s.cb[i + 1] * a.ley[i + 1];
-    dhx = (fy - fy_z) - (fz - fz_y);
-    dhy = (fz - fz_x) - (fx - fx_z);
-    dhz = (fx - fx_y) - (fy - fy_x);
+  const long long i = idx(s, z, y, x0);
+  T lhx[kVec], lhy[kVec], lhz[kVec], dhx[kVec], dhy[kVec], dhz[kVec];
+  ld4(lhx, a.lhx + i);
+  ld4(lhy, a.lhy + i);
+  ld4(lhz, a.lhz + i);
+  if (z >= m && z < s.nz - m - 1 && y >= m && y < s.ny - m - 1 && x0 >= m &&
+      x0 + kVec < s.nx - m) {
+    // no H face at the vector, no E face or domain edge at it or its +x,
+    // +y, +z neighbours
+    e_to_h_vec<T, true>(s, a, z, y, x0, dhx, dhy, dhz);
   } else {
-    if (!first) h_own_part(s, a, z, y, x, lhx, lhy, lhz);
-    e_to_h_terms(s, a, z, y, x, dhx, dhy, dhz);
+    if (!first) h_own_vec(s, a, z, y, x0, lhx, lhy, lhz);
+    e_to_h_vec<T, false>(s, a, z, y, x0, dhx, dhy, dhz);
   }
-  phasor_h_src(s, a, t, z, y, x, phx, phy);
-  // components outside their update range keep a zero adjoint (e_own_part)
-  a.lhx[i] = rh_x(s, z, y, x) ? lhx + dhx + phx : T(0);
-  a.lhy[i] = rh_y(s, z, y, x) ? lhy + dhy + phy : T(0);
-  a.lhz[i] = rh_z(s, z, y, x) ? lhz + dhz : T(0);
+  const int pz = s.nz - m - 1;
+  if (z == pz || z == pz - 1) {
+#pragma unroll
+    for (int j = 0; j < kVec; ++j) {
+      T phx, phy;
+      phasor_h_src(s, a, t, z, y, x0 + j, phx, phy);
+      dhx[j] += phx;
+      dhy[j] += phy;
+    }
+  }
+  bool rx[kVec], ry[kVec], rz[kVec];
+  h_ranges(s, z, y, x0, rx, ry, rz);
+#pragma unroll
+  for (int j = 0; j < kVec; ++j) {
+    lhx[j] = rx[j] ? lhx[j] + dhx[j] : T(0);
+    lhy[j] = ry[j] ? lhy[j] + dhy[j] : T(0);
+    lhz[j] = rz[j] ? lhz[j] + dhz[j] : T(0);
+  }
+  st4(a.lhx + i, lhx);
+  st4(a.lhy + i, lhy);
+  st4(a.lhz + i, lhz);
 }
 
 // K2 (step n): gradients and the E auxiliaries' adjoint, then
@@ -449,44 +791,54 @@ __global__ void __launch_bounds__(128) k_adj_k1(const __grid_constant__ State<T>
 template <class T>
 __global__ void __launch_bounds__(128) k_adj_k2(const __grid_constant__ State<T> s, Adj<T> a,
                                                 int t_prev) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
-  const int z = blockIdx.z;
-  if (x >= s.nx || y >= s.ny) return;
-  const long long i = idx(s, z, y, x);
+  int z, y, x0;
+  if (!vec_cell(s, z, y, x0)) return;
   const int m = s.npml;
-  T ex, ey, ez, dex, dey, dez, pex = T(0), pey = T(0);
-  if (z >= m && z < s.nz - m && y >= m && y < s.ny - m && x >= m && x < s.nx - m) {
-    // the cell and its -x, -y, -z neighbours are away from every CPML face
-    // and domain edge
-    const long long P = s.plane, W = s.pitch;
-    const T lx = a.lex[i], ly = a.ley[i], lz = a.lez[i];
-    if (z < a.nz_grad) {
-      const T* hx = s.ihx; const T* hy = s.ihy; const T* hz = s.ihz;
-      a.gca[i] += (double)lx * (double)s.iex[i] + (double)ly * (double)s.iey[i] +
-                  (double)lz * (double)s.iez[i];
-      a.gcb[i] += (double)lx * (double)((hz[i] - hz[i - W]) - (hy[i] - hy[i - P])) +
-                  (double)ly * (double)((hx[i] - hx[i - P]) - (hz[i] - hz[i - 1])) +
-                  (double)lz * (double)((hy[i] - hy[i - 1]) - (hx[i] - hx[i - W]));
-    }
-    const T ca = s.ca[i], db = s.db;
-    ex = ca * lx;
-    ey = ca * ly;
-    ez = ca * lz;
-    const T gx = db * a.lhx[i], gy = db * a.lhy[i], gz = db * a.lhz[i];
-    const T gy_z = db * a.lhy[i - P], gx_z = db * a.lhx[i - P];
-    const T gz_y = db * a.lhz[i - W], gx_y = db * a.lhx[i - W];
-    const T gz_x = db * a.lhz[i - 1], gy_x = db * a.lhy[i - 1];
-    dex = (gy - gy_z) - (gz - gz_y);
-    dey = (gz - gz_x) - (gx - gx_z);
-    dez = (gx - gx_y) - (gy - gy_x);
+  const long long i = idx(s, z, y, x0);
+  T ex[kVec], ey[kVec], ez[kVec], dex[kVec], dey[kVec], dez[kVec];
+  if (z >= m && z < s.nz - m && y >= m && y < s.ny - m && x0 >= m && x0 + kVec - 1 < s.nx - m) {
+    // no E or H face at the vector, no H face or domain edge at its -x, -y,
+    // -z neighbours
+    e_own_vec<T, true>(s, a, z, y, x0, ex, ey, ez);
+    h_to_e_vec<T, true>(s, a, z, y, x0, dex, dey, dez);
   } else {
-    e_own_part(s, a, z, y, x, ex, ey, ez);
-    h_to_e_terms(s, a, z, y, x, dex, dey, dez);
+    e_own_vec<T, false>(s, a, z, y, x0, ex, ey, ez);
+    h_to_e_vec<T, false>(s, a, z, y, x0, dex, dey, dez);
   }
-  if (t_prev >= 0) phasor_e_src(s, a, t_prev, z, y, x, pex, pey);
-  a.lex[i] = re_x(s, z, y, x) ? ex + dex + pex : T(0);
-  a.ley[i] = re_y(s, z, y, x) ? ey + dey + pey : T(0);
-  a.lez[i] = re_z(s, z, y, x) ? ez + dez : T(0);
+  if (t_prev >= 0 && z == s.nz - m - 1) {
+#pragma unroll
+    for (int j = 0; j < kVec; ++j) {
+      T pex, pey;
+      phasor_e_src(s, a, t_prev, z, y, x0 + j, pex, pey);
+      dex[j] += pex;
+      dey[j] += pey;
+    }
+  }
+  bool rx[kVec], ry[kVec], rz[kVec];
+  e_ranges(s, z, y, x0, rx, ry, rz);
+#pragma unroll
+  for (int j = 0; j < kVec; ++j) {
+    ex[j] = rx[j] ? ex[j] + dex[j] : T(0);
+    ey[j] = ry[j] ? ey[j] + dey[j] : T(0);
+    ez[j] = rz[j] ? ez[j] + dez[j] : T(0);
+  }
+  st4(a.lex + i, ex);
+  st4(a.ley + i, ey);
+  st4(a.lez + i, ez);
+}
+
+// lanes per row: the width (8, 16 or 32 threads of four cells) that pads the
+// row least, the wider on a tie
+inline int adj_lanes(int nx) {
+  int best = 32, pad = 1 << 30;
+  for (int w : {32, 16, 8}) {
+    const int cells = kVec * w, p = ((nx + cells - 1) / cells) * cells - nx;
+    if (p < pad) {
+      pad = p;
+      best = w;
+    }
+  }
+  return best;
 }
 
 // 32 x 4 cells per block: little x padding on grids a few hundred cells wide
@@ -497,7 +849,8 @@ void launch_adjoint_first(const State<T>& s, const Adj<T>& a, int t, cudaStream_
 
 template <class T>
 void launch_adjoint_step(const State<T>& s, const Adj<T>& a, int t, bool first, cudaStream_t st) {
-  const dim3 grd((s.nx + 31) / 32, (s.ny + 3) / 4, s.nz), blk(32, 4, 1);
+  const int w = adj_lanes(s.nx), rows = 128 / w;
+  const dim3 grd((s.nx + kVec * w - 1) / (kVec * w), (s.ny + rows - 1) / rows, s.nz), blk(w, rows, 1);
   k_adj_k1<T><<<grd, blk, 0, st>>>(s, a, t, first ? 1 : 0);
   k_adj_k2<T><<<grd, blk, 0, st>>>(s, a, t - 1);
 }
