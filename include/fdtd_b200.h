@@ -277,6 +277,64 @@ int fdtd_near2far_noalloc(const void *ex_u, const void *ey_u,
                           const double *phis_deg, int nphi, double freq,
                           int device, double *out);
 
+/* ---- incident beam ----------------------------------------------------------
+ * The beam generation of IncidentBeam.setup (incidentbeam.py:41-71): the
+ * excitation of create_inc_excitation (incidentbeam.py:206-298, taper_k
+ * :301-433) and the vacuum FDTD run of IncidentSimCpu (cpu/incident_sim.py:
+ * 22-171), which records ex, ey, hx, hy of its read-out plane at every step
+ * (the datasets of the incident file) and the four incident phasors.
+ * Geometry: nx, ny, npml, dtype, cell_size, timestep, frequency, db and dtm0
+ * as for the main simulation; nz the incident grid's height,
+ * int(3 wavelengths / cell_size) (cpu/incident_sim.py:33-37); nt the steps
+ * run and recorded (size_t_inc); dte0dx the vacuum's Cb,
+ * timestep / (eps0 cell_size) with scipy's eps0 (cpu/incident_sim.py:
+ * 104-116); tfsf_z and nt_inc are not used. The hard source overwrites ex,
+ * ey on plane nz / 2 + 4 while t < nt_pulse (size_t_pulse) and the read-out
+ * plane is nz / 2 (cpu/incident_sim.py:101-103,141-144). */
+typedef struct fdtd_incident fdtd_incident;
+
+#define FDTD_POL_HH   0
+#define FDTD_POL_VV   1
+#define FDTD_POL_RHCP 2
+#define FDTD_POL_LHCP 3
+
+int fdtd_incident_create(const fdtd_geometry *geom, int nt_pulse, int device,
+                         fdtd_incident **out);
+int fdtd_incident_destroy(fdtd_incident *inc);
+/* 8 * npml profiles, packed as for fdtd_set_absorbers (Absorbers(params)
+ * of the incident simulation, cpu/fdtd_sim.py:14-23). */
+int fdtd_incident_set_absorbers(fdtd_incident *inc, const void *profiles);
+/* Computes the excitation on the device (create_inc_excitation): for each of
+ * the nt_fft pulse bins, its wavenumber k_vals[i] (2 pi pulse_freqs[i] / c)
+ * and its pulse spectrum value pulse_fft[2i], pulse_fft[2i+1] (re, im; the
+ * FFT of create_pulse, incidentbeam.py:174-199); incidence angles in
+ * degrees, polarisation FDTD_POL_*, taper radius in metres
+ * (incidentbeam.py:231-233). The excitation's imaginary parts of the first
+ * nt_pulse samples are kept for fdtd_incident_run; `peak` (may be NULL)
+ * gets the peak magnitude before the normalisation to 10. */
+int fdtd_incident_make_excitation(fdtd_incident *inc, const double *k_vals,
+                                  const double *pulse_fft, int nt_fft,
+                                  double theta_deg, double phi_deg, int pol,
+                                  double gauss_radius, double *peak);
+/* The excitation's imaginary parts (np.imag(pulse_ex)[:nt_pulse], and ey),
+ * (nt_pulse, ny, nx) of the element type, from / to host memory. */
+int fdtd_incident_set_excitation(fdtd_incident *inc, const void *ex_imag,
+                                 const void *ey_imag);
+int fdtd_incident_get_excitation(fdtd_incident *inc, void *ex_imag, void *ey_imag);
+/* Runs all nt steps from zero fields (IncidentSimCpu._sim_loop). */
+int fdtd_incident_run(fdtd_incident *inc);
+/* The recorded planes, (nt, ny, nx) each (the datasets ex, ey, hx, hy of
+ * the incident file), and the incident phasors, complex (ny - 2 npml,
+ * nx - 2 npml) each (phasors/{ex,ey,hx,hy}_inc_phasor). */
+int fdtd_incident_get_planes(fdtd_incident *inc, void *ex, void *ey, void *hx, void *hy);
+int fdtd_incident_get_phasors(fdtd_incident *inc, void *ex_ph, void *ey_ph,
+                              void *hx_ph, void *hy_ph);
+/* Device-to-device: the first nt_inc recorded planes of an incident run as
+ * the incident beam of a main simulation with the same nx, ny, element type
+ * and device (replaces writing the incident file and reading it back,
+ * cpu/incident_sim.py:140-160 and gpu/main_sim.py:256-264). */
+int fdtd_set_incident_from(fdtd_sim *sim, const fdtd_incident *inc);
+
 #ifdef __cplusplus
 }
 #endif

@@ -63,7 +63,7 @@ def build(force=False, verbose=False, extra_flags=()):
         msg = '\n'.join(' '.join(c) + '\n' + out for c, out in failed)
         raise RuntimeError('nvcc failed:\n' + msg)
     if force or jobs or not os.path.exists(LIB) or os.path.getmtime(LIB) < _newest(objs):
-        cmd = [NVCC] + ARCH + ['-shared', '-o', LIB] + objs + ['-lcudart', '-lcuda']
+        cmd = [NVCC] + ARCH + ['-shared', '-o', LIB] + objs + ['-lcudart', '-lcuda', '-lcufft']
         if verbose:
             print(' '.join(cmd), flush=True)
         p = subprocess.run(cmd, capture_output=True, text=True)

@@ -1223,3 +1223,259 @@ int fdtd_grad_backward(fdtd_sim* s, const double* dj_dre, const double* dj_dim, 
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// incident beam: excitation and vacuum run (fdtd_incident_*)
+// ---------------------------------------------------------------------------
+// The run uses an ordinary simulation handle for its grid: Ca = 1, Cb the
+// vacuum's, no TFSF injection (nt_inc = 0), the split passes in place.
+struct fdtd_incident {
+  fdtd_sim* sim = nullptr;
+  int nt_pulse = 0;            // source steps (size_t_pulse, at most nt)
+  int feed_in = 0, read_out = 0;
+  void* exc[2] = {};           // excitation imaginary parts, (nt_pulse, ny, pitch)
+  void* rec[4] = {};           // recorded ex, ey, hx, hy, (nt, ny, pitch)
+  void* iph = nullptr;         // incident phasors, 4 x (ny_ph, nx_ph) complex
+  bool have_exc = false, ran = false;
+};
+
+namespace {
+
+int check_inc(fdtd_incident* b) {
+  if (!b || !b->sim) return fail(FDTD_ERR_INVALID, "null incident handle");
+  return check_sim(b->sim);
+}
+
+template <class T>
+int incident_run(fdtd_incident* b) {
+  fdtd_sim* s = b->sim;
+  const fdtd_geometry& g = s->g;
+  int rc = fdtd_reset(s);
+  if (rc) return rc;
+  const size_t phb = (size_t)8 * s->ny_ph * s->nx_ph * s->esz;
+  CK(cudaMemsetAsync(b->iph, 0, phb, s->stream));
+  ShellBoxes whole;
+  memset(&whole, 0, sizeof(whole));
+  add_shell_box(whole, 0, g.nx, 0, g.ny, 0, g.nz);
+  const State<T> st = make_state<T>(s, 0, 0);   // split passes in place on set 0
+  const int* zero_t = s->tdev + 2;
+  IncidentRecord<T> r;
+  r.ex = st.iex; r.ey = st.iey; r.hx = st.ihx; r.hy = st.ihy;
+  r.rex = (T*)b->rec[0]; r.rey = (T*)b->rec[1]; r.rhx = (T*)b->rec[2]; r.rhy = (T*)b->rec[3];
+  r.ph = (T*)b->iph;
+  r.phase = s->phase;
+  r.nx = g.nx; r.ny = g.ny; r.pitch = s->pitch; r.plane = s->plane;
+  r.npml = g.npml; r.read_out = b->read_out; r.nx_ph = s->nx_ph; r.ny_ph = s->ny_ph;
+  for (int t = 0; t < g.nt; ++t) {
+    // E update and E CPML, hard source, H update and H CPML, read-out
+    // (cpu/incident_sim.py:134-160)
+    launch_shell_pass<T>(st, zero_t, t, whole, false, s->stream);
+    if (t < b->nt_pulse)
+      launch_inc_source<T>(st.oex, st.oey, (const T*)b->exc[0], (const T*)b->exc[1], g.nx, g.ny, s->pitch,
+                           s->plane, b->feed_in, t, s->stream);
+    launch_shell_pass<T>(st, zero_t, t, whole, true, s->stream);
+    launch_inc_record<T>(r, t, s->stream);
+  }
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(s->stream));
+  s->t = g.nt;
+  b->ran = true;
+  return FDTD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fdtd_incident_create(const fdtd_geometry* geom, int nt_pulse, int device, fdtd_incident** out) {
+  if (!geom || !out) return fail(FDTD_ERR_INVALID, "null argument");
+  *out = nullptr;
+  if (nt_pulse < 0) return fail(FDTD_ERR_INVALID, "negative pulse length");
+  if (geom->nt < 1) return fail(FDTD_ERR_INVALID, "incident run needs at least one step");
+  fdtd_geometry g = *geom;
+  g.nt_inc = 0;            // no TFSF injection in the incident grid
+  g.tfsf_z = g.nz / 2;     // unused; any plane inside the grid
+  fdtd_incident* b = new fdtd_incident();
+  int rc = fdtd_create(&g, device, &b->sim);
+  if (rc) {
+    delete b;
+    return rc;
+  }
+  fdtd_sim* s = b->sim;
+  b->nt_pulse = std::min(nt_pulse, g.nt);   // the reference's loop ends at nt
+  b->feed_in = g.nz / 2 + 4;                // cpu/incident_sim.py:101-103
+  b->read_out = b->feed_in - 4;
+  if (b->feed_in >= g.nz - 1) {
+    fdtd_incident_destroy(b);
+    return fail(FDTD_ERR_INVALID, "incident grid of %d planes too thin for its source plane", g.nz);
+  }
+  const size_t pb = (size_t)g.ny * s->pitch * s->esz;
+  for (int c = 0; c < 2 && !rc; ++c) rc = alloc(s, pb * std::max(b->nt_pulse, 1), &b->exc[c]);
+  for (int c = 0; c < 4 && !rc; ++c) rc = alloc(s, pb * g.nt, &b->rec[c]);
+  if (!rc) rc = alloc(s, (size_t)8 * s->ny_ph * s->nx_ph * s->esz, &b->iph);
+  if (!rc) {
+    // vacuum: Ca = 1, Cb = dt / (eps0 dx) (cpu/incident_sim.py:112-116)
+    if (g.dtype == FDTD_F32) {
+      launch_fill<float>((float*)s->ca, s->vol, 1.0f, s->stream);
+      launch_fill<float>((float*)s->cb, s->vol, (float)g.dte0dx, s->stream);
+    } else {
+      launch_fill<double>((double*)s->ca, s->vol, 1.0, s->stream);
+      launch_fill<double>((double*)s->cb, s->vol, g.dte0dx, s->stream);
+    }
+    cudaError_t e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) rc = fail(FDTD_ERR_CUDA, "vacuum coefficients: %s", cudaGetErrorString(e));
+    s->have_mat = true;
+  }
+  if (rc) {
+    fdtd_incident_destroy(b);
+    return rc;
+  }
+  *out = b;
+  return FDTD_OK;
+}
+
+int fdtd_incident_destroy(fdtd_incident* b) {
+  if (!b) return FDTD_OK;
+  if (b->sim) fdtd_destroy(b->sim);
+  delete b;
+  return FDTD_OK;
+}
+
+int fdtd_incident_set_absorbers(fdtd_incident* b, const void* profiles) {
+  int rc = check_inc(b);
+  if (rc) return rc;
+  return fdtd_set_absorbers(b->sim, profiles);
+}
+
+int fdtd_incident_make_excitation(fdtd_incident* b, const double* k_vals, const double* pulse_fft,
+                                  int nt_fft, double theta_deg, double phi_deg, int pol,
+                                  double gauss_radius, double* peak) {
+  int rc = check_inc(b);
+  if (rc) return rc;
+  if (!k_vals || !pulse_fft) return fail(FDTD_ERR_INVALID, "null pulse spectrum");
+  if (nt_fft < 1 || nt_fft < b->nt_pulse)
+    return fail(FDTD_ERR_INVALID, "pulse spectrum of %d bins shorter than the source (%d steps)", nt_fft,
+                b->nt_pulse);
+  if (nt_fft > 65535) return fail(FDTD_ERR_INVALID, "pulse spectrum of %d bins too long", nt_fft);
+  if (!(gauss_radius > 0)) return fail(FDTD_ERR_INVALID, "taper radius must be positive");
+  IncidentTaper p;
+  switch (pol) {   // (Eh, Ev) of incidentbeam.py:405-419
+    case FDTD_POL_HH: p.eh = make_double2(1, 0); p.ev = make_double2(0, 0); break;
+    case FDTD_POL_VV: p.eh = make_double2(0, 0); p.ev = make_double2(1, 0); break;
+    case FDTD_POL_RHCP: p.eh = make_double2(0, -1); p.ev = make_double2(1, 0); break;
+    case FDTD_POL_LHCP: p.eh = make_double2(0, 1); p.ev = make_double2(1, 0); break;
+    default: return fail(FDTD_ERR_INVALID, "Invalid polarization value %d", pol);
+  }
+  fdtd_sim* s = b->sim;
+  const fdtd_geometry& g = s->g;
+  p.nx = g.nx; p.ny = g.ny; p.nt = nt_fft;
+  p.dfx = 1.0 / (g.nx * g.cell_size);   // numpy.fft.fftfreq spacing
+  p.dfy = 1.0 / (g.ny * g.cell_size);
+  const double th = theta_deg * (M_PI / 180.0), ph = phi_deg * (M_PI / 180.0);
+  p.sin_theta = std::sin(th);
+  p.cos_phi = std::cos(ph);
+  p.sin_phi = std::sin(ph);
+  p.r2 = gauss_radius * gauss_radius;
+  p.r2_4pi = p.r2 / (4 * M_PI);
+  rc = g.dtype == FDTD_F32
+           ? make_incident_excitation<float>(p, k_vals, pulse_fft, b->nt_pulse, s->pitch, (float*)b->exc[0],
+                                             (float*)b->exc[1], peak, s->stream)
+           : make_incident_excitation<double>(p, k_vals, pulse_fft, b->nt_pulse, s->pitch, (double*)b->exc[0],
+                                              (double*)b->exc[1], peak, s->stream);
+  if (rc) return rc;
+  b->have_exc = true;
+  return FDTD_OK;
+}
+
+int fdtd_incident_set_excitation(fdtd_incident* b, const void* ex_imag, const void* ey_imag) {
+  int rc = check_inc(b);
+  if (rc) return rc;
+  if ((!ex_imag || !ey_imag) && b->nt_pulse > 0) return fail(FDTD_ERR_INVALID, "null excitation");
+  fdtd_sim* s = b->sim;
+  const size_t w = (size_t)s->g.nx * s->esz;
+  const void* src[2] = {ex_imag, ey_imag};
+  for (int c = 0; c < 2 && b->nt_pulse > 0; ++c)
+    CK(cudaMemcpy2DAsync(b->exc[c], (size_t)s->pitch * s->esz, src[c], w, w, (size_t)s->g.ny * b->nt_pulse,
+                         cudaMemcpyHostToDevice, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  b->have_exc = true;
+  return FDTD_OK;
+}
+
+int fdtd_incident_get_excitation(fdtd_incident* b, void* ex_imag, void* ey_imag) {
+  int rc = check_inc(b);
+  if (rc) return rc;
+  if (!b->have_exc) return fail(FDTD_ERR_STATE, "no excitation (fdtd_incident_make_excitation)");
+  fdtd_sim* s = b->sim;
+  const size_t w = (size_t)s->g.nx * s->esz;
+  void* dst[2] = {ex_imag, ey_imag};
+  for (int c = 0; c < 2 && b->nt_pulse > 0; ++c)
+    if (dst[c])
+      CK(cudaMemcpy2DAsync(dst[c], w, b->exc[c], (size_t)s->pitch * s->esz, w, (size_t)s->g.ny * b->nt_pulse,
+                           cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return FDTD_OK;
+}
+
+int fdtd_incident_run(fdtd_incident* b) {
+  int rc = check_inc(b);
+  if (rc) return rc;
+  if (!b->sim->have_abs) return fail(FDTD_ERR_STATE, "absorbers not set (fdtd_incident_set_absorbers)");
+  if (!b->have_exc) return fail(FDTD_ERR_STATE, "no excitation (fdtd_incident_make_excitation)");
+  return b->sim->g.dtype == FDTD_F32 ? incident_run<float>(b) : incident_run<double>(b);
+}
+
+int fdtd_incident_get_planes(fdtd_incident* b, void* ex, void* ey, void* hx, void* hy) {
+  int rc = check_inc(b);
+  if (rc) return rc;
+  if (!b->ran) return fail(FDTD_ERR_STATE, "incident run not done (fdtd_incident_run)");
+  fdtd_sim* s = b->sim;
+  const size_t w = (size_t)s->g.nx * s->esz;
+  void* dst[4] = {ex, ey, hx, hy};
+  for (int c = 0; c < 4; ++c)
+    if (dst[c])
+      CK(cudaMemcpy2DAsync(dst[c], w, b->rec[c], (size_t)s->pitch * s->esz, w, (size_t)s->g.ny * s->g.nt,
+                           cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return FDTD_OK;
+}
+
+int fdtd_incident_get_phasors(fdtd_incident* b, void* ex_ph, void* ey_ph, void* hx_ph, void* hy_ph) {
+  int rc = check_inc(b);
+  if (rc) return rc;
+  if (!b->ran) return fail(FDTD_ERR_STATE, "incident run not done (fdtd_incident_run)");
+  fdtd_sim* s = b->sim;
+  const size_t n = (size_t)2 * s->ny_ph * s->nx_ph * s->esz;
+  void* dst[4] = {ex_ph, ey_ph, hx_ph, hy_ph};
+  for (int c = 0; c < 4; ++c)
+    if (dst[c])
+      CK(cudaMemcpyAsync(dst[c], (unsigned char*)b->iph + c * n, n, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return FDTD_OK;
+}
+
+int fdtd_set_incident_from(fdtd_sim* s, const fdtd_incident* b) {
+  int rc = check_sim(s);
+  if (rc) return rc;
+  if (!b || !b->sim) return fail(FDTD_ERR_INVALID, "null incident handle");
+  const fdtd_geometry& g = s->g;
+  const fdtd_geometry& gi = b->sim->g;
+  if (!b->ran) return fail(FDTD_ERR_STATE, "incident run not done (fdtd_incident_run)");
+  if (gi.nx != g.nx || gi.ny != g.ny || gi.dtype != g.dtype || b->sim->device != s->device)
+    return fail(FDTD_ERR_INVALID, "incident run of %dx%d (dtype %d, device %d) does not fit %dx%d (dtype %d, "
+                "device %d)", gi.ny, gi.nx, gi.dtype, b->sim->device, g.ny, g.nx, g.dtype, s->device);
+  if (g.nt_inc > gi.nt)
+    return fail(FDTD_ERR_INVALID, "incident run has %d steps, the simulation injects %d", gi.nt, g.nt_inc);
+  const size_t bytes = (size_t)std::max(g.nt_inc, 1) * s->plane * s->esz;
+  for (int c = 0; c < 4; ++c) {
+    if (!s->inc[c] && (rc = alloc(s, bytes, &s->inc[c]))) return rc;
+    if (g.nt_inc > 0)
+      CK(cudaMemcpyAsync(s->inc[c], b->rec[c], (size_t)g.nt_inc * s->plane * s->esz, cudaMemcpyDeviceToDevice,
+                         s->stream));
+  }
+  CK(cudaStreamSynchronize(s->stream));
+  s->inc_nt = g.nt_inc;
+  return FDTD_OK;
+}
+
+}  // extern "C"

@@ -67,6 +67,51 @@ void launch_adjoint_first(const State<T>& s, const Adj<T>& a, int t, cudaStream_
 template <class T>
 void launch_adjoint_step(const State<T>& s, const Adj<T>& a, int t, bool first, cudaStream_t st);
 
+// Incident beam (fdtd_incident.cu). The taper of incidentbeam.py:317-433
+// for a lateral grid of nx x ny cells and nt pulse bins: dfx = 1 / (nx dx),
+// dfy = 1 / (ny dx) (numpy.fft.fftfreq spacing), the incidence angles'
+// sines and cosines, r2 = radius^2, r2_4pi = radius^2 / (4 pi), and the
+// polarisation weights (Eh, Ev) as complex numbers.
+struct IncidentTaper {
+  int nx, ny, nt;
+  double dfx, dfy;
+  double sin_theta, cos_phi, sin_phi;
+  double r2, r2_4pi;
+  double2 eh, ev;
+};
+
+// The excitation of the incident run: the imaginary parts of its first
+// nt_pulse time samples into ex, ey ((nt_pulse, ny, pitch), element type T),
+// from the pulse bins' wavenumbers and spectrum (host arrays of nt doubles /
+// nt complex doubles). peak_out gets the peak magnitude before the
+// normalisation to 10. Returns an FDTD status code.
+template <class T>
+int make_incident_excitation(const IncidentTaper& p, const double* k_host, const double* pfft_host,
+                             int nt_pulse, int pitch, T* ex, T* ey, double* peak_out, cudaStream_t st);
+
+// The read-out plane of the incident run and the incident phasors: fields
+// of the run (its current set), the recorded planes (nt, ny, pitch), the
+// four phasor planes (complex, (ny_ph, nx_ph) each, consecutive) and the
+// run's phase table (per step: cos/sin of the t and t - 1/2 angles).
+template <class T>
+struct IncidentRecord {
+  const T* ex; const T* ey; const T* hx; const T* hy;
+  T* rex; T* rey; T* rhx; T* rhy;
+  T* ph;
+  const double* phase;
+  int nx, ny, pitch;
+  long long plane;
+  int npml, read_out, nx_ph, ny_ph;
+};
+
+template <class T>
+void launch_inc_source(T* ex, T* ey, const T* sx, const T* sy, int nx, int ny, int pitch, long long plane,
+                       int feed_in, int t, cudaStream_t st);
+template <class T>
+void launch_inc_record(const IncidentRecord<T>& r, int t, cudaStream_t st);
+template <class T>
+void launch_fill(T* p, long long n, T v, cudaStream_t st);
+
 // Records an error message for fdtd_last_error(); returns code.
 int report_error(int code, const char* msg);
 

@@ -40,6 +40,8 @@ OPT_ZCHUNK = 8
 TIME_STEP = 0
 TIME_PHASOR = 1
 
+POLARIZATIONS = {'HH': 0, 'VV': 1, 'RHCP': 2, 'LHCP': 3}   # FDTD_POL_*
+
 PHASOR_NAMES = (
     'ex_ph_d', 'ey_ph_d', 'hx_ph_d', 'hy_ph_d',
     'ex_ph_u', 'ey_ph_u', 'hx_ph_u', 'hy_ph_u',
@@ -112,6 +114,16 @@ SIGNATURES = {
     'fdtd_check_cell_division': [_I, _D, _I, ctypes.POINTER(ctypes.c_int64),
                                  ctypes.POINTER(ctypes.c_int64)],
     'fdtd_near2far_noalloc': [_P, _P, _P, _P, _I, _I, _I, _I, _D, _D, _P, _I, _P, _I, _D, _I, _P],
+    'fdtd_incident_create': [ctypes.POINTER(Geometry), _I, _I, ctypes.POINTER(_P)],
+    'fdtd_incident_destroy': [_P],
+    'fdtd_incident_set_absorbers': [_P, _P],
+    'fdtd_incident_make_excitation': [_P, _P, _P, _I, _D, _D, _I, _D, ctypes.POINTER(_D)],
+    'fdtd_incident_set_excitation': [_P, _P, _P],
+    'fdtd_incident_get_excitation': [_P, _P, _P],
+    'fdtd_incident_run': [_P],
+    'fdtd_incident_get_planes': [_P, _P, _P, _P, _P],
+    'fdtd_incident_get_phasors': [_P, _P, _P, _P, _P],
+    'fdtd_set_incident_from': [_P, _P],
 }
 
 
@@ -310,6 +322,90 @@ class NativeSim:
 
     def get_fields(self):
         return {c: self.get_field(c) for c in FIELD_NAMES}
+
+    def set_incident_from(self, inc):
+        """The first nt_inc planes recorded by a NativeIncident run, device
+        to device (fdtd_set_incident_from)."""
+        check(lib.fdtd_set_incident_from(self.h, inc.h))
+
+
+class NativeIncident:
+    """Owning wrapper of one ``fdtd_incident`` handle: the excitation and
+    the vacuum run that record the incident beam. ``geom`` is the incident
+    grid (nz its height, nt the recorded steps, dte0dx the vacuum's Cb)."""
+
+    def __init__(self, geom: Geometry, nt_pulse: int, device: int = 0):
+        self.geom = geom
+        self.dtype = np.float32 if geom.dtype == FDTD_F32 else np.float64
+        self.cdtype = np.complex64 if geom.dtype == FDTD_F32 else np.complex128
+        self.nt_pulse = min(int(nt_pulse), int(geom.nt))
+        h = ctypes.c_void_p()
+        check(lib.fdtd_incident_create(ctypes.byref(geom), int(nt_pulse), int(device), ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, 'h', None) is not None and self.h.value:
+            lib.fdtd_incident_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_absorbers(self, packed):
+        a = np.ascontiguousarray(packed, dtype=self.dtype)
+        if a.shape != (8 * self.geom.npml,):
+            raise ValueError(f'expected {8 * self.geom.npml} profile values, got {a.shape}')
+        check(lib.fdtd_incident_set_absorbers(self.h, ptr(a)))
+
+    def make_excitation(self, k_vals, pulse_fft, theta_deg, phi_deg, pol, gauss_radius):
+        """Excitation on the device from the pulse bins' wavenumbers and
+        spectrum; returns the peak magnitude before normalisation."""
+        if pol not in POLARIZATIONS:
+            raise ValueError('Invalid polarization value')
+        k = np.ascontiguousarray(k_vals, dtype=np.float64)
+        pf = np.ascontiguousarray(pulse_fft, dtype=np.complex128)
+        if k.shape != pf.shape or k.ndim != 1:
+            raise ValueError('wavenumbers and pulse spectrum must be 1-D of one length')
+        peak = ctypes.c_double(0)
+        check(lib.fdtd_incident_make_excitation(self.h, ptr(k), ptr(pf), int(k.size), float(theta_deg),
+                                                float(phi_deg), POLARIZATIONS[pol], float(gauss_radius),
+                                                ctypes.byref(peak)))
+        return peak.value
+
+    def _exc_shape(self):
+        return (self.nt_pulse, self.geom.ny, self.geom.nx)
+
+    def set_excitation(self, ex_imag, ey_imag):
+        a = np.ascontiguousarray(ex_imag, dtype=self.dtype)
+        b = np.ascontiguousarray(ey_imag, dtype=self.dtype)
+        if a.shape != self._exc_shape() or b.shape != self._exc_shape():
+            raise ValueError(f'excitation must be {self._exc_shape()}')
+        check(lib.fdtd_incident_set_excitation(self.h, ptr(a), ptr(b)))
+
+    def get_excitation(self):
+        a = np.zeros(self._exc_shape(), self.dtype)
+        b = np.zeros(self._exc_shape(), self.dtype)
+        check(lib.fdtd_incident_get_excitation(self.h, ptr(a), ptr(b)))
+        return a, b
+
+    def run(self):
+        check(lib.fdtd_incident_run(self.h))
+
+    def get_planes(self):
+        g = self.geom
+        out = {c: np.zeros((g.nt, g.ny, g.nx), self.dtype) for c in ('ex', 'ey', 'hx', 'hy')}
+        check(lib.fdtd_incident_get_planes(self.h, *[ptr(out[c]) for c in ('ex', 'ey', 'hx', 'hy')]))
+        return out
+
+    def get_phasors(self):
+        g = self.geom
+        shape = (g.ny - 2 * g.npml, g.nx - 2 * g.npml)
+        out = {c: np.zeros(shape, self.cdtype) for c in ('ex', 'ey', 'hx', 'hy')}
+        check(lib.fdtd_incident_get_phasors(self.h, *[ptr(out[c]) for c in ('ex', 'ey', 'hx', 'hy')]))
+        return {f'{c}_inc_phasor': v for c, v in out.items()}
 
 
 def near2far(ex_u, ey_u, hx_u, hy_u, nx, ny, nz, dx, r, thetas_deg, phis_deg, freq, device=0,

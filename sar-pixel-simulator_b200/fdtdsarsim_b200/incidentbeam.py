@@ -41,13 +41,39 @@ class IncidentBeam:
         return resultsio.exists(inc_filename(self.params))
 
     def setup(self):
+        """Load the geometry's incident file, or make the beam on the device
+        and write it first (incidentbeam.py:41-71)."""
         if not self.inc_beam_params.generate_new and self.inc_beam_exists():
             logger.info('Loading existing incident beam files')
             self.load_existing()
             return
+        logger.info('Generating new incident beam on the device')
         from .incident import generate_incident_beam
-        generate_incident_beam(self.params)
+        _, _, sim = generate_incident_beam(self.params)
+        sim.close()
         self.load_existing()
+
+    def create_pulse(self):
+        """The temporal pulse and its spectrum (incidentbeam.py:174-204):
+        sets time_vals, pulse, pulse_fft and pulse_freqs."""
+        from .incident import create_pulse
+        self.time_vals, self.pulse, self.pulse_fft, self.pulse_freqs = create_pulse(self.params)
+
+    def create_inc_excitation(self):
+        """The excitation of the incident simulation, computed on the device
+        (incidentbeam.py:206-298). Returns the part of the reference's
+        complex (size_t_inc, ny, nx) arrays that the simulation injects: the
+        imaginary parts of the first size_t_pulse samples
+        (cpu/incident_sim.py:108-110,141-144), as (Ex, Ey) real arrays of the
+        simulation dtype. Call create_pulse() first."""
+        from .incident import IncidentSimGpu
+        from .gpu.main_sim import _device_of
+        sim = IncidentSimGpu(self.params, _device_of(self.params))
+        try:
+            sim.make_excitation(self.pulse_fft, self.pulse_freqs)
+            return sim.native.get_excitation()
+        finally:
+            sim.close()
 
     def load_existing(self):
         with resultsio.File(inc_filename(self.params), 'r') as f:

@@ -16,6 +16,9 @@ Outputs (all small, committed):
   near2far.npz         FarFieldTransform (near2far.py:28-112)
   pipeline_cfg1.npz    run_experiment end to end (experiment.py:41-97),
                        incident beam generation included
+  incident_*.npz       IncidentBeam.create_pulse / create_inc_excitation
+                       (incidentbeam.py:174-298) and IncidentSimCpu
+                       (cpu/incident_sim.py:22-171) on small geometries
 """
 import json
 import os
@@ -289,8 +292,67 @@ def gen_pipeline_cfg1():
     np.savez_compressed(os.path.join(HERE, 'pipeline_cfg1.npz'), **out)
 
 
+# (tag, dtype, pol, theta, phi, size_x, size_y, duration, store_full_excitation)
+INCIDENT_CASES = [
+    ('hh_f32', 'float32', 'HH', 20.0, 0.0, 1.5, 1.5, 2.0, True),
+    ('vv_f64', 'float64', 'VV', 35.0, 30.0, 1.3, 1.6, 2.0, False),
+]
+
+
+def gen_incident(tag, dtype, pol, theta, phi, sx, sy, duration, full):
+    """The incident beam of a small geometry: the temporal pulse, the
+    excitation fed into the incident simulation, and the planes and phasors
+    that simulation records."""
+    from fdtdsarsim.cpu.incident_sim import IncidentSimCpu
+    from fdtdsarsim.incidentbeam import IncidentBeam
+    import h5py
+    with tempfile.TemporaryDirectory() as proj:
+        pc = make_params(dtype, proj, threads=3)
+        pc.inc_beam_params.polarization = pol
+        pc.inc_beam_params.theta_angle = theta
+        pc.inc_beam_params.phi_angle = phi
+        pc.inc_beam_params.duration = duration
+        pc.inc_beam_params.illumination_width = 0.8 * sx
+        pc.material_params.material_fraction = 0.5
+        set_geom_params(pc, sx, sy, 0.5, 18.0, 0.05, 'wavelength')
+        g = pc.geom_params
+        beam = IncidentBeam(pc)
+        beam.create_pulse()
+        pulse_ex, pulse_ey = beam.create_inc_excitation()
+        sim = IncidentSimCpu(pc)
+        sim.run(pulse_ex, pulse_ey)
+        ntp, npulse = g.size_t_inc, g.size_t_pulse
+        out = {'dtype': dtype, 'pol': pol, 'theta': theta, 'phi': phi,
+               'freq': pc.inc_beam_params.frequency, 'duration': duration,
+               'illumination_width': pc.inc_beam_params.illumination_width,
+               'nx': g.size_x, 'ny': g.size_y, 'nz_inc': sim.params.geom_params.size_z,
+               'npml': g.size_pml, 'dx': g.cell_size, 'dt': g.timestep,
+               'size_t_inc': ntp, 'size_t_pulse': npulse,
+               'time_vals': beam.time_vals, 'pulse': beam.pulse,
+               'pulse_fft': beam.pulse_fft, 'pulse_freqs': beam.pulse_freqs}
+        exi, eyi = np.imag(pulse_ex), np.imag(pulse_ey)
+        if full:
+            out['exc_ex_imag'] = exi[:npulse]
+            out['exc_ey_imag'] = eyi[:npulse]
+        steps = np.arange(0, npulse, 7)
+        out['exc_steps'] = steps
+        out['exc_ex_imag_at'] = exi[steps]
+        out['exc_ey_imag_at'] = eyi[steps]
+        out['exc_ex_real_at'] = np.real(pulse_ex)[steps]
+        out['exc_absmax'] = max(np.abs(pulse_ex).max(), np.abs(pulse_ey).max())
+        with h5py.File(inc_filename(pc), 'r') as f:
+            rec = np.arange(0, ntp, 6)
+            out['rec_steps'] = rec
+            for comp in ('ex', 'ey', 'hx', 'hy'):
+                d = f[comp][:]
+                out[f'inc_{comp}_at'] = d[rec]
+                out[f'inc_{comp}_stepsum'] = np.sum(d, axis=(1, 2), dtype=np.float64)
+                out[f'{comp}_inc_phasor'] = f['phasors'][f'{comp}_inc_phasor'][:]
+    np.savez_compressed(os.path.join(HERE, f'incident_{tag}.npz'), **out)
+
+
 if __name__ == '__main__':
-    which = sys.argv[1:] or ['geom', 'abs', 'mat', 'main', 'n2f', 'pipe']
+    which = sys.argv[1:] or ['geom', 'abs', 'mat', 'main', 'n2f', 'pipe', 'inc']
     if 'geom' in which:
         gen_geom()
     if 'abs' in which:
@@ -306,3 +368,6 @@ if __name__ == '__main__':
         gen_near2far()
     if 'pipe' in which:
         gen_pipeline_cfg1()
+    if 'inc' in which:
+        for case in INCIDENT_CASES:
+            gen_incident(*case)
