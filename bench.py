@@ -40,7 +40,7 @@ def parse():
     ap.add_argument('--warmup', type=int, default=5)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--workload', default='plain_16x16',
-                    choices=['plain_16x16', 'plain_8x8', 'batch64', 'adjoint_4x4'])
+                    choices=['plain_16x16', 'plain_8x8', 'batch64', 'adjoint_4x4', 'incident_16x16'])
     ap.add_argument('--fd-cells', type=int, default=32, help='adjoint_4x4: cells checked by FD')
     ap.add_argument('--profile-region', action='store_true',
                     help='adjoint_4x4: run one extra gradient between cudaProfilerStart/Stop')
@@ -611,6 +611,94 @@ def run_adjoint(a):
     print(json.dumps(line))
 
 
+# ---------------------------------------------------------------------------
+# incident beam: the full-size beam of the 16x16 wavelength geometry
+# ---------------------------------------------------------------------------
+def run_incident(a):
+    import torch
+    torch.cuda.set_device(0)
+    from fdtdsarsim_b200 import synthetic
+    from fdtdsarsim_b200.incident import IncidentSimGpu, create_pulse
+    pc = synthetic.config_params('plain_16x16', a.dtype)
+    g = pc.geom_params
+    _, _, pulse_fft, pulse_freqs = create_pulse(pc)
+    sim = IncidentSimGpu(pc, 0)
+    gi = sim.params.geom_params
+
+    def wall(fn):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out = fn()
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0, out
+
+    # one untimed pass (module loading, cuFFT set-up), then the timed pass
+    sim.make_excitation(pulse_fft, pulse_freqs)
+    sim.run()
+    clocks = ClockSampler(0)
+    clocks.start()
+    t_exc, peak = wall(lambda: sim.make_excitation(pulse_fft, pulse_freqs))
+    t_run, _ = wall(sim.run)
+    clk = clocks.stop()
+    t_read, planes = wall(sim.planes)
+    sim.close()
+    cells = gi.size_x * gi.size_y * gi.size_z
+    steps = g.size_t_inc
+    # CPU: the C oracle's steps on the same grid (all host cores), and the
+    # numpy oracle's excitation on a sample of pulse bins, scaled to all bins
+    sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+    base = None
+    if not a.no_cpu_baseline:
+        ca = np.ones((gi.size_z, gi.size_y, gi.size_x), a.dtype)
+        cb = np.full_like(ca, native_cb(sim.params))
+        base = cpu_baseline(sim.params, ca, cb, None, a.cpu_steps)
+        import incident_oracle as IO
+        kx_sample = 4
+        t0 = time.perf_counter()
+        idx = np.linspace(1, len(pulse_fft) - 1, kx_sample).astype(int)
+        kx, ky = IO.spatial_freqs(g.size_x, g.size_y, g.cell_size)
+        for i in idx:
+            k = (2 * np.pi * pulse_freqs[i]) / 299792458
+            spec = IO.taper_k(k, kx, ky, pc.inc_beam_params.theta_angle, pc.inc_beam_params.phi_angle,
+                              IO.gauss_radius(pc.inc_beam_params.illumination_width,
+                                              pc.inc_beam_params.frequency),
+                              pc.inc_beam_params.polarization)
+            for c in spec:
+                np.fft.fftshift(np.fft.fft2(np.fft.ifftshift(c)))
+        per_bin = (time.perf_counter() - t0) / kx_sample
+        base['excitation_estimate_s'] = round(per_bin * len(pulse_fft), 1)
+        base['excitation_sample'] = (f'taper and 2-D FFT of {kx_sample} of {len(pulse_fft)} pulse bins '
+                                     f'(numpy oracle, one thread), scaled to all bins; time-axis '
+                                     f'transforms not included')
+    mcells = cells * steps / t_run / 1e6
+    line = {
+        'metric': 'Mcell-updates/s', 'value': round(mcells, 1), 'unit': 'Mcell-updates/s',
+        'higher_is_better': True, 'n_gpus': 1, 'steps': steps, 'warmup': 1,
+        'ms_per_step': round(t_run / steps * 1e3, 4), 'scaling': 'weak', 'vs_baseline': None,
+        'dtype': 'f32' if a.dtype == 'float32' else 'f64',
+        'data': 'synthetic (the geometry\'s own incident beam: tapered-wave excitation from its '
+                'pulse, vacuum run)',
+        'config': {'workload': f'incident_16x16: incident beam of the 16x16 wavelength geometry, '
+                               f'grid {gi.size_z}x{gi.size_y}x{gi.size_x}, {steps} steps, source '
+                               f'{g.size_t_pulse} steps, {pc.inc_beam_params.polarization}',
+                   'grid': [gi.size_z, gi.size_y, gi.size_x], 'cells': cells,
+                   'pulse_bins': len(pulse_fft)},
+        'excitation_s': round(t_exc, 3), 'run_s': round(t_run, 3),
+        'planes_to_host_s': round(t_read, 3),
+        'planes_bytes': int(sum(v.nbytes for v in planes.values())),
+        'excitation_peak_before_normalisation': peak,
+        'cpu_baseline': base, 'clocks': clk,
+        'gpu_launches': 4 * steps,
+    }
+    print(json.dumps(line))
+
+
+def native_cb(params):
+    """Cb of the vacuum in the simulation dtype (cpu/incident_sim.py:116)."""
+    from fdtdsarsim_b200.gpu.main_sim import native_geometry
+    return native_geometry(params).dte0dx
+
+
 def main():
     a = parse()
     if a.impl == 'reference':
@@ -619,6 +707,8 @@ def main():
         run_batch(a)
     elif a.workload == 'adjoint_4x4':
         run_adjoint(a)
+    elif a.workload == 'incident_16x16':
+        run_incident(a)
     else:
         run_ours(a)
 

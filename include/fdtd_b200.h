@@ -147,15 +147,20 @@ int fdtd_reset(fdtd_sim *sim);
 int fdtd_run(fdtd_sim *sim, int nsteps);
 
 /* Runs `nsteps` time steps while streaming the incident planes of those
- * steps from host memory (four (nt_inc, ny, nx) arrays) through pinned
- * staging buffers on a copy stream, overlapped with the time stepping.
+ * steps from host memory (four (nt_inc, ny, nx) arrays) on a copy stream,
+ * 16 steps' planes per transfer, overlapped with the time stepping: each
+ * group of steps waits only for its own planes. Page-locked arrays are
+ * copied directly; pageable ones through two pinned staging buffers.
  * Synchronous. This is the reference's per-step incident transfer
  * (gpu/main_sim.py:256-264,305-313) made asynchronous. */
 int fdtd_run_streamed(fdtd_sim *sim, int nsteps, const void *ex,
                       const void *ey, const void *hx, const void *hy);
 
 /* Blocks until all enqueued work of the handle is done; reports deferred
- * CUDA errors and the non-finite check. */
+ * CUDA errors and, with FDTD_OPT_CHECK_EVERY = k > 0, FDTD_ERR_NONFINITE
+ * when a scan of the six fields after every k-th step found a NaN or an
+ * infinity (the message names the first such step; fdtd_reset clears it).
+ * The reference has no such check: a diverging run writes NaN phasors. */
 int fdtd_synchronize(fdtd_sim *sim);
 
 /* Number of completed (enqueued) steps since the last reset. */

@@ -75,6 +75,7 @@ struct fdtd_sim {
   long long ph_elems = 0;
   double* phase = nullptr;
   int* tdev = nullptr;
+  int* flags = nullptr;                  // non-finite check: found, step
   int64_t t = 0;
   int cur = 0;
   cudaStream_t own = nullptr;
@@ -83,6 +84,12 @@ struct fdtd_sim {
   // interior pass (fork and join by events)
   cudaStream_t side = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
+  // fdtd_run_streamed: copy stream, one event per staging slot, and pinned
+  // staging buffers for pageable host planes (created on first use)
+  cudaStream_t copy = nullptr;
+  cudaEvent_t copy_ev[2] = {nullptr, nullptr};
+  void* stage[2] = {nullptr, nullptr};
+  size_t stage_bytes = 0;
   bool have_abs = false, have_mat = false;
   std::vector<unsigned char> prof;       // 8 * npml values of the element type
   int kernel = FDTD_KERNEL_SPLIT;
@@ -93,6 +100,12 @@ struct fdtd_sim {
   int plan_ok = 0, plan_tile_y = 0, plan_zchunk = 0;
   int graph_chunk = 0;
   int check_every = 0;
+  // captured step chunks (FDTD_OPT_GRAPH_CHUNK), one per starting field set,
+  // with the settings they were captured under; absorber uploads bump the
+  // epoch (the profiles are captured by value)
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  int gsig[2][7] = {};
+  int graph_epoch = 0;
   // gradient (fdtd_grad_*): checkpoints of the forward solve, the segment
   // of recomputed states and the adjoint state; a state is the 6 fields
   // followed by one CPML auxiliary set
@@ -270,9 +283,73 @@ int enqueue_steps(fdtd_sim* s, int n, bool phasors = true) {
       if (phasors) launch_phasors<T>(st, s->tdev, k, s->stream);
     }
     mark(s, e2);
+    const long long done = s->t + k + 1;
+    if (s->check_every > 0 && done % s->check_every == 0) {
+      FieldPtrs<T> f;
+      for (int c = 0; c < 6; ++c) f.p[c] = (const T*)s->fld[s->cur][c];
+      launch_check_finite<T>(f, s->vol, (int)done, s->flags, s->stream);
+    }
   }
   launch_advance(s->tdev, n, s->stream);
   CK(cudaGetLastError());
+  return FDTD_OK;
+}
+
+// One chunk of `chunk` steps replayed from a captured graph (captured on
+// first use, and again when a setting it depends on changed). The graph
+// holds the step kernels with their step offsets, the phasor passes and the
+// step-counter advance, so every replay continues from the counter.
+template <class T>
+int enqueue_graph_chunk(fdtd_sim* s, int chunk) {
+  const int start = s->cur;
+  const int sig[7] = {chunk, s->kernel, s->tile_x, s->tile_y, s->zchunk, s->phasor_mode, s->graph_epoch};
+  if (!s->gexec[start] || memcmp(sig, s->gsig[start], sizeof(sig)) != 0) {
+    if (s->gexec[start]) {
+      cudaGraphExecDestroy(s->gexec[start]);
+      s->gexec[start] = nullptr;
+    }
+    CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    const int rc = enqueue_steps<T>(s, chunk);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(s->stream, &graph);
+    s->cur = start;   // capturing ran nothing
+    if (rc || e != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      cudaGetLastError();
+      return rc ? rc : fail(FDTD_ERR_CUDA, "step graph capture: %s", cudaGetErrorString(e));
+    }
+    const cudaError_t ei = cudaGraphInstantiate(&s->gexec[start], graph, 0);
+    cudaGraphDestroy(graph);
+    if (ei != cudaSuccess) {
+      s->gexec[start] = nullptr;
+      return fail(FDTD_ERR_CUDA, "step graph instantiation: %s", cudaGetErrorString(ei));
+    }
+    memcpy(s->gsig[start], sig, sizeof(sig));
+  }
+  CK(cudaGraphLaunch(s->gexec[start], s->stream));
+  if (s->kernel == FDTD_KERNEL_FUSED && (chunk & 1)) s->cur = 1 - start;
+  return FDTD_OK;
+}
+
+// Steps of fdtd_run: graph chunks when FDTD_OPT_GRAPH_CHUNK is set and
+// neither per-kernel timing nor the non-finite check (both tied to the
+// absolute step) is on, direct launches otherwise and for the remainder.
+template <class T>
+int run_steps(fdtd_sim* s, int nsteps) {
+  const int chunk = s->graph_chunk;
+  if (chunk > 0 && !s->timing && s->check_every == 0) {
+    while (nsteps >= chunk) {
+      const int rc = enqueue_graph_chunk<T>(s, chunk);
+      if (rc) return rc;
+      s->t += chunk;
+      nsteps -= chunk;
+    }
+  }
+  if (nsteps > 0) {
+    const int rc = enqueue_steps<T>(s, nsteps);
+    if (rc) return rc;
+    s->t += nsteps;
+  }
   return FDTD_OK;
 }
 
@@ -386,6 +463,7 @@ int fdtd_create(const fdtd_geometry* geom, int device, fdtd_sim** out) {
   A((size_t)off * s->esz, &s->phc);
   A((size_t)std::max(g.nt, 1) * 4 * sizeof(double), (void**)&s->phase);
   A(sizeof(int) * 4, (void**)&s->tdev);
+  A(sizeof(int) * 2, (void**)&s->flags);
   if (rc != FDTD_OK) {
     fdtd_destroy(s);
     return rc;
@@ -440,7 +518,15 @@ int fdtd_destroy(fdtd_sim* s) {
   if (s->own) cudaStreamSynchronize(s->own);
   for (auto& b : s->bufs) cudaFree(b.p);
   if (s->side) cudaStreamSynchronize(s->side);
+  if (s->copy) cudaStreamSynchronize(s->copy);
+  for (int k = 0; k < 2; ++k) {
+    if (s->copy_ev[k]) cudaEventDestroy(s->copy_ev[k]);
+    if (s->stage[k]) cudaFreeHost(s->stage[k]);
+  }
+  if (s->copy) cudaStreamDestroy(s->copy);
   for (auto e : s->ev) cudaEventDestroy(e);
+  for (int k = 0; k < 2; ++k)
+    if (s->gexec[k]) cudaGraphExecDestroy(s->gexec[k]);
   if (s->fork) cudaEventDestroy(s->fork);
   if (s->join) cudaEventDestroy(s->join);
   if (s->side) cudaStreamDestroy(s->side);
@@ -514,6 +600,7 @@ int fdtd_set_absorbers(fdtd_sim* s, const void* profiles) {
   const size_t n = 8 * (size_t)s->g.npml * s->esz;
   s->prof.assign((const unsigned char*)profiles, (const unsigned char*)profiles + n);
   s->have_abs = true;
+  s->graph_epoch++;
   return FDTD_OK;
 }
 
@@ -603,6 +690,7 @@ int fdtd_reset(fdtd_sim* s) {
   CK(cudaMemsetAsync(s->ph, 0, (size_t)s->ph_elems * s->esz, s->stream));
   CK(cudaMemsetAsync(s->phc, 0, (size_t)s->ph_elems * s->esz, s->stream));
   CK(cudaMemsetAsync(s->tdev, 0, sizeof(int) * 4, s->stream));
+  CK(cudaMemsetAsync(s->flags, 0, sizeof(int) * 2, s->stream));
   CK(cudaStreamSynchronize(s->stream));
   s->t = 0;
   s->cur = 0;
@@ -620,21 +708,82 @@ int fdtd_run(fdtd_sim* s, int nsteps) {
   if (s->g.nt_inc > 0 && s->t < s->g.nt_inc && s->inc_nt < s->g.nt_inc)
     return fail(FDTD_ERR_STATE, "incident beam not set (fdtd_set_incident)");
   if (nsteps == 0) return FDTD_OK;
-  rc = s->g.dtype == FDTD_F32 ? enqueue_steps<float>(s, nsteps) : enqueue_steps<double>(s, nsteps);
-  if (rc) return rc;
-  s->t += nsteps;
-  return FDTD_OK;
+  return s->g.dtype == FDTD_F32 ? run_steps<float>(s, nsteps) : run_steps<double>(s, nsteps);
 }
 
 int fdtd_run_streamed(fdtd_sim* s, int nsteps, const void* ex, const void* ey, const void* hx,
                       const void* hy) {
-  // First version: upload the incident planes the run needs, then run.
   int rc = check_sim(s);
   if (rc) return rc;
-  if (s->g.nt_inc > 0 && s->inc_nt < s->g.nt_inc) {
-    if ((rc = fdtd_set_incident(s, ex, ey, hx, hy, s->g.nt_inc))) return rc;
+  if (nsteps < 0) return fail(FDTD_ERR_INVALID, "negative step count");
+  if (!s->have_abs) return fail(FDTD_ERR_STATE, "absorbers not set (fdtd_set_absorbers)");
+  if (!s->have_mat) return fail(FDTD_ERR_STATE, "materials not set (fdtd_set_materials)");
+  const fdtd_geometry& g = s->g;
+  if (s->t + nsteps > g.nt)
+    return fail(FDTD_ERR_INVALID, "step %lld + %d exceeds size_t %d", (long long)s->t, nsteps, g.nt);
+  const int t0 = (int)s->t, t1 = t0 + nsteps;
+  // planes [t0, need) come from the given arrays; earlier ones are not
+  // read again
+  const int need = std::min(t1, g.nt_inc);
+  if (need <= t0) {
+    if ((rc = fdtd_run(s, nsteps))) return rc;
+    return fdtd_synchronize(s);
   }
-  if ((rc = fdtd_run(s, nsteps))) return rc;
+  const void* src[4] = {ex, ey, hx, hy};
+  for (int c = 0; c < 4; ++c)
+    if (!src[c]) return fail(FDTD_ERR_INVALID, "null incident component %d", c);
+  const size_t pb = (size_t)s->plane * s->esz;           // one pitched device plane
+  const size_t row = (size_t)g.nx * s->esz;
+  const size_t hb = row * g.ny;                         // one packed host plane
+  for (int c = 0; c < 4; ++c)
+    if (!s->inc[c] && (rc = alloc(s, pb * std::max(g.nt_inc, 1), &s->inc[c]))) return rc;
+  if (!s->copy) {
+    CK(cudaStreamCreateWithFlags(&s->copy, cudaStreamNonBlocking));
+    for (int k = 0; k < 2; ++k) CK(cudaEventCreateWithFlags(&s->copy_ev[k], cudaEventDisableTiming));
+  }
+  // Page-locked host planes are copied straight from the caller's arrays;
+  // pageable ones through two pinned staging slots (a host copy into a slot
+  // waits for that slot's previous transfer).
+  bool pinned = true;
+  for (int c = 0; c < 4; ++c) {
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, src[c]) != cudaSuccess || at.type != cudaMemoryTypeHost) pinned = false;
+  }
+  cudaGetLastError();
+  const int chunk = 16;   // steps whose planes travel in one transfer
+  if (!pinned && s->stage_bytes < 4 * hb * chunk) {
+    for (int k = 0; k < 2; ++k) {
+      if (s->stage[k]) cudaFreeHost(s->stage[k]);
+      s->stage[k] = nullptr;
+    }
+    s->stage_bytes = 0;
+    for (int k = 0; k < 2; ++k) CK(cudaHostAlloc(&s->stage[k], 4 * hb * chunk, cudaHostAllocDefault));
+    s->stage_bytes = 4 * hb * chunk;
+  }
+  for (int c0 = t0, slot = 0; c0 < t1; c0 += chunk, slot ^= 1) {
+    const int n = std::min(chunk, t1 - c0);
+    const int p1 = std::min(c0 + n, need);
+    if (p1 > c0) {
+      const size_t np = (size_t)(p1 - c0);
+      for (int c = 0; c < 4; ++c) {
+        const unsigned char* from = static_cast<const unsigned char*>(src[c]) + (size_t)c0 * hb;
+        if (!pinned) {
+          if (c == 0) CK(cudaEventSynchronize(s->copy_ev[slot]));
+          unsigned char* st = static_cast<unsigned char*>(s->stage[slot]) + (size_t)c * hb * chunk;
+          memcpy(st, from, np * hb);
+          from = st;
+        }
+        CK(cudaMemcpy2DAsync(static_cast<unsigned char*>(s->inc[c]) + (size_t)c0 * pb, (size_t)s->pitch * s->esz,
+                             from, row, row, (size_t)g.ny * np, cudaMemcpyHostToDevice, s->copy));
+      }
+      CK(cudaEventRecord(s->copy_ev[slot], s->copy));
+      CK(cudaStreamWaitEvent(s->stream, s->copy_ev[slot], 0));
+    }
+    rc = g.dtype == FDTD_F32 ? enqueue_steps<float>(s, n) : enqueue_steps<double>(s, n);
+    if (rc) return rc;
+    s->t += n;
+  }
+  if (t0 <= s->inc_nt) s->inc_nt = std::max(s->inc_nt, need);
   return fdtd_synchronize(s);
 }
 
@@ -643,6 +792,11 @@ int fdtd_synchronize(fdtd_sim* s) {
   if (rc) return rc;
   CK(cudaStreamSynchronize(s->stream));
   CK(cudaGetLastError());
+  if (s->check_every > 0) {
+    int f[2] = {0, 0};
+    CK(cudaMemcpy(f, s->flags, sizeof(f), cudaMemcpyDeviceToHost));
+    if (f[0]) return fail(FDTD_ERR_NONFINITE, "non-finite field value found after step %d", f[1]);
+  }
   return FDTD_OK;
 }
 

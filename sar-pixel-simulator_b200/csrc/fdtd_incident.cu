@@ -21,6 +21,7 @@
 // plane feed_in, the H pass (the split passes of the main step, without
 // injection), then k_inc_record copies the read-out plane and accumulates the
 // incident phasors (cpu/field_updates.py:465-491).
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 
@@ -232,8 +233,6 @@ int make_incident_excitation(const IncidentTaper& p, const double* k_host, const
   double* kv = nullptr;
   double2* pf = nullptr;
   unsigned long long* peak = nullptr;
-  cufftHandle p2 = 0, p1 = 0;
-  bool have2 = false, have1 = false;
   int rc = 0;
   auto cuda_fail = [&](const char* what, cudaError_t e) {
     snprintf(msg, sizeof(msg), "incident excitation: %s: %s", what, cudaGetErrorString(e));
@@ -259,30 +258,42 @@ int make_incident_excitation(const IncidentTaper& p, const double* k_host, const
     k_inc_taper<<<dim3((p.nx + 255) / 256, p.ny, p.nt), 256, 0, st>>>(p, kv, pf, sx, sy);
     if ((e = cudaGetLastError()) != cudaSuccess) cuda_fail("taper", e);
   }
-  // 2-D forward transforms, one per bin, in place
+  // Transforms in place, in batches that bound cuFFT's work area: 2-D
+  // forward transforms of kBins2d bins at a time, then inverse transforms
+  // along the bins (stride ny*nx) of kCells1d lateral cells at a time.
+  const int kBins2d = 32, kCells1d = 1 << 16;
+  auto run_batches = [&](int rank, int* dims, int* embed, int stride, int dist, int total, int per, int dir,
+                         long long step, const char* what) {
+    cufftHandle plans[2] = {0, 0};
+    bool made[2] = {false, false};
+    const int full = std::min(per, total), rest = total % full;
+    const int counts[2] = {full, rest};
+    for (int k = 0; k < 2 && !rc; ++k) {
+      if (counts[k] == 0) continue;
+      cufftResult r = cufftPlanMany(&plans[k], rank, dims, embed, stride, dist, embed, stride, dist, CUFFT_Z2Z,
+                                    counts[k]);
+      if (r != CUFFT_SUCCESS) { fft_fail(what, r); break; }
+      made[k] = true;
+      if ((r = cufftSetStream(plans[k], st)) != CUFFT_SUCCESS) fft_fail(what, r);
+    }
+    for (double2* a : {sx, sy}) {
+      for (int b = 0; b < total && !rc; b += full) {
+        const int k = (total - b < full) ? 1 : 0;
+        cufftDoubleComplex* q = (cufftDoubleComplex*)(a + (long long)b * step);
+        const cufftResult r = cufftExecZ2Z(plans[k], q, q, dir);
+        if (r != CUFFT_SUCCESS) fft_fail(what, r);
+      }
+    }
+    for (int k = 0; k < 2; ++k)
+      if (made[k]) cufftDestroy(plans[k]);
+  };
   if (!rc) {
     int dims[2] = {p.ny, p.nx};
-    cufftResult r = cufftPlanMany(&p2, 2, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_Z2Z, p.nt);
-    if (r != CUFFT_SUCCESS) fft_fail("2-D plan", r);
-    else have2 = true;
-    if (!rc && (r = cufftSetStream(p2, st)) != CUFFT_SUCCESS) fft_fail("2-D stream", r);
-    if (!rc && (r = cufftExecZ2Z(p2, (cufftDoubleComplex*)sx, (cufftDoubleComplex*)sx, CUFFT_FORWARD)) != CUFFT_SUCCESS)
-      fft_fail("2-D forward x", r);
-    if (!rc && (r = cufftExecZ2Z(p2, (cufftDoubleComplex*)sy, (cufftDoubleComplex*)sy, CUFFT_FORWARD)) != CUFFT_SUCCESS)
-      fft_fail("2-D forward y", r);
+    run_batches(2, dims, nullptr, 1, 0, p.nt, kBins2d, CUFFT_FORWARD, (long long)p.ny * p.nx, "2-D forward");
   }
-  // inverse transforms along the bins, one per lateral cell (stride ny*nx)
   if (!rc) {
     int len[1] = {p.nt};
-    const int lat = p.ny * p.nx;
-    cufftResult r = cufftPlanMany(&p1, 1, len, len, lat, 1, len, lat, 1, CUFFT_Z2Z, lat);
-    if (r != CUFFT_SUCCESS) fft_fail("time plan", r);
-    else have1 = true;
-    if (!rc && (r = cufftSetStream(p1, st)) != CUFFT_SUCCESS) fft_fail("time stream", r);
-    if (!rc && (r = cufftExecZ2Z(p1, (cufftDoubleComplex*)sx, (cufftDoubleComplex*)sx, CUFFT_INVERSE)) != CUFFT_SUCCESS)
-      fft_fail("time inverse x", r);
-    if (!rc && (r = cufftExecZ2Z(p1, (cufftDoubleComplex*)sy, (cufftDoubleComplex*)sy, CUFFT_INVERSE)) != CUFFT_SUCCESS)
-      fft_fail("time inverse y", r);
+    run_batches(1, len, len, p.ny * p.nx, 1, p.ny * p.nx, kCells1d, CUFFT_INVERSE, 1, "time inverse");
   }
   if (!rc) {
     k_inc_absmax<<<4 * 148, 256, 0, st>>>(sx, sy, n, peak);
@@ -300,8 +311,6 @@ int make_incident_excitation(const IncidentTaper& p, const double* k_host, const
     memcpy(&v, &bits, sizeof(v));
     *peak_out = v / (double)p.nt;   // the peak of the normalised inverse transform
   }
-  if (have2) cufftDestroy(p2);
-  if (have1) cufftDestroy(p1);
   cudaStreamSynchronize(st);
   for (void* q : {(void*)sx, (void*)sy, (void*)kv, (void*)pf, (void*)peak})
     if (q) cudaFree(q);

@@ -112,6 +112,15 @@ void launch_inc_record(const IncidentRecord<T>& r, int t, cudaStream_t st);
 template <class T>
 void launch_fill(T* p, long long n, T v, cudaStream_t st);
 
+// Non-finite check of one field set (fdtd_split.cu): flags[0] = 1,
+// flags[1] = step on the first NaN or infinity in any of the six fields.
+template <class T>
+struct FieldPtrs {
+  const T* p[6];
+};
+template <class T>
+void launch_check_finite(const FieldPtrs<T>& f, long long vol, int step, int* flags, cudaStream_t st);
+
 // Records an error message for fdtd_last_error(); returns code.
 int report_error(int code, const char* msg);
 

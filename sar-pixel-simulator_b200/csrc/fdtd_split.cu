@@ -357,6 +357,35 @@ void launch_advance(int* tdev, int n, cudaStream_t st) {
   k_advance<<<1, 1, 0, st>>>(tdev, n);
 }
 
+// ---------------------------------------------------------------------------
+// non-finite check: flags[0] = 1 and flags[1] = step when any of the six
+// fields holds a NaN or an infinity (cells, padding included: the padding
+// is never written and stays zero). The first detection wins.
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(256) k_check_finite(FieldPtrs<T> f, long long vol, int step,
+                                                      int* __restrict__ flags) {
+  if (*(volatile int*)flags) return;
+  bool bad = false;
+  for (int c = 0; c < 6; ++c) {
+    const T* p = f.p[c];
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < vol;
+         i += (long long)gridDim.x * blockDim.x)
+      bad |= !isfinite(p[i]);
+  }
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) {
+    if (atomicCAS(flags, 0, 1) == 0) flags[1] = step;
+  }
+}
+
+template <class T>
+void launch_check_finite(const FieldPtrs<T>& f, long long vol, int step, int* flags, cudaStream_t st) {
+  k_check_finite<T><<<8 * 148, 256, 0, st>>>(f, vol, step, flags);
+}
+
+template void launch_check_finite<float>(const FieldPtrs<float>&, long long, int, int*, cudaStream_t);
+template void launch_check_finite<double>(const FieldPtrs<double>&, long long, int, int*, cudaStream_t);
+
 template <class T>
 void launch_eps_sigma(int nx, int ny, int nz, int nz_mat, int pitch, const T* eps,
                       const T* sig, T eps0, T dt, T dx, T* ca, T* cb, cudaStream_t st) {

@@ -236,3 +236,101 @@ def test_state_errors():
     with pytest.raises(ValueError):
         sim.set_materials(np.zeros((3, 3, 3), np.float32), np.zeros((3, 3, 3), np.float32))
     sim.close()
+
+
+@pytest.mark.parametrize('pinned', [False, True], ids=['pageable', 'pinned'])
+@pytest.mark.parametrize('kernel', [SPLIT, FUSED], ids=['split', 'fused'])
+def test_streamed_run_equals_resident_planes(pinned, kernel):
+    """fdtd_run_streamed (planes copied 16 steps at a time beside the time
+    stepping) steps exactly like a run on planes uploaded beforehand, across
+    calls that end inside a transfer group and past the last incident step."""
+    import torch
+    pc = make_params(150, 41, 33, 16, 60, 45)
+    _, _, ca, cb, inc = random_problem(pc, 21)
+    comps = [inc[c] for c in ('ex', 'ey', 'hx', 'hy')]
+    if pinned:
+        comps = [torch.from_numpy(c).pin_memory().numpy() for c in comps]
+    a, b = native_for(pc, kernel), native_for(pc, kernel)
+    try:
+        for s in (a, b):
+            s.set_materials(ca, cb)
+        a.set_incident(*comps)
+        a.run(60)
+        a.synchronize()
+        for n in (7, 20, 33):
+            b.run_streamed(n, *comps)
+        for c in ('ex', 'ey', 'ez', 'hx', 'hy', 'hz'):
+            assert bits_equal(a.get_field(c), b.get_field(c)), c
+        for k in (4, 7, 13):
+            assert bits_equal(a.get_phasor(k), b.get_phasor(k)), k
+    finally:
+        a.close()
+        b.close()
+
+
+def test_non_finite_check_reports_the_step():
+    """FDTD_OPT_CHECK_EVERY: a NaN planted in the host-side initial field
+    (no device fault involved) is reported by fdtd_synchronize as
+    FDTD_ERR_NONFINITE with the first checked step after it; a clean run
+    with the check on passes and steps exactly like one without."""
+    pc = make_params(41, 37, 29, 16, 12, 10)
+    _, _, ca, cb, inc = random_problem(pc, 33)
+    comps = [inc[c] for c in ('ex', 'ey', 'hx', 'hy')]
+    a, b = native_for(pc), native_for(pc)
+    try:
+        for s in (a, b):
+            s.set_materials(ca, cb)
+            s.set_incident(*comps)
+        b.set_option(_native.OPT_CHECK_EVERY, 3)
+        a.run(12)
+        b.run(12)
+        a.synchronize()
+        b.synchronize()
+        assert bits_equal(a.get_field('ey'), b.get_field('ey'))
+        b.reset()
+        hz = np.zeros((29, 37, 41), np.float32)
+        hz[14, 18, 20] = np.nan
+        b.set_field('hz', hz)
+        b.run(7)
+        with pytest.raises(_native.FdtdError) as ei:
+            b.synchronize()
+        assert ei.value.code == _native.FDTD_ERR_NONFINITE
+        assert 'after step 3' in str(ei.value)
+        b.reset()
+        b.run(4)
+        b.synchronize()
+    finally:
+        a.close()
+        b.close()
+
+
+@pytest.mark.parametrize('kernel', [SPLIT, FUSED], ids=['split', 'fused'])
+def test_graph_chunks_equal_direct_launches(kernel):
+    """FDTD_OPT_GRAPH_CHUNK: steps replayed from captured graphs (odd chunk,
+    so the fused step's field sets alternate between replays; a tile change
+    forces a new capture) equal directly launched steps bit for bit."""
+    pc = make_params(150, 41, 33, 16, 40, 30)
+    _, _, ca, cb, inc = random_problem(pc, 44)
+    comps = [inc[c] for c in ('ex', 'ey', 'hx', 'hy')]
+    a, b = native_for(pc, kernel), native_for(pc, kernel)
+    try:
+        for s in (a, b):
+            s.set_materials(ca, cb)
+            s.set_incident(*comps)
+        b.set_option(_native.OPT_GRAPH_CHUNK, 5)
+        for s in (a, b):
+            s.run(13)
+        if kernel == FUSED:
+            for s in (a, b):
+                s.set_option(_native.OPT_TILE_Y, 8)
+        for s in (a, b):
+            s.run(27)
+            s.synchronize()
+        for c in ('ex', 'ey', 'ez', 'hx', 'hy', 'hz'):
+            assert bits_equal(a.get_field(c), b.get_field(c)), c
+        for k in (0, 4, 9, 17):
+            assert bits_equal(a.get_phasor(k), b.get_phasor(k)), k
+        assert b.step_index() == 40
+    finally:
+        a.close()
+        b.close()
