@@ -278,9 +278,9 @@ def run_ours(a):
         dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
     ms_max = float(ms_t.item())
     value = world * cells * a.steps / (ms_max / 1e3) / 1e6
-    # split: H pass, E pass, phasors; fused: interior pass, shell H pass,
+    # split: H pass, E pass, phasors; fused: interior pass (and z-slab pass), shell H pass,
     # shell E pass, phasors; plus one step-counter advance per run call
-    launches_per_step = 3 if choice['kernel'] == _native.FDTD_KERNEL_SPLIT else 4
+    launches_per_step = 3 if choice['kernel'] == _native.FDTD_KERNEL_SPLIT else 4 + int(bool(choice.get('slab', 0)))
     gpu_launches = launches_per_step * a.steps + 1
 
     # live per-kernel timing for the roofline (separate pass, same state)
@@ -357,10 +357,11 @@ def run_ours(a):
                            parallelism=f'replicas x{world}' if world > 1 else 'single GPU',
                            kernel=kname, tile=[choice['tile_x'], choice['tile_y']]
                            if choice['kernel'] == _native.FDTD_KERNEL_FUSED else None,
-                           zchunk=choice.get('zchunk', 0),
+                           zchunk=choice.get('zchunk', 0), z_slabs_fused=bool(choice.get('slab', 0)),
                            autotuned=None if tuned is None else
                            [{'ms': t, 'kernel': 'fused' if c['kernel'] else 'split',
-                             'tile_y': c['tile_y'], 'zchunk': c['zchunk']} for t, c in tuned]),
+                             'tile_y': c['tile_y'], 'zchunk': c['zchunk'], 'slab': c.get('slab', 0)}
+                            for t, c in tuned]),
             'roofline': roofline, 'cpu_baseline': base, 'e2e': e2e,
             'gpu_launches': gpu_launches, 'clocks': clk,
         }

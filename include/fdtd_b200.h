@@ -62,6 +62,8 @@ extern "C" {
 #define FDTD_OPT_CHECK_EVERY  6  /* non-finite check period in steps (0 = off) */
 #define FDTD_OPT_TIMING       7  /* 1: record CUDA events around every kernel */
 #define FDTD_OPT_ZCHUNK       8  /* fused kernel z planes per block (0 = automatic) */
+#define FDTD_OPT_FUSED_SLAB   9  /* 1: the fused step marches the CPML z slabs too
+                                    (default 0: the split passes sweep them) */
 
 /* kernel kinds of fdtd_get_kernel_time */
 #define FDTD_TIME_STEP    0   /* the field-update kernel(s) of a step */
@@ -256,6 +258,14 @@ int fdtd_batch_get_stream(fdtd_batch *b, void **stream);
 int fdtd_check_cell_division(int dtype, double cell_size, int device, int64_t *tested,
                              int64_t *mismatches);
 
+/* Diagnostic (no counterpart in the reference): the boxes of the fused
+ * step's decomposition of a grid, host computation only (no device use).
+ * Rows of 7 ints (kind, x0, x1, y0, y1, z0, z1), kind 0 the interior
+ * z-march, 1 the CPML z slabs (with slab = 1, FDTD_OPT_FUSED_SLAB), 2 the
+ * shell swept by the split passes; every cell lies in exactly one box. */
+int fdtd_fused_plan_boxes(int nx, int ny, int nz, int npml, int tfsf_z, int tile_y, int zchunk,
+                          int slab, int *out, int cap, int *count);
+
 /* fdtd_near2far without any device allocation. This entry point has no
  * counterpart in the reference; it exists for callers that cannot call
  * cudaMalloc when they need a far field: code whose device memory is owned
@@ -306,6 +316,10 @@ typedef struct fdtd_incident fdtd_incident;
 int fdtd_incident_create(const fdtd_geometry *geom, int nt_pulse, int device,
                          fdtd_incident **out);
 int fdtd_incident_destroy(fdtd_incident *inc);
+/* FDTD_OPT_KERNEL (default FDTD_KERNEL_FUSED: the fused step, its source
+ * plane written after each step), FDTD_OPT_TILE_Y, FDTD_OPT_ZCHUNK,
+ * FDTD_OPT_FUSED_SLAB. */
+int fdtd_incident_set_option(fdtd_incident *inc, int option, int value);
 /* 8 * npml profiles, packed as for fdtd_set_absorbers (Absorbers(params)
  * of the incident simulation, cpu/fdtd_sim.py:14-23). */
 int fdtd_incident_set_absorbers(fdtd_incident *inc, const void *profiles);

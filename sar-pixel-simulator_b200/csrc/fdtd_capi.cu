@@ -96,15 +96,16 @@ struct fdtd_sim {
   int phasor_mode = FDTD_PHASOR_REFERENCE;
   int tile_x = 32, tile_y = 8;
   int zchunk = 0;
+  int slab = 0;                          // FDTD_OPT_FUSED_SLAB
   FusedPlan plan;
-  int plan_ok = 0, plan_tile_y = 0, plan_zchunk = 0;
+  int plan_ok = 0, plan_tile_y = 0, plan_zchunk = 0, plan_slab = 0;
   int graph_chunk = 0;
   int check_every = 0;
   // captured step chunks (FDTD_OPT_GRAPH_CHUNK), one per starting field set,
   // with the settings they were captured under; absorber uploads bump the
   // epoch (the profiles are captured by value)
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
-  int gsig[2][7] = {};
+  int gsig[2][8] = {};
   int graph_epoch = 0;
   // gradient (fdtd_grad_*): checkpoints of the forward solve, the segment
   // of recomputed states and the adjoint state; a state is the 6 fields
@@ -253,9 +254,13 @@ int enqueue_steps(fdtd_sim* s, int n, bool phasors = true) {
       const int nxt = 1 - s->cur;
       if (!fused_supported_tile(s->tile_x, s->tile_y, (int)sizeof(T)))
         return fail(FDTD_ERR_INVALID, "unsupported fused tile %dx%d", s->tile_x, s->tile_y);
-      if (!s->plan_ok || s->plan_tile_y != s->tile_y || s->plan_zchunk != s->zchunk) {
+      if (!s->plan_ok || s->plan_tile_y != s->tile_y || s->plan_zchunk != s->zchunk ||
+          s->plan_slab != s->slab) {
         const fdtd_geometry& g = s->g;
-        s->plan = make_fused_plan(g.nx, g.ny, g.nz, g.npml, g.tfsf_z, s->tile_y, s->zchunk);
+        s->plan = make_fused_plan(g.nx, g.ny, g.nz, g.npml, g.tfsf_z, s->tile_y, s->zchunk, s->slab != 0);
+        s->plan_slab = s->slab;
+        if (s->plan.shell.dropped)
+          return fail(FDTD_ERR_INVALID, "fused plan needs more than %d shell boxes", kMaxShellBoxes);
         s->plan_tile_y = s->tile_y;
         s->plan_zchunk = s->zchunk;
         s->plan_ok = 1;
@@ -267,6 +272,7 @@ int enqueue_steps(fdtd_sim* s, int n, bool phasors = true) {
       CK(cudaStreamWaitEvent(s->side, s->fork, 0));
       launch_shell_pass<T>(st, s->tdev, k, s->plan.shell, true, s->side);
       launch_fused_interior<T>(st, s->plan, s->tile_y, s->stream);
+      launch_fused_slab<T>(st, s->plan, s->tile_y, s->stream);
       CK(cudaEventRecord(s->join, s->side));
       CK(cudaStreamWaitEvent(s->stream, s->join, 0));
       State<T> se = st;
@@ -302,7 +308,7 @@ int enqueue_steps(fdtd_sim* s, int n, bool phasors = true) {
 template <class T>
 int enqueue_graph_chunk(fdtd_sim* s, int chunk) {
   const int start = s->cur;
-  const int sig[7] = {chunk, s->kernel, s->tile_x, s->tile_y, s->zchunk, s->phasor_mode, s->graph_epoch};
+  const int sig[8] = {chunk, s->kernel, s->tile_x, s->tile_y, s->zchunk, s->phasor_mode, s->graph_epoch, s->slab};
   if (!s->gexec[start] || memcmp(sig, s->gsig[start], sizeof(sig)) != 0) {
     if (s->gexec[start]) {
       cudaGraphExecDestroy(s->gexec[start]);
@@ -563,6 +569,9 @@ int fdtd_set_option(fdtd_sim* s, int option, int value) {
       if (value < 0) return fail(FDTD_ERR_INVALID, "bad z chunk %d", value);
       s->zchunk = value;
       return FDTD_OK;
+    case FDTD_OPT_FUSED_SLAB:
+      s->slab = value ? 1 : 0;
+      return FDTD_OK;
     case FDTD_OPT_GRAPH_CHUNK:
       if (value < 0) return fail(FDTD_ERR_INVALID, "bad graph chunk %d", value);
       s->graph_chunk = value;
@@ -586,6 +595,7 @@ int fdtd_get_option(fdtd_sim* s, int option, int* value) {
     case FDTD_OPT_TILE_X: *value = s->tile_x; return FDTD_OK;
     case FDTD_OPT_TILE_Y: *value = s->tile_y; return FDTD_OK;
     case FDTD_OPT_ZCHUNK: *value = s->zchunk; return FDTD_OK;
+    case FDTD_OPT_FUSED_SLAB: *value = s->slab; return FDTD_OK;
     case FDTD_OPT_GRAPH_CHUNK: *value = s->graph_chunk; return FDTD_OK;
     case FDTD_OPT_CHECK_EVERY: *value = s->check_every; return FDTD_OK;
     case FDTD_OPT_TIMING: *value = s->timing; return FDTD_OK;
@@ -1414,21 +1424,42 @@ int incident_run(fdtd_incident* b) {
   const State<T> st = make_state<T>(s, 0, 0);   // split passes in place on set 0
   const int* zero_t = s->tdev + 2;
   IncidentRecord<T> r;
-  r.ex = st.iex; r.ey = st.iey; r.hx = st.ihx; r.hy = st.ihy;
   r.rex = (T*)b->rec[0]; r.rey = (T*)b->rec[1]; r.rhx = (T*)b->rec[2]; r.rhy = (T*)b->rec[3];
   r.ph = (T*)b->iph;
   r.phase = s->phase;
   r.nx = g.nx; r.ny = g.ny; r.pitch = s->pitch; r.plane = s->plane;
   r.npml = g.npml; r.read_out = b->read_out; r.nx_ph = s->nx_ph; r.ny_ph = s->ny_ph;
-  for (int t = 0; t < g.nt; ++t) {
-    // E update and E CPML, hard source, H update and H CPML, read-out
-    // (cpu/incident_sim.py:134-160)
-    launch_shell_pass<T>(st, zero_t, t, whole, false, s->stream);
+  auto source = [&](int set, int t) {
     if (t < b->nt_pulse)
-      launch_inc_source<T>(st.oex, st.oey, (const T*)b->exc[0], (const T*)b->exc[1], g.nx, g.ny, s->pitch,
-                           s->plane, b->feed_in, t, s->stream);
-    launch_shell_pass<T>(st, zero_t, t, whole, true, s->stream);
-    launch_inc_record<T>(r, t, s->stream);
+      launch_inc_source<T>((T*)s->fld[set][0], (T*)s->fld[set][1], (const T*)b->exc[0], (const T*)b->exc[1],
+                           g.nx, g.ny, s->pitch, s->plane, b->feed_in, t, s->stream);
+  };
+  // E update and E CPML, hard source, H update and H CPML, read-out
+  // (cpu/incident_sim.py:134-160)
+  launch_shell_pass<T>(st, zero_t, 0, whole, false, s->stream);
+  source(0, 0);
+  if (s->kernel == FDTD_KERNEL_FUSED) {
+    // the fused step of t gives H^{t+1/2} and the next step's E update; the
+    // read-out takes E^t from the source set and H^{t+1/2} from the
+    // destination set, and the next step's source goes onto the destination
+    for (int t = 0; t < g.nt; ++t) {
+      const int src = s->cur;
+      if ((rc = enqueue_steps<T>(s, 1, false))) return rc;
+      r.ex = (const T*)s->fld[src][0]; r.ey = (const T*)s->fld[src][1];
+      r.hx = (const T*)s->fld[s->cur][3]; r.hy = (const T*)s->fld[s->cur][4];
+      launch_inc_record<T>(r, t, s->stream);
+      source(s->cur, t + 1);
+    }
+  } else {
+    r.ex = st.iex; r.ey = st.iey; r.hx = st.ihx; r.hy = st.ihy;
+    for (int t = 0; t < g.nt; ++t) {
+      if (t > 0) {
+        launch_shell_pass<T>(st, zero_t, t, whole, false, s->stream);
+        source(0, t);
+      }
+      launch_shell_pass<T>(st, zero_t, t, whole, true, s->stream);
+      launch_inc_record<T>(r, t, s->stream);
+    }
   }
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(s->stream));
@@ -1456,6 +1487,12 @@ int fdtd_incident_create(const fdtd_geometry* geom, int nt_pulse, int device, fd
     return rc;
   }
   fdtd_sim* s = b->sim;
+  // no injection plane: the fused step's interior and slab boxes cover every
+  // plane of the grid
+  s->g.tfsf_z = -2;
+  s->kernel = FDTD_KERNEL_FUSED;
+  s->tile_x = 32;
+  s->tile_y = 4;
   b->nt_pulse = std::min(nt_pulse, g.nt);   // the reference's loop ends at nt
   b->feed_in = g.nz / 2 + 4;                // cpu/incident_sim.py:101-103
   b->read_out = b->feed_in - 4;
@@ -1493,6 +1530,44 @@ int fdtd_incident_destroy(fdtd_incident* b) {
   if (b->sim) fdtd_destroy(b->sim);
   delete b;
   return FDTD_OK;
+}
+
+int fdtd_fused_plan_boxes(int nx, int ny, int nz, int npml, int tfsf_z, int tile_y, int zchunk, int slab,
+                          int* out, int cap, int* count) {
+  if (!out || !count || cap < 0) return fail(FDTD_ERR_INVALID, "null argument");
+  if (npml < 2 || npml > kMaxPml || nx < 2 * npml + 3 || ny < 2 * npml + 3 || nz < 2 * npml + 3)
+    return fail(FDTD_ERR_INVALID, "grid %dx%dx%d too small for npml %d", nz, ny, nx, npml);
+  const FusedPlan p = make_fused_plan(nx, ny, nz, npml, tfsf_z, tile_y, zchunk, slab != 0);
+  if (p.shell.dropped) return fail(FDTD_ERR_INVALID, "plan needs more than %d shell boxes", kMaxShellBoxes);
+  int n = 0;
+  auto put = [&](int kind, int x0, int x1, int y0, int y1, int z0, int z1) {
+    if (n < cap) {
+      int* r = out + 7 * n;
+      r[0] = kind; r[1] = x0; r[2] = x1; r[3] = y0; r[4] = y1; r[5] = z0; r[6] = z1;
+    }
+    ++n;
+  };
+  if (p.has_interior)
+    for (int k = 0; k < p.interior.nz_ranges; ++k)
+      put(0, p.interior.xa, p.interior.xb, p.interior.ya, p.interior.yb, p.interior.z0[k], p.interior.z1[k]);
+  if (p.has_slab)
+    for (int k = 0; k < p.slab.nz_ranges; ++k)
+      put(1, p.slab.xa, p.slab.xb, p.slab.ya, p.slab.yb, p.slab.z0[k], p.slab.z1[k]);
+  for (int k = 0; k < p.shell.n; ++k) {
+    const ShellBox& b = p.shell.b[k];
+    put(2, b.x0, b.x1, b.y0, b.y1, b.z0, b.z1);
+  }
+  *count = n;
+  return n <= cap ? FDTD_OK : fail(FDTD_ERR_INVALID, "%d boxes, room for %d", n, cap);
+}
+
+int fdtd_incident_set_option(fdtd_incident* b, int option, int value) {
+  int rc = check_inc(b);
+  if (rc) return rc;
+  if (option != FDTD_OPT_KERNEL && option != FDTD_OPT_TILE_Y && option != FDTD_OPT_ZCHUNK &&
+      option != FDTD_OPT_FUSED_SLAB)
+    return fail(FDTD_ERR_INVALID, "option %d does not apply to an incident run", option);
+  return fdtd_set_option(b->sim, option, value);
 }
 
 int fdtd_incident_set_absorbers(fdtd_incident* b, const void* profiles) {

@@ -116,9 +116,10 @@ struct ShellBox {
   int width, gx, gy;
   int first;
 };
-constexpr int kMaxShellBoxes = 16;
+constexpr int kMaxShellBoxes = 24;
 struct ShellBoxes {
   int n, total_blocks;
+  int dropped;   // boxes that did not fit (a plan with any is rejected)
   ShellBox b[kMaxShellBoxes];
 };
 

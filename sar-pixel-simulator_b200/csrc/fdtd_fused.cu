@@ -12,11 +12,14 @@
 //    and Cb once and writes every field once (56 B per FP32 cell-update),
 //    with no boundary code at all, so nothing diverges and the kernel needs
 //    few registers;
-//  * the shell (CPML slabs, the injection planes, the strips beside the
-//    interior box): the split H pass over the shell boxes (source E, H ->
-//    destination H), then the split E pass (destination H, source E ->
-//    destination E). The E pass runs after the interior pass, whose
-//    destination H it reads at the shell's inner edge.
+//  * the z slabs of the same x-y box (the bottom and top npml planes): the
+//    same march with the z-face CPML terms, whose coefficients are uniform
+//    over a plane (k_fused_slab);
+//  * the shell (x and y CPML strips, the injection planes, the domain's
+//    edge rows and columns): the split H pass over the shell boxes (source
+//    E, H -> destination H), then the split E pass (destination H, source
+//    E -> destination E). The E pass runs after the interior and slab
+//    passes, whose destination H it reads at the shell's inner edge.
 //
 // Interior kernel. A block owns a tile of 128 x cells (32 lanes x 4 cells)
 // by TY rows and a chunk of z planes, and marches up the chunk one plane at
@@ -142,6 +145,173 @@ k_fused_interior(const __grid_constant__ State<T> s, InteriorBox ib) {
   }
 }
 
+// The z slabs of the same x-y box: z in [0, npml) and [nz - npml, nz), one
+// chunk each (blockIdx.z), marched like the interior. Every plane carries
+// z-face CPML terms with coefficients uniform over the plane (Taflove 7.x:
+// psi_H = bh psi_H + (ch / dx) dE, psi_E = be psi_E + (ce / dx) dH,
+// cpu/field_updates.py:66-105, 243-282), applied after the curl update of
+// the same component as the split kernels apply them; the domain's first and
+// last planes keep the components outside their update ranges
+// (cpu/field_updates.py:18-63, 198-240). No x or y face touches the box.
+template <class T, int TY>
+__global__ void __launch_bounds__(kLanes * (TY + 1), 1)
+k_fused_slab(const __grid_constant__ State<T> s, InteriorBox ib) {
+  using M = R<T>;
+  __shared__ __align__(32) T sEx[TY + 1][kRowCells];
+  __shared__ __align__(32) T sEz[TY + 1][kRowCells];
+  __shared__ __align__(32) T sHx[TY + 1][kRowCells];
+  __shared__ __align__(32) T sHz[TY + 1][kRowCells];
+
+  const int nz = s.nz, m = s.npml;
+  const int lane = threadIdx.x, r = threadIdx.y;
+  const int x0 = ib.xa + blockIdx.x * kRowCells + lane * kVec;
+  const int y = ib.ya + blockIdx.y * TY + r - 1;
+  const int k = blockIdx.z;
+  const int z0 = ib.z0[k], z1 = ib.z1[k];
+  const int zs = max(z0 - 1, 0);   // the bottom slab starts at plane 0: nothing below
+  const bool vin = x0 < s.pitch && y < s.ny;
+  const bool own = vin && r >= 1 && y < ib.yb && x0 < ib.xb;
+  const long long P = s.plane, W = s.pitch;
+  long long i = (long long)zs * P + (vin ? (long long)y * W + x0 : 0);
+  const int so = lane * kVec;
+
+  EVec<T> e;
+  HVec<T> h;
+  T ezz[kVec];
+  if (vin) { ld4(e.ex, s.iex + i); ld4(e.ey, s.iey + i); ld4(e.ez, s.iez + i); }
+  else { zero4(e.ex); zero4(e.ey); zero4(e.ez); }
+  zero4(h.hxz); zero4(h.hyz);
+
+  for (int z = zs; z < z1; ++z, i += P) {
+    const bool work = own && z >= z0;
+    const bool top = z + 1 >= nz;   // last plane: nothing above, nothing updated
+    // update ranges and CPML faces of plane z (uniform over the plane)
+    const bool h_xy = z < nz - 1, h_z = z >= 1 && z < nz - 1;
+    const bool e_xy = z >= 1 && z < nz - 1, e_z = z < nz - 1;
+    const bool hf = z < nz - 1 && (z < m - 1 || z >= nz - m);
+    const bool ef = z < nz - 1 && ((z >= 1 && z < m) || z >= nz - m);
+    const int hside = z < m - 1 ? 0 : 1, hq = hside ? z - (nz - m) : z;
+    const int eside = z < m ? 0 : 1, eq = eside ? z - (nz - m) : z;
+    if (vin && !top) {
+      ld4(e.exz, s.iex + i + P); ld4(e.eyz, s.iey + i + P); ld4(ezz, s.iez + i + P);
+    } else {
+      zero4(e.exz); zero4(e.eyz); zero4(ezz);
+    }
+    if (vin) { ld4(h.hx, s.ihx + i); ld4(h.hy, s.ihy + i); ld4(h.hz, s.ihz + i); }
+    else { zero4(h.hx); zero4(h.hy); zero4(h.hz); }
+    T ca[kVec], cb[kVec];
+    if (work) { ld4(ca, s.ca + i); ld4(cb, s.cb + i); }
+    else { zero4(ca); zero4(cb); }
+    if (r == TY) {
+      if (vin && y + 1 < s.ny) { ld4(e.exy, s.iex + i + W); ld4(e.ezy, s.iez + i + W); }
+      else { zero4(e.exy); zero4(e.ezy); }
+    }
+    T eyr = T(0), ezr = T(0);
+    if (lane == kLanes - 1 && vin && x0 + kVec < s.pitch) { eyr = s.iey[i + kVec]; ezr = s.iez[i + kVec]; }
+    T gx = T(0), gy = T(0), gz = T(0), gxz = T(0), gxy = T(0), ghy = T(0), ghz = T(0), gpy = T(0);
+    if (work && lane == 0) {
+      const long long j = i - 1;
+      gx = s.iex[j]; gy = s.iey[j]; gz = s.iez[j];
+      ghy = s.ihy[j]; ghz = s.ihz[j];
+      gxz = top ? T(0) : s.iex[j + P];
+      gxy = s.iex[j + W];
+      if (hf) gpy = s.ps.z[hside][3][((long long)hq * s.ny + y) * W + x0 - 1];
+    }
+    // ---- H^{n+1/2}(z) -----------------------------------------------------
+    st4(&sEx[r][so], e.ex);
+    st4(&sEz[r][so], e.ez);
+    __syncthreads();
+    if (r < TY) { ld4(e.exy, &sEx[r + 1][so]); ld4(e.ezy, &sEz[r + 1][so]); }
+    e.eyn = __shfl_down_sync(kFull, e.ey[0], 1);
+    e.ezn = __shfl_down_sync(kFull, e.ez[0], 1);
+    if (lane == kLanes - 1) { e.eyn = eyr; e.ezn = ezr; }
+    {
+      T hx[kVec], hy[kVec], hz[kVec];
+      copy4(hx, h.hx); copy4(hy, h.hy); copy4(hz, h.hz);
+      h_vec_interior(s, e, hx, hy, hz);
+      if (h_xy) { copy4(h.hx, hx); copy4(h.hy, hy); }
+      if (h_z) copy4(h.hz, hz);
+    }
+    if (hf) {   // z faces: psi_Hyz from dEx/dz, psi_Hxz from dEy/dz
+      const long long kq = ((long long)hq * s.ny + y) * W + x0;
+      const T b = s.prof[hside ? BH_U : BH_D][hq];
+      const T c = s.prof[hside ? CH_U : CH_D][hq];
+      T p3[kVec], p2[kVec];
+      if (vin) { ld4(p3, s.ps.z[hside][3] + kq); ld4(p2, s.ps.z[hside][2] + kq); }
+      else { zero4(p3); zero4(p2); }
+#pragma unroll
+      for (int j = 0; j < kVec; ++j) {
+        p3[j] = M::add(M::mul(b, p3[j]), div_dx(s, M::mul(c, M::sub(e.exz[j], e.ex[j]))));
+        p2[j] = M::add(M::mul(b, p2[j]), div_dx(s, M::mul(c, M::sub(e.eyz[j], e.ey[j]))));
+        h.hy[j] = M::sub(h.hy[j], M::mul(s.dtm0, p3[j]));
+        h.hx[j] = M::add(h.hx[j], M::mul(s.dtm0, p2[j]));
+      }
+      if (work) { st4(s.pd.z[hside][3] + kq, p3); st4(s.pd.z[hside][2] + kq, p2); }
+    }
+    st4(&sHx[r][so], h.hx);
+    st4(&sHz[r][so], h.hz);
+    __syncthreads();
+    // ---- E^{n+1}(z) ---------------------------------------------------------
+    h.hyp = __shfl_up_sync(kFull, h.hy[kVec - 1], 1);
+    h.hzp = __shfl_up_sync(kFull, h.hz[kVec - 1], 1);
+    if (work) {
+      ld4(h.hxy, &sHx[r - 1][so]);
+      ld4(h.hzy, &sHz[r - 1][so]);
+      if (lane == 0) {   // hy, hz at x0 - 1, with the z-face term of hy
+        T hyp = ghy, hzp = ghz;
+        if (h_xy) {
+          hyp = M::sub(ghy, M::mul(s.db, M::sub(M::sub(gxz, gx), M::sub(e.ez[0], gz))));
+          if (hf) {
+            const T b = s.prof[hside ? BH_U : BH_D][hq];
+            const T c = s.prof[hside ? CH_U : CH_D][hq];
+            const T p3 = M::add(M::mul(b, gpy), div_dx(s, M::mul(c, M::sub(gxz, gx))));
+            hyp = M::sub(hyp, M::mul(s.dtm0, p3));
+          }
+        }
+        if (h_z) hzp = M::sub(ghz, M::mul(s.db, M::sub(M::sub(e.ey[0], gy), M::sub(gxy, gx))));
+        h.hyp = hyp;
+        h.hzp = hzp;
+      }
+      T ex[kVec], ey[kVec], ez[kVec];
+      copy4(ex, e.ex); copy4(ey, e.ey); copy4(ez, e.ez);
+      e_vec_interior(h, ca, cb, ex, ey, ez);
+      T ox[kVec], oy[kVec], oz[kVec];
+      copy4(ox, e.ex); copy4(oy, e.ey); copy4(oz, e.ez);
+      if (e_xy) { copy4(ox, ex); copy4(oy, ey); }
+      if (e_z) copy4(oz, ez);
+      if (ef) {   // z faces: psi_Eyz from dHx/dz, psi_Exz from dHy/dz
+        const long long kq = ((long long)eq * s.ny + y) * W + x0;
+        const T b = s.prof[eside ? BE_U : BE_D][eq];
+        const T c = s.prof[eside ? CE_U : CE_D][eq];
+        T p1[kVec], p0[kVec];
+        ld4(p1, s.ps.z[eside][1] + kq);
+        ld4(p0, s.ps.z[eside][0] + kq);
+#pragma unroll
+        for (int j = 0; j < kVec; ++j) {
+          const T cbdx = M::mul(cb[j], s.dx);
+          p1[j] = M::add(M::mul(b, p1[j]), div_dx(s, M::mul(c, M::sub(h.hx[j], h.hxz[j]))));
+          p0[j] = M::add(M::mul(b, p0[j]), div_dx(s, M::mul(c, M::sub(h.hy[j], h.hyz[j]))));
+          oy[j] = M::add(oy[j], M::mul(cbdx, p1[j]));
+          ox[j] = M::sub(ox[j], M::mul(cbdx, p0[j]));
+        }
+        st4(s.pd.z[eside][1] + kq, p1);
+        st4(s.pd.z[eside][0] + kq, p0);
+      }
+      st4(s.ohx + i, h.hx); st4(s.ohy + i, h.hy); st4(s.ohz + i, h.hz);
+      st4(s.oex + i, ox); st4(s.oey + i, oy); st4(s.oez + i, oz);
+    }
+    copy4(e.ex, e.exz); copy4(e.ey, e.eyz); copy4(e.ez, ezz);
+    copy4(h.hxz, h.hx); copy4(h.hyz, h.hy);
+  }
+}
+
+template <class T, int TY>
+void launch_slab_ty(const State<T>& s, const InteriorBox& sb, cudaStream_t st) {
+  const dim3 blk(kLanes, TY + 1, 1);
+  const dim3 grd((sb.xb - sb.xa + kRowCells - 1) / kRowCells, (sb.yb - sb.ya + TY - 1) / TY, sb.nz_ranges);
+  k_fused_slab<T, TY><<<grd, blk, 0, st>>>(s, sb);
+}
+
 template <class T, int TY>
 void launch_interior_ty(const State<T>& s, const InteriorBox& ib, cudaStream_t st) {
   const dim3 blk(kLanes, TY + 1, 1);
@@ -163,11 +333,14 @@ bool fused_supported_tile(int tile_x, int tile_y, int elem_bytes) {
 // planes; E faces 1 <= q < npml below), from the domain edges and from the
 // injection plane tfsf_z (and tfsf_z + 1, whose recomputed plane below would
 // be the injection plane).
-FusedPlan make_fused_plan(int nx, int ny, int nz, int npml, int tfsf_z, int tile_y, int zchunk) {
+FusedPlan make_fused_plan(int nx, int ny, int nz, int npml, int tfsf_z, int tile_y, int zchunk,
+                          bool use_slab) {
   FusedPlan p;
   memset(&p, 0, sizeof(p));
   const int m = npml;
   InteriorBox& ib = p.interior;
+  // rows start on a 128-byte line (starting at npml rounded up to 4 cells
+  // instead left 48-byte offsets and measured 5 % slower at 203 x 761 x 761)
   ib.xa = (m + 31) / 32 * 32;
   ib.xb = (nx - m) / kVec * kVec;
   ib.ya = m;
@@ -175,7 +348,7 @@ FusedPlan make_fused_plan(int nx, int ny, int nz, int npml, int tfsf_z, int tile
   // interior z ranges: [m, nz - m) without tfsf_z, tfsf_z + 1
   int zr[2][2] = {{0, 0}, {0, 0}}, nzr = 0;
   const int za = m, zb = nz - m;
-  if (tfsf_z >= za && tfsf_z < zb) {
+  if (tfsf_z >= za - 1 && tfsf_z < zb) {   // also the plane below the first chunk
     if (tfsf_z > za) { zr[nzr][0] = za; zr[nzr][1] = tfsf_z; ++nzr; }
     if (tfsf_z + 2 < zb) { zr[nzr][0] = tfsf_z + 2; zr[nzr][1] = zb; ++nzr; }
   } else if (za < zb) {
@@ -187,6 +360,24 @@ FusedPlan make_fused_plan(int nx, int ny, int nz, int npml, int tfsf_z, int tile
     add_shell_box(bl, 0, nx, 0, ny, 0, nz);
     return p;
   }
+  // with use_slab, the z slabs of the same x-y box (CPML in z only):
+  // [0, m) and [nz - m, nz), each unless the injection plane lies in it or
+  // is the plane below it (the slab kernel does not inject); otherwise the
+  // split passes sweep the whole slab planes
+  InteriorBox& sb = p.slab;
+  sb = ib;
+  sb.nz_ranges = 0;
+  const int slab[2][2] = {{0, m}, {nz - m, nz}};
+  for (int k = 0; k < 2 && use_slab; ++k) {
+    if (tfsf_z >= slab[k][0] - 1 && tfsf_z < slab[k][1]) continue;
+    sb.z0[sb.nz_ranges] = slab[k][0];
+    sb.z1[sb.nz_ranges] = slab[k][1];
+    ++sb.nz_ranges;
+  }
+  sb.zchunk = m;
+  sb.chunks0 = 1;
+  sb.chunks = sb.nz_ranges;
+  p.has_slab = sb.nz_ranges > 0;
   int planes = 0;
   for (int k = 0; k < nzr; ++k) planes += zr[k][1] - zr[k][0];
   if (zchunk <= 0) {
@@ -209,19 +400,25 @@ FusedPlan make_fused_plan(int nx, int ny, int nz, int npml, int tfsf_z, int tile
     if (k == 0) ib.chunks0 = ch;
     ib.chunks += ch;
   }
-  // the shell: z planes outside the interior ranges (whole planes), then per
-  // interior range the y strips (whole rows) and the x strips
+  // the shell: z planes that neither box covers (whole planes), then per
+  // covered z range (slabs and interior ranges, in z order) the y strips
+  // (whole rows) and the x strips beside the box
+  int cz0[4], cz1[4], nc = 0;
+  if (sb.nz_ranges > 0 && sb.z0[0] == 0) { cz0[nc] = sb.z0[0]; cz1[nc++] = sb.z1[0]; }
+  for (int k = 0; k < nzr; ++k) { cz0[nc] = ib.z0[k]; cz1[nc++] = ib.z1[k]; }
+  for (int k = 0; k < sb.nz_ranges; ++k)
+    if (sb.z0[k] != 0) { cz0[nc] = sb.z0[k]; cz1[nc++] = sb.z1[k]; }
   int zc = 0;
-  for (int k = 0; k < nzr; ++k) {
-    add_shell_box(bl, 0, nx, 0, ny, zc, ib.z0[k]);
-    zc = ib.z1[k];
+  for (int k = 0; k < nc; ++k) {
+    add_shell_box(bl, 0, nx, 0, ny, zc, cz0[k]);
+    zc = cz1[k];
   }
   add_shell_box(bl, 0, nx, 0, ny, zc, nz);
-  for (int k = 0; k < nzr; ++k) {
-    add_shell_box(bl, 0, nx, 0, ib.ya, ib.z0[k], ib.z1[k]);
-    add_shell_box(bl, 0, nx, ib.yb, ny, ib.z0[k], ib.z1[k]);
-    add_shell_box(bl, 0, ib.xa, ib.ya, ib.yb, ib.z0[k], ib.z1[k]);
-    add_shell_box(bl, ib.xb, nx, ib.ya, ib.yb, ib.z0[k], ib.z1[k]);
+  for (int k = 0; k < nc; ++k) {
+    add_shell_box(bl, 0, nx, 0, ib.ya, cz0[k], cz1[k]);
+    add_shell_box(bl, 0, nx, ib.yb, ny, cz0[k], cz1[k]);
+    add_shell_box(bl, 0, ib.xa, ib.ya, ib.yb, cz0[k], cz1[k]);
+    add_shell_box(bl, ib.xb, nx, ib.ya, ib.yb, cz0[k], cz1[k]);
   }
   return p;
 }
@@ -243,6 +440,25 @@ bool launch_fused_interior(const State<T>& s, const FusedPlan& p, int tile_y, cu
   return false;
 }
 
+template <class T>
+bool launch_fused_slab(const State<T>& s, const FusedPlan& p, int tile_y, cudaStream_t st) {
+  if (!p.has_slab) return true;
+  switch (tile_y) {
+    case 4: launch_slab_ty<T, 4>(s, p.slab, st); return true;
+    case 7: launch_slab_ty<T, 7>(s, p.slab, st); return true;
+    case 8: launch_slab_ty<T, 8>(s, p.slab, st); return true;
+  }
+  if constexpr (sizeof(T) == 4) {
+    switch (tile_y) {
+      case 15: launch_slab_ty<T, 15>(s, p.slab, st); return true;
+      case 16: launch_slab_ty<T, 16>(s, p.slab, st); return true;
+    }
+  }
+  return false;
+}
+
+template bool launch_fused_slab<float>(const State<float>&, const FusedPlan&, int, cudaStream_t);
+template bool launch_fused_slab<double>(const State<double>&, const FusedPlan&, int, cudaStream_t);
 template bool launch_fused_interior<float>(const State<float>&, const FusedPlan&, int, cudaStream_t);
 template bool launch_fused_interior<double>(const State<double>&, const FusedPlan&, int, cudaStream_t);
 

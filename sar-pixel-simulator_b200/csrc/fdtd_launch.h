@@ -34,18 +34,25 @@ void launch_eps_sigma(int nx, int ny, int nz, int nz_mat, int pitch, const T* ep
 struct FusedPlan {
   int has_interior;
   InteriorBox interior;
+  int has_slab;
+  InteriorBox slab;   // the z slabs [0, npml), [nz - npml, nz) of the same x-y box
   ShellBoxes shell;
 };
 
-// Interior box and shell boxes of a grid; zchunk 0 picks the z chunk.
-FusedPlan make_fused_plan(int nx, int ny, int nz, int npml, int tfsf_z, int tile_y, int zchunk);
+// Interior box, z slabs (with use_slab) and shell boxes of a grid; zchunk 0
+// picks the z chunk.
+FusedPlan make_fused_plan(int nx, int ny, int nz, int npml, int tfsf_z, int tile_y, int zchunk,
+                          bool use_slab);
 
 // Tile shapes the interior kernel is built for: 32 lanes wide, tile_y rows.
 bool fused_supported_tile(int tile_x, int tile_y, int elem_bytes);
 
-// Interior pass: reads the source set, writes the destination set.
+// Interior pass and z-slab pass: read the source set, write the
+// destination set.
 template <class T>
 bool launch_fused_interior(const State<T>& s, const FusedPlan& p, int tile_y, cudaStream_t st);
+template <class T>
+bool launch_fused_slab(const State<T>& s, const FusedPlan& p, int tile_y, cudaStream_t st);
 
 // Appends the box [x0, x1) x [y0, y1) x [z0, z1) to a box list, with the
 // row width (32, 16 or 8 lanes) that pads x the least.

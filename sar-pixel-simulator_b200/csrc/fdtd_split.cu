@@ -298,7 +298,11 @@ __global__ void k_eps_sigma(int nx, int ny, int nz, int nz_mat, int pitch,
 // launchers
 // ---------------------------------------------------------------------------
 void add_shell_box(ShellBoxes& bl, int x0, int x1, int y0, int y1, int z0, int z1) {
-  if (x0 >= x1 || y0 >= y1 || z0 >= z1 || bl.n >= kMaxShellBoxes) return;
+  if (x0 >= x1 || y0 >= y1 || z0 >= z1) return;
+  if (bl.n >= kMaxShellBoxes) {
+    ++bl.dropped;
+    return;
+  }
   ShellBox& b = bl.b[bl.n++];
   b.x0 = x0; b.x1 = x1; b.y0 = y0; b.y1 = y1; b.z0 = z0; b.z1 = z1;
   // row width with the least x padding (ties: the wider rows)

@@ -36,6 +36,7 @@ OPT_GRAPH_CHUNK = 5
 OPT_CHECK_EVERY = 6
 OPT_TIMING = 7
 OPT_ZCHUNK = 8
+OPT_FUSED_SLAB = 9
 
 TIME_STEP = 0
 TIME_PHASOR = 1
@@ -114,8 +115,10 @@ SIGNATURES = {
     'fdtd_check_cell_division': [_I, _D, _I, ctypes.POINTER(ctypes.c_int64),
                                  ctypes.POINTER(ctypes.c_int64)],
     'fdtd_near2far_noalloc': [_P, _P, _P, _P, _I, _I, _I, _I, _D, _D, _P, _I, _P, _I, _D, _I, _P],
+    'fdtd_fused_plan_boxes': [_I, _I, _I, _I, _I, _I, _I, _I, _P, _I, ctypes.POINTER(_I)],
     'fdtd_incident_create': [ctypes.POINTER(Geometry), _I, _I, ctypes.POINTER(_P)],
     'fdtd_incident_destroy': [_P],
+    'fdtd_incident_set_option': [_P, _I, _I],
     'fdtd_incident_set_absorbers': [_P, _P],
     'fdtd_incident_make_excitation': [_P, _P, _P, _I, _D, _D, _I, _D, ctypes.POINTER(_D)],
     'fdtd_incident_set_excitation': [_P, _P, _P],
@@ -354,6 +357,9 @@ class NativeIncident:
         except Exception:
             pass
 
+    def set_option(self, opt, value):
+        check(lib.fdtd_incident_set_option(self.h, int(opt), int(value)))
+
     def set_absorbers(self, packed):
         a = np.ascontiguousarray(packed, dtype=self.dtype)
         if a.shape != (8 * self.geom.npml,):
@@ -439,6 +445,16 @@ def check_cell_division(dtype, cell_size, device=0):
     check(lib.fdtd_check_cell_division(dtype_code(dtype), float(cell_size), int(device),
                                        ctypes.byref(tested), ctypes.byref(bad)))
     return tested.value, bad.value
+
+
+def fused_plan_boxes(nx, ny, nz, npml, tfsf_z, tile_y=4, zchunk=0, slab=False):
+    """(kind, x0, x1, y0, y1, z0, z1) rows of the fused step's boxes
+    (fdtd_fused_plan_boxes; host computation, no device needed)."""
+    out = np.zeros((64, 7), np.int32)
+    n = ctypes.c_int(0)
+    check(lib.fdtd_fused_plan_boxes(int(nx), int(ny), int(nz), int(npml), int(tfsf_z), int(tile_y),
+                                    int(zchunk), int(bool(slab)), ptr(out), out.shape[0], ctypes.byref(n)))
+    return out[:n.value].copy()
 
 
 class Batch:

@@ -19,13 +19,16 @@ from . import _native
 
 DEFAULT_TILE = (32, 4)
 
-# (kernel, tile_y, zchunk); zchunk 0 lets the library pick
+# (kernel, tile_y, zchunk, slab); zchunk 0 lets the library pick; slab 1
+# marches the CPML z slabs with the fused step too
 CANDIDATES = [
-    (_native.FDTD_KERNEL_SPLIT, 4, 0),
-    (_native.FDTD_KERNEL_FUSED, 4, 0),
-    (_native.FDTD_KERNEL_FUSED, 4, 26),
-    (_native.FDTD_KERNEL_FUSED, 7, 0),
-    (_native.FDTD_KERNEL_FUSED, 8, 0),
+    (_native.FDTD_KERNEL_SPLIT, 4, 0, 0),
+    (_native.FDTD_KERNEL_FUSED, 4, 0, 0),
+    (_native.FDTD_KERNEL_FUSED, 4, 26, 0),
+    (_native.FDTD_KERNEL_FUSED, 7, 0, 0),
+    (_native.FDTD_KERNEL_FUSED, 8, 0, 0),
+    (_native.FDTD_KERNEL_FUSED, 4, 0, 1),
+    (_native.FDTD_KERNEL_FUSED, 7, 0, 1),
 ]
 
 
@@ -61,15 +64,15 @@ def lookup(geom, device=0):
 
 
 def choose(geom, kernel=None, tile=None, device=0, use_cache=True):
-    """{'kernel', 'tile_x', 'tile_y', 'zchunk'} for a geometry."""
+    """{'kernel', 'tile_x', 'tile_y', 'zchunk', 'slab'} for a geometry."""
     if kernel is None and tile is None and use_cache:
         hit = lookup(geom, device)
         if hit:
             return {'kernel': int(hit['kernel']), 'tile_x': 32, 'tile_y': int(hit['tile_y']),
-                    'zchunk': int(hit['zchunk'])}
+                    'zchunk': int(hit['zchunk']), 'slab': int(hit.get('slab', 0))}
     k = _native.FDTD_KERNEL_FUSED if kernel is None else int(kernel)
     tx, ty = tile if tile is not None else DEFAULT_TILE
-    return {'kernel': k, 'tile_x': int(tx), 'tile_y': int(ty), 'zchunk': 0}
+    return {'kernel': k, 'tile_x': int(tx), 'tile_y': int(ty), 'zchunk': 0, 'slab': 0}
 
 
 def apply(sim, choice):
@@ -79,6 +82,7 @@ def apply(sim, choice):
         sim.set_option(_native.OPT_TILE_X, choice['tile_x'])
         sim.set_option(_native.OPT_TILE_Y, choice['tile_y'])
         sim.set_option(_native.OPT_ZCHUNK, choice.get('zchunk', 0))
+        sim.set_option(_native.OPT_FUSED_SLAB, choice.get('slab', 0))
 
 
 def autotune(geom, device=0, steps=6, candidates=None, save=True):
@@ -101,8 +105,8 @@ def autotune(geom, device=0, steps=6, candidates=None, save=True):
     cb = np.full((g.nz, g.ny, g.nx), g.dte0dx, ft)
     sim.set_materials(ca, cb)
     timings = []
-    for kernel, ty, zc in (candidates or CANDIDATES):
-        choice = {'kernel': kernel, 'tile_x': 32, 'tile_y': ty, 'zchunk': zc}
+    for kernel, ty, zc, slab in (candidates or CANDIDATES):
+        choice = {'kernel': kernel, 'tile_x': 32, 'tile_y': ty, 'zchunk': zc, 'slab': slab}
         try:
             apply(sim, choice)
             sim.reset()

@@ -61,7 +61,7 @@ def oracle_for(pc):
                        pc.processing_params.datatype, cpml_profiles(pc))
 
 
-def native_for(pc, kernel=_native.FDTD_KERNEL_SPLIT, tile=(32, 8), phasor_mode=0, zchunk=0):
+def native_for(pc, kernel=_native.FDTD_KERNEL_SPLIT, tile=(32, 8), phasor_mode=0, zchunk=0, slab=False):
     from fdtdsarsim_b200.gpu.main_sim import native_geometry
     sim = _native.NativeSim(native_geometry(pc), 0)
     sim.set_absorbers(packed_profiles(pc))
@@ -70,6 +70,7 @@ def native_for(pc, kernel=_native.FDTD_KERNEL_SPLIT, tile=(32, 8), phasor_mode=0
         sim.set_option(_native.OPT_TILE_X, tile[0])
         sim.set_option(_native.OPT_TILE_Y, tile[1])
         sim.set_option(_native.OPT_ZCHUNK, zchunk)
+        sim.set_option(_native.OPT_FUSED_SLAB, int(slab))
     sim.set_option(_native.OPT_PHASOR_MODE, phasor_mode)
     return sim
 

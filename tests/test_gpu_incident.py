@@ -64,11 +64,15 @@ def test_excitation_matches_reference(tag):
         assert np.max(np.abs(ey - g['exc_ey_imag'])) <= tol
 
 
-def test_run_bit_exact_from_reference_excitation():
+@pytest.mark.parametrize('kernel', [_native.FDTD_KERNEL_SPLIT, _native.FDTD_KERNEL_FUSED],
+                         ids=['split', 'fused'])
+def test_run_bit_exact_from_reference_excitation(kernel):
     """From the reference's excitation, the recorded planes and incident
-    phasors equal the reference's bit for bit (float32)."""
+    phasors equal the reference's bit for bit (float32), on the split step
+    and on the fused step (whose source plane is written after each step)."""
     g = load('hh_f32')
     inc = native_incident(g)
+    inc.set_option(_native.OPT_KERNEL, kernel)
     try:
         inc.set_excitation(g['exc_ex_imag'], g['exc_ey_imag'])
         inc.run()

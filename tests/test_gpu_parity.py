@@ -35,6 +35,10 @@ WIDE = [
     # injection plane at the lower / upper end of the fused interior z range
     (300, 70, 40, 10, 12, 8, 'float32'),
     (173, 53, 40, 28, 12, 8, 'float32'),
+    # injection plane just below the interior (npml - 1) and just below the
+    # upper CPML slab (nz - npml - 1): neither box may march through it
+    (41, 37, 29, 9, 20, 15, 'float32'),
+    (41, 37, 29, 18, 20, 15, 'float32'),
 ]
 
 
@@ -75,6 +79,27 @@ def test_fused_matches_oracle_bit_exact(case):
     orc, sim = _run_both(case, seed=202, kernel=FUSED)
     _assert_matches(orc, sim)
     sim.close()
+
+
+@pytest.mark.parametrize('case', CASES + WIDE)
+def test_fused_slab_matches_oracle_bit_exact(case):
+    """FDTD_OPT_FUSED_SLAB: the CPML z slabs marched by the slab kernel."""
+    pc = make_params(*case[:6], dtype=case[6])
+    _, _, ca, cb, inc = random_problem(pc, 71)
+    o = oracle_for(pc)
+    o.run(ca, cb, inc, pc.geom_params.size_t)
+    sim = native_for(pc, FUSED, (32, 4), slab=True)
+    try:
+        sim.set_materials(ca, cb)
+        sim.set_incident(inc['ex'], inc['ey'], inc['hx'], inc['hy'])
+        sim.run(pc.geom_params.size_t)
+        sim.synchronize()
+        for c in ('ex', 'ey', 'ez', 'hx', 'hy', 'hz'):
+            assert bits_equal(sim.get_field(c), getattr(o, c)), c
+        for k, name in enumerate(_native.PHASOR_NAMES):
+            assert bits_equal(sim.get_phasor(k), o.ph[name]), name
+    finally:
+        sim.close()
 
 
 @pytest.mark.parametrize('tile_y,zchunk', [(4, 3), (7, 5), (8, 0), (15, 7), (16, 1)])
