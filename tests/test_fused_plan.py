@@ -34,4 +34,5 @@ def test_boxes_partition_the_grid(grid, tile_y, slab):
         if kind == 0:   # the interior: no z face either
             assert z0 - 1 >= m - 1 and z1 <= nz - m
     assert (count == 1).all()
-    assert (boxes[:, 0] == 0).any()
+    if nx - m >= 36:   # room for a 32-aligned interior start
+        assert (boxes[:, 0] == 0).any()
