@@ -104,8 +104,13 @@ __device__ __forceinline__ const ShellBox& find_box(const ShellBoxes& bl, int bi
   return bl.b[k];
 }
 
+// Resident blocks per SM the split passes ask for (float: register cap 72;
+// the passes are latency-bound, so more warps in flight beat a few spills)
+template <class T>
+constexpr int split_min_blocks() { return sizeof(T) == 4 ? 7 : 1; }
+
 template <class T, bool kH>
-__global__ void __launch_bounds__(128) k_shell(State<T> s, const int* __restrict__ tp, int toff,
+__global__ void __launch_bounds__(128, split_min_blocks<T>()) k_shell(State<T> s, const int* __restrict__ tp, int toff,
                                                ShellBoxes bl) {
   const int bid = blockIdx.x;
   const ShellBox& b = find_box(bl, bid);
@@ -225,11 +230,21 @@ __device__ __forceinline__ int find_model(const int* __restrict__ start, int n, 
 }
 
 template <class T, bool kH>
-__global__ void __launch_bounds__(128) k_batch_split(const BatchModel<T>* __restrict__ bm,
+__global__ void __launch_bounds__(128, split_min_blocks<T>()) k_batch_split(const BatchModel<T>* __restrict__ bm,
                                                      const int* __restrict__ start, int n, int toff) {
   const int bid = blockIdx.x;
   const int mi = find_model(start, n, bid);
   const BatchModel<T>& b = bm[mi];
+  // the member's State, staged once per block in shared memory: the update
+  // reads its scalars, pointers and profiles many times per thread
+  static_assert(sizeof(State<T>) % 8 == 0, "State is copied in 8-byte words");
+  __shared__ unsigned long long st_words[sizeof(State<T>) / 8];
+  {
+    const unsigned long long* src = reinterpret_cast<const unsigned long long*>(&b.s);
+    for (int k = threadIdx.x; k < (int)(sizeof(State<T>) / 8); k += blockDim.x) st_words[k] = src[k];
+  }
+  __syncthreads();
+  const State<T>& s = *reinterpret_cast<const State<T>*>(st_words);
   int local = bid - start[mi];
   const int bx = local % b.gx;
   local /= b.gx;
@@ -239,8 +254,8 @@ __global__ void __launch_bounds__(128) k_batch_split(const BatchModel<T>* __rest
   const int x0 = (bx * b.width + lane) * kVec;
   const int y = by * (128 / b.width) + row;
   const int t = *b.tdev + toff;
-  if (kH) h_split_vec(b.s, t, z, y, x0, lane, b.width, true);
-  else e_split_vec(b.s, t, z, y, x0, lane, b.width, true);
+  if (kH) h_split_vec(s, t, z, y, x0, lane, b.width, true);
+  else e_split_vec(s, t, z, y, x0, lane, b.width, true);
 }
 
 template <class T>
