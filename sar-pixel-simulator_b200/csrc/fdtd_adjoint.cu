@@ -789,7 +789,7 @@ __global__ void __launch_bounds__(128) k_adj_k1(const __grid_constant__ State<T>
 // lambda_E = Ca lambda_E + (H step)^T lambda_H + the E phasor source of
 // step n - 1 (t_prev < 0: none).
 template <class T>
-__global__ void __launch_bounds__(128) k_adj_k2(const __grid_constant__ State<T> s, Adj<T> a,
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 4 : 1) k_adj_k2(const __grid_constant__ State<T> s, Adj<T> a,
                                                 int t_prev) {
   int z, y, x0;
   if (!vec_cell(s, z, y, x0)) return;
