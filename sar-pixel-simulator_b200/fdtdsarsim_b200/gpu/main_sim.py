@@ -92,6 +92,24 @@ class MainSimGpu:
         if self._incident_loaded is not None:
             return
         fname = inc_filename(self.params)
+        from ..incident import take_resident
+        held = take_resident(fname)
+        if held is not None:
+            # the beam IncidentBeam.setup just made in this process: copy its
+            # planes device to device instead of reading the file back
+            run, phasors = held
+            try:
+                g = run.native.geom
+                if (g.nx, g.ny, g.dtype) == (self.geom.nx, self.geom.ny, self.geom.dtype) and \
+                        g.nt >= self.geom.nt_inc:
+                    self.native.set_incident_from(run.native)   # checks the device too
+                    self._inc_phasors = {k: np.asarray(v) for k, v in phasors.items()}
+                    self._incident_loaded = fname
+                    return
+            except _native.FdtdError:
+                pass   # another device: read the file
+            finally:
+                run.close()
         with resultsio.File(fname, 'r') as f:
             comps = [np.asarray(f[c][:], dtype=self.dtype) for c in ('ex', 'ey', 'hx', 'hy')]
             self._inc_phasors = {f'{c}_inc_phasor': np.asarray(f['phasors'][f'{c}_inc_phasor'][:])

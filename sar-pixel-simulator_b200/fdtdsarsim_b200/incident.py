@@ -111,6 +111,32 @@ class IncidentSimGpu:
         self.native.close()
 
 
+# Incident runs just made by IncidentBeam.setup, kept on the device for the
+# next main simulation of the same geometry: {absolute incident file name:
+# (IncidentSimGpu, phasors)}. MainSimGpu takes an entry (device-to-device
+# copy of the planes, then the run is closed) instead of reading the file
+# back; the file is still written, for other processes and later runs.
+_RESIDENT = {}
+
+
+def keep_resident(fname: str, sim: 'IncidentSimGpu', phasors):
+    """Hold an incident run for the next main simulation that needs its
+    file (replacing any run held for that file)."""
+    import os
+    key = os.path.abspath(fname)
+    old = _RESIDENT.pop(key, None)
+    if old is not None:
+        old[0].close()
+    _RESIDENT[key] = (sim, phasors)
+
+
+def take_resident(fname: str):
+    """(IncidentSimGpu, phasors) held for an incident file, or None; the
+    caller closes the run."""
+    import os
+    return _RESIDENT.pop(os.path.abspath(fname), None)
+
+
 def generate_incident_beam(params: ParameterCollection, write: bool = True, device=None):
     """Make the incident beam of a geometry on the device and, with
     ``write``, store it as the reference's incident file. Returns

@@ -48,9 +48,11 @@ class IncidentBeam:
             self.load_existing()
             return
         logger.info('Generating new incident beam on the device')
-        from .incident import generate_incident_beam
-        _, _, sim = generate_incident_beam(self.params)
-        sim.close()
+        from .incident import generate_incident_beam, keep_resident
+        _, phasors, sim = generate_incident_beam(self.params)
+        # the planes stay on the device for the main simulation of this
+        # geometry (MainSimGpu takes them without reading the file back)
+        keep_resident(inc_filename(self.params), sim, phasors)
         self.load_existing()
 
     def create_pulse(self):

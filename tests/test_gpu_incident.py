@@ -187,3 +187,28 @@ def test_run_experiment_cfg1_with_device_beam(tmp_path):
         pw = np.asarray(f['farfield']['out_pwr_far_h'])
         r = ref['ff_out_pwr_far_h']
         assert np.max(np.abs(pw - r)) <= 1e-4 * np.max(np.abs(r))
+
+
+def test_run_experiment_hands_the_beam_over_on_the_device(tmp_path):
+    """The beam IncidentBeam.setup makes is copied device to device into
+    the main simulation (nothing is left held afterwards); a later
+    experiment that reads the written incident file gets bit-identical
+    phasors."""
+    import fdtdsarsim_b200 as fdtd
+    from fdtdsarsim_b200 import incident, resultsio
+    from fdtdsarsim_b200.parameters import results_filename
+    ref = np.load(os.path.join(GOLDEN, 'pipeline_cfg1.npz'))
+    user = json.loads(str(ref['params_json']))
+    user.update({'processing_type': 'gpu', 'project_dir': str(tmp_path), 'gpu_num': 0})
+    path = tmp_path / 'params.json'
+    path.write_text(json.dumps(user))
+    pc = fdtd.load_from_json(str(path))
+    fdtd.run_experiment(pc, fdtd.materials.flat_surface(pc, 6.0, 0.01, name='first'))
+    assert not incident._RESIDENT
+    fdtd.run_experiment(pc, fdtd.materials.flat_surface(pc, 6.0, 0.01, name='second'))
+    out = []
+    for name in ('first', 'second'):
+        with resultsio.File(results_filename(pc, name), 'r') as f:
+            out.append({k: np.asarray(f['phasors'][k]) for k in _native.PHASOR_NAMES})
+    for k in _native.PHASOR_NAMES:
+        assert bits_equal(out[0][k], out[1][k]), k
