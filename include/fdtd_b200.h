@@ -150,7 +150,8 @@ int fdtd_run(fdtd_sim *sim, int nsteps);
 
 /* Runs `nsteps` time steps while streaming the incident planes of those
  * steps from host memory (four (nt_inc, ny, nx) arrays) on a copy stream,
- * 16 steps' planes per transfer, overlapped with the time stepping: each
+ * 16 steps' planes per transfer (2 in the first, so that the stepping
+ * starts early), overlapped with the time stepping: each
  * group of steps waits only for its own planes. Page-locked arrays are
  * copied directly; pageable ones through two pinned staging buffers.
  * Synchronous. This is the reference's per-step incident transfer
@@ -188,6 +189,10 @@ int fdtd_clear_kernel_time(fdtd_sim *sim);
  * (ny-2npml, nx-2npml); l/r (nz-2npml, ny-2npml); f/b (nz-2npml, nx-2npml).
  * Replaces the phasor memcpy_dtoh block (gpu/main_sim.py:357-385). */
 int fdtd_get_phasor(fdtd_sim *sim, int plane, void *out);
+/* All 24 planes in one call: packed one after the other in that order into
+ * `out` (complex of the element type); one synchronisation, and direct
+ * transfers when `out` is page-locked. */
+int fdtd_get_phasors(fdtd_sim *sim, void *out);
 
 /* Copies a field component (0..5 = ex, ey, ez, hx, hy, hz) of the current
  * state to / from host memory, shape (nz, ny, nx). The reference exposes

@@ -25,6 +25,10 @@ void launch_batch_step(const BatchModel<T>* bm, const int* start, int n, int blo
 template <class T>
 void launch_batch_advance(const BatchModel<T>* bm, int n, int steps, cudaStream_t st);
 
+// Packed rows of nx elements into rows of `pitch` elements.
+template <class T>
+void launch_repitch(T* dst, const T* src, int nx, long long rows, int pitch, cudaStream_t st);
+
 template <class T>
 void launch_eps_sigma(int nx, int ny, int nz, int nz_mat, int pitch, const T* eps,
                       const T* sig, T eps0, T dt, T dx, T* ca, T* cb, cudaStream_t st);

@@ -12,6 +12,8 @@
 // shell of the fused step (fdtd_fused.cu).
 #include <cstring>
 
+#include <algorithm>
+
 #include "fdtd_launch.h"
 #include "fdtd_vec.cuh"
 
@@ -404,6 +406,24 @@ void launch_check_finite(const FieldPtrs<T>& f, long long vol, int step, int* fl
 
 template void launch_check_finite<float>(const FieldPtrs<float>&, long long, int, int*, cudaStream_t);
 template void launch_check_finite<double>(const FieldPtrs<double>&, long long, int, int*, cudaStream_t);
+
+// Packed rows (nx elements each) into pitched rows.
+template <class T>
+__global__ void __launch_bounds__(256) k_repitch(T* __restrict__ dst, const T* __restrict__ src, int nx,
+                                                 long long rows, int pitch) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= nx) return;
+  for (long long r = blockIdx.y; r < rows; r += gridDim.y) dst[r * pitch + x] = src[r * nx + x];
+}
+
+template <class T>
+void launch_repitch(T* dst, const T* src, int nx, long long rows, int pitch, cudaStream_t st) {
+  const dim3 grd((nx + 255) / 256, (unsigned)std::min<long long>(rows, 65535), 1);
+  k_repitch<T><<<grd, 256, 0, st>>>(dst, src, nx, rows, pitch);
+}
+
+template void launch_repitch<float>(float*, const float*, int, long long, int, cudaStream_t);
+template void launch_repitch<double>(double*, const double*, int, long long, int, cudaStream_t);
 
 template <class T>
 void launch_eps_sigma(int nx, int ny, int nz, int nz_mat, int pitch, const T* eps,

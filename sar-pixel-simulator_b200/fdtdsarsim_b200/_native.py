@@ -101,6 +101,7 @@ SIGNATURES = {
     'fdtd_get_kernel_time': [_P, _I, ctypes.POINTER(_D), ctypes.POINTER(_I)],
     'fdtd_clear_kernel_time': [_P],
     'fdtd_get_phasor': [_P, _I, _P],
+    'fdtd_get_phasors': [_P, _P],
     'fdtd_get_field': [_P, _I, _P],
     'fdtd_set_field': [_P, _I, _P],
     'fdtd_near2far': [_P, _P, _P, _P, _I, _I, _I, _I, _D, _D, _P, _I, _P, _I, _D, _I, _P],
@@ -287,8 +288,28 @@ class NativeSim:
         check(lib.fdtd_get_phasor(self.h, int(k), ptr(out)))
         return out
 
-    def get_phasors(self):
-        return {name: self.get_phasor(k) for k, name in enumerate(PHASOR_NAMES)}
+    def phasors_size(self):
+        """Complex elements of the 24 phasor planes together."""
+        return sum(int(np.prod(self.phasor_shape(k))) for k in range(24))
+
+    def get_phasors(self, out=None):
+        """All 24 phasor planes by name, read in one call
+        (fdtd_get_phasors). ``out``: an optional flat buffer of
+        phasors_size() complex elements (page-locked memory makes the
+        transfer direct); the planes are views of it."""
+        n = self.phasors_size()
+        if out is None:
+            out = np.empty(n, self.cdtype)
+        if out.dtype != self.cdtype or out.size != n or not out.flags['C_CONTIGUOUS']:
+            raise ValueError(f'phasor buffer must be {n} contiguous {np.dtype(self.cdtype).name}')
+        check(lib.fdtd_get_phasors(self.h, ptr(out)))
+        planes, off = {}, 0
+        for k, name in enumerate(PHASOR_NAMES):
+            shape = self.phasor_shape(k)
+            m = int(np.prod(shape))
+            planes[name] = out[off:off + m].reshape(shape)
+            off += m
+        return planes
 
     def get_field(self, comp):
         g = self.geom

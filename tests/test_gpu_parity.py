@@ -359,3 +359,24 @@ def test_graph_chunks_equal_direct_launches(kernel):
     finally:
         a.close()
         b.close()
+
+
+def test_all_phasors_in_one_call():
+    """fdtd_get_phasors (one call, into a pageable or a page-locked buffer)
+    returns the 24 planes of fdtd_get_phasor bit for bit."""
+    import torch
+    pc = make_params(41, 37, 29, 16, 12, 10)
+    _, _, ca, cb, inc = random_problem(pc, 35)
+    sim = native_for(pc, FUSED, (32, 4))
+    try:
+        sim.set_materials(ca, cb)
+        sim.set_incident(inc['ex'], inc['ey'], inc['hx'], inc['hy'])
+        sim.run(12)
+        sim.synchronize()
+        pinned = torch.empty(2 * sim.phasors_size(), dtype=torch.float32).pin_memory().numpy()
+        for out in (None, pinned.view(np.complex64)):
+            got = sim.get_phasors(out)
+            for k, name in enumerate(_native.PHASOR_NAMES):
+                assert bits_equal(got[name], sim.get_phasor(k)), name
+    finally:
+        sim.close()
