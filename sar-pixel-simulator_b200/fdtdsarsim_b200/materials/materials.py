@@ -55,3 +55,33 @@ def flat_surface(params: ParameterCollection, epsilon_r: float, conductivity: fl
     meta = {'epsilon_r': epsilon_r, 'conductivity': conductivity}
     yield MaterialModel(epsilon_r * np.ones(shape, dtype=dtype),
                         conductivity * np.ones(shape, dtype=dtype), g.cell_size, name, meta)
+
+
+def rough_dielectric(params: ParameterCollection, epsilon_r: float, conductivity: float,
+                     height_rms: float, mean_depth: float, corr_len: float, count: int,
+                     seed=None):
+    """``count`` models of one dielectric under a Gaussian-correlated rough
+    surface of mean depth ``mean_depth`` [m] (materials/materials.py:
+    112-164): a cell is dielectric when its z index is at most the surface
+    height in cells. The reference draws unseeded surfaces; ``seed`` (this
+    package's addition) makes surface i use seed + i."""
+    from .roughsurface import gaussian_correlated_surface
+    g = params.geom_params
+    nx, ny, nz, dx = g.size_x, g.size_y, g.size_z_material, g.cell_size
+    dtype = params.processing_params.datatype
+    mean_cells = mean_depth / dx
+    if mean_depth > nz * dx:
+        raise ValueError('Requested mean soil depth is greater than the max height of the '
+                         'simulator space.')
+    meta = {'epsilon_r': epsilon_r, 'conductivity': conductivity, 'height_rms': height_rms,
+            'mean_depth': mean_depth, 'mean_depth_cells': mean_cells, 'corr_len': corr_len}
+    z = np.arange(nz)[:, None, None]
+    for i in range(count):
+        h = gaussian_correlated_surface(nx, ny, dx, corr_len, corr_len, height_rms,
+                                        seed=None if seed is None else seed + i)
+        h /= dx
+        h += mean_cells
+        below = z <= h[np.newaxis]
+        yield MaterialModel(np.where(below, epsilon_r, 1.0).astype(dtype),
+                            np.where(below, conductivity, 0.0).astype(dtype), dx,
+                            f'rough_surf_{i}', dict(meta))

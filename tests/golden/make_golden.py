@@ -16,6 +16,9 @@ Outputs (all small, committed):
   near2far.npz         FarFieldTransform (near2far.py:28-112)
   pipeline_cfg1.npz    run_experiment end to end (experiment.py:41-97),
                        incident beam generation included
+  material_gen.npz     the material generators (materials/roughsurface.py,
+                       dielectricmodels.py, bubbles.py, soilmodels.py,
+                       materials.py:112-164) on small seeded cases
   incident_*.npz       IncidentBeam.create_pulse / create_inc_excitation
                        (incidentbeam.py:174-298) and IncidentSimCpu
                        (cpu/incident_sim.py:22-171) on small geometries
@@ -351,8 +354,79 @@ def gen_incident(tag, dtype, pol, theta, phi, sx, sy, duration, full):
     np.savez_compressed(os.path.join(HERE, f'incident_{tag}.npz'), **out)
 
 
+def gen_material_generators():
+    """Seeded runs of the reference's material generators. rough_dielectric
+    draws unseeded surfaces; it is run with gaussian_correlated_surface
+    wrapped to seeds 300 + i (the port takes those seeds as an argument)."""
+    import fdtdsarsim.materials.materials as rm
+    from fdtdsarsim.materials import bubbles, dielectricmodels as dm, roughsurface as rs, soilmodels as sm
+    out = {}
+    dx = 0.003
+    out['gcs'] = rs.gaussian_correlated_surface(41, 37, dx, 0.010, 0.015, 0.002, seed=11)
+    out['gcs_rabus'] = rs.gaussian_correlated_surface(41, 37, dx, 0.010, 0.015, 0.002, seed=11,
+                                                      rabus_compat=True)
+    out['gcs_fast'] = rs.gaussian_correlated_surface_fast(41, 37, dx, 0.010, 0.015, 0.002,
+                                                          np.random.default_rng(12))
+    out['two_layer'] = rs.two_layer_gaussian_correlated_surface(41, 37, dx, 0.010, 0.012, 0.002,
+                                                                0.6, seed=13)
+    out['two_layer_full'] = rs.two_layer_gaussian_correlated_surface(41, 37, dx, 0.010, 0.012,
+                                                                     0.002, 1.0, seed=14)
+    cases = np.array([(mv, sand, clay, f) for mv in (0.05, 0.2, 0.41)
+                      for sand, clay in ((0.3, 0.2), (0.6, 0.1))
+                      for f in (1.4e9, 5.4e9, 9.7e9, 18e9)])
+    out['hall_cases'] = cases
+    model = dm.HallikainenSoilModel()
+    out['hall_class'] = np.array([model.get_epsilon(*c) for c in cases])
+    out['hall_func'] = np.array([dm.hallikainen_soil_model(*c) for c in cases])
+    pc = make_params('float32')
+    raw_geom(pc, 23, 21, 30, 20, 10, 5)
+    g = pc.geom_params
+    g.size_z_material = 12
+    g.cell_size = dx
+    orig = rm.gaussian_correlated_surface
+    seeds = iter(range(300, 400))
+    rm.gaussian_correlated_surface = lambda *a, **k: orig(*a, seed=next(seeds), **k)
+    try:
+        for i, m in enumerate(rm.rough_dielectric(pc, 7.0, 0.03, 0.004, 0.02, 0.01, 2)):
+            out[f'rough_{i}_eps'] = m.relative_permittivity
+            out[f'rough_{i}_sig'] = m.conductivity
+    finally:
+        rm.gaussian_correlated_surface = orig
+    for tag, gen in (
+            ('one', sm.one_layer_gaussian(pc, [0.1, 0.3], 0.4, 0.2, 0.004, 0.01, 0.02, 2, 21)),
+            ('one_groove', sm.one_layer_gaussian(pc, [0.2], 0.4, 0.2, 0.004, 0.01, 0.02, 1, 22,
+                                                 grooved=True, rabus_compat=True)),
+            ('two', sm.two_layer_gaussian(pc, 0.15, [0.3, 0.35], 0.5, 0.1, 0.003, 0.01, 0.7,
+                                          0.025, 0.01, 1, 23)),
+            ('grad', sm.gradient_gaussian(pc, 0.1, [0.35], 0.5, 0.1, 0.003, 0.01, 0.7,
+                                          0.025, 0.01, 1, 24)),
+            ('grad_groove', sm.gradient_gaussian(pc, 0.1, [0.3], 0.5, 0.1, 0.003, 0.01, 0.7,
+                                                 0.025, 0.01, 1, 25, grooved=True))):
+        for i, m in enumerate(gen):
+            out[f'{tag}_{i}_eps'] = m.relative_permittivity
+            out[f'{tag}_{i}_sig'] = m.conductivity
+            out[f'{tag}_{i}_name'] = m.name
+    # bubbles in a one-layer model with a flat surface at 9 cells
+    surf = np.full((21, 23), 9.0)
+    for tag, fn, args in (('bub', bubbles.add_bubbles, (0.15, 0.0065, 3.2, 0.0, 31)),
+                          ('bub_rand', bubbles.add_bubbles_randsize, (0.15, 0.004, 0.008, 3.2, 0.0, 32))):
+        m = next(sm.one_layer_gaussian(pc, [0.2], 0.4, 0.2, 0.0, 0.01, 0.03, 1, 26))
+        eps = np.where(np.arange(12)[:, None, None] <= 9, m.relative_permittivity[0, 0, 0], 1.0)
+        sig = np.where(np.arange(12)[:, None, None] <= 9, m.conductivity[0, 0, 0], 0.0)
+        m.relative_permittivity = np.broadcast_to(eps, (12, 21, 23)).astype(np.float32).copy()
+        m.conductivity = np.broadcast_to(sig, (12, 21, 23)).astype(np.float32).copy()
+        m.metadata = {}
+        out[f'{tag}_in_eps'] = m.relative_permittivity.copy()
+        out[f'{tag}_in_sig'] = m.conductivity.copy()
+        r = fn(m, surf, *args)
+        out[f'{tag}_eps'] = r.relative_permittivity
+        out[f'{tag}_sig'] = r.conductivity
+    out['bub_surf'] = surf
+    np.savez_compressed(os.path.join(HERE, 'material_gen.npz'), **out)
+
+
 if __name__ == '__main__':
-    which = sys.argv[1:] or ['geom', 'abs', 'mat', 'main', 'n2f', 'pipe', 'inc']
+    which = sys.argv[1:] or ['geom', 'abs', 'mat', 'main', 'n2f', 'pipe', 'inc', 'matgen']
     if 'geom' in which:
         gen_geom()
     if 'abs' in which:
@@ -371,3 +445,5 @@ if __name__ == '__main__':
     if 'inc' in which:
         for case in INCIDENT_CASES:
             gen_incident(*case)
+    if 'matgen' in which:
+        gen_material_generators()
