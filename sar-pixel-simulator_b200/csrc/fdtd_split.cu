@@ -106,10 +106,10 @@ __device__ __forceinline__ const ShellBox& find_box(const ShellBoxes& bl, int bi
   return bl.b[k];
 }
 
-// Resident blocks per SM the split passes ask for (float: register cap 72;
+// Resident blocks per SM the split passes ask for (float: register cap 64;
 // the passes are latency-bound, so more warps in flight beat a few spills)
 template <class T>
-constexpr int split_min_blocks() { return sizeof(T) == 4 ? 7 : 1; }
+constexpr int split_min_blocks() { return sizeof(T) == 4 ? 8 : 1; }
 
 template <class T, bool kH>
 __global__ void __launch_bounds__(128, split_min_blocks<T>()) k_shell(State<T> s, const int* __restrict__ tp, int toff,
