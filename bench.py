@@ -210,16 +210,46 @@ def cpu_baseline(pc, ca, cb, inc, steps):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
-def run_ours(a):
+def init_replicas(backend='nccl', timeout_s=120):
+    """(rank, world, local) of this process from the launcher's environment
+    (RANK, WORLD_SIZE, LOCAL_RANK, MASTER_ADDR/PORT); with more than one
+    rank, a process group on ``backend`` with a short timeout, so that ranks
+    waiting for a lost peer end with an error. Replicas only: the group
+    carries barriers and the max-over-ranks timing, no data."""
+    import datetime
     import torch
     import torch.distributed as dist
     world = int(os.environ.get('WORLD_SIZE', '1'))
     rank = int(os.environ.get('RANK', '0'))
     local = int(os.environ.get('LOCAL_RANK', '0'))
     if world > 1:
-        import datetime
-        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device('cuda', local))
+        kw = {'device_id': torch.device('cuda', local)} if backend == 'nccl' else {}
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s), **kw)
+    return rank, world, local
+
+
+def max_over_ranks(x, world, device):
+    """The largest of every rank's value (the job's time is its slowest
+    replica's)."""
+    if world == 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(units, steps, ms, world):
+    """Whole-job Mcell-updates/s: every rank processed ``units`` cells for
+    ``steps`` steps in at most ``ms`` milliseconds."""
+    return world * units * steps / (ms / 1e3) / 1e6
+
+
+def run_ours(a):
+    import torch
+    import torch.distributed as dist
+    rank, world, local = init_replicas('nccl')
     torch.cuda.set_device(local)
     from fdtdsarsim_b200 import _native
     from fdtdsarsim_b200.absorbers import packed_profiles
@@ -273,11 +303,8 @@ def run_ours(a):
     barrier()
     clk = clocks.stop()
     ms = t_start.elapsed_time(t_end)
-    ms_t = torch.tensor([ms], dtype=torch.float64, device='cuda')
-    if world > 1:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
-    value = world * cells * a.steps / (ms_max / 1e3) / 1e6
+    ms_max = max_over_ranks(ms, world, 'cuda')
+    value = job_rate(cells, a.steps, ms_max, world)
     # split: H pass, E pass, phasors; fused: interior pass (and z-slab pass), shell H pass,
     # shell E pass, phasors; plus one step-counter advance per run call
     launches_per_step = 3 if choice['kernel'] == _native.FDTD_KERNEL_SPLIT else 4 + int(bool(choice.get('slab', 0)))
@@ -329,11 +356,7 @@ def run_ours(a):
         sim2.run_streamed(a.steps, pin['ex'], pin['ey'], pin['hx'], pin['hy'])
         phs = sim2.get_phasors(ph_buf)
         t1 = time.perf_counter()
-        el = t1 - t0
-        el_t = torch.tensor([el], dtype=torch.float64, device='cuda')
-        if world > 1:
-            dist.all_reduce(el_t, op=dist.ReduceOp.MAX)
-        el = float(el_t.item())
+        el = max_over_ranks(t1 - t0, world, 'cuda')
         esz = np.dtype(a.dtype).itemsize
         h2d = 2 * cells * esz + 4 * g.size_t_inc * g.size_x * g.size_y * esz
         d2h = sum(p.nbytes for p in phs.values())
