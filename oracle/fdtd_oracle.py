@@ -3,7 +3,7 @@
 This module restates, in vectorised numpy, the algorithm of the reference
 package ``fdtdsarsim`` (wyatt-sfu/sar-pixel-simulator) for one Yee time step
 with CPML absorbers, one-plane incident injection and running phasor DFTs.
-It is the checker for the CUDA path: only ``tests/``, ``__graft_entry__.smoke``
+The CUDA path's results are compared against it: only ``tests/``, ``__graft_entry__.smoke``
 and ``bench.py`` (its CPU-baseline leg) may import it, and never as the thing
 that is measured or shipped.
 

@@ -2,8 +2,8 @@
 
 Restates in numpy how the reference package ``fdtdsarsim``
 (wyatt-sfu/sar-pixel-simulator) makes the incident beam that a main
-simulation injects. It is the checker for the CUDA path (only ``tests/`` may
-import it) and is never the thing that is measured or shipped.
+simulation injects. The CUDA path's results are compared against it (only
+``tests/`` may import it); it is never the thing that is measured or shipped.
 
 * ``create_pulse``: the Gaussian-tapered complex carrier and its FFT
   (``incidentbeam.py:174-204``);
