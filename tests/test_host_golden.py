@@ -120,3 +120,34 @@ def test_resultsio_roundtrip(tmp_path):
         f.create_group('farfield').create_dataset('e_phi', data=np.ones(3))
     with resultsio.File(fname, 'r') as f:
         assert f['farfield']['e_phi'].shape == (3,)
+
+
+def test_incident_file_roundtrip_and_checks(tmp_path):
+    """An incident file written in the reference's layout passes
+    IncidentBeam's shape, dtype and metadata checks (incidentbeam.py:
+    74-165), and each kind of mismatch is rejected with the reference's
+    ValueError."""
+    import copy
+    from fdtdsarsim_b200 import resultsio
+    from fdtdsarsim_b200.incidentbeam import IncidentBeam, write_incident_file
+    from fdtdsarsim_b200.parameters import inc_filename
+    from helpers import make_params
+    pc = make_params(25, 23, 27, 14, 10, 6)
+    pc.processing_params.project_dir = str(tmp_path)
+    g = pc.geom_params
+    planes = [np.full((g.size_t_inc, g.size_y, g.size_x), k, np.float32) for k in range(4)]
+    ph = {f'{c}_inc_phasor': np.zeros((g.size_y - 20, g.size_x - 20), np.complex64)
+          for c in ('ex', 'ey', 'hx', 'hy')}
+    write_incident_file(pc, *planes, ph)
+    beam = IncidentBeam(pc)
+    assert beam.inc_beam_exists()
+    beam.load_existing()
+    other = copy.deepcopy(pc)
+    other.inc_beam_params.duration = pc.inc_beam_params.duration + 1.0
+    with resultsio.File(inc_filename(pc), 'r') as f:
+        with pytest.raises(ValueError, match='duration'):
+            IncidentBeam(other).check_metadata(f.attrs)
+    with pytest.raises(ValueError, match='wrong shape'):
+        beam.check_array_sizes(np.zeros((1, 2, 3), np.float32))
+    with pytest.raises(ValueError, match='incorrect datatype'):
+        beam.check_array_sizes(np.zeros((g.size_t_inc, g.size_y, g.size_x), np.float64))
