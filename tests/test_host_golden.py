@@ -151,3 +151,51 @@ def test_incident_file_roundtrip_and_checks(tmp_path):
         beam.check_array_sizes(np.zeros((1, 2, 3), np.float32))
     with pytest.raises(ValueError, match='incorrect datatype'):
         beam.check_array_sizes(np.zeros((g.size_t_inc, g.size_y, g.size_x), np.float64))
+
+
+def test_tuning_cache_choose_and_apply(tmp_path, monkeypatch):
+    """tuning.choose takes an explicit choice, else a cached measurement,
+    else the default; tuning.apply sets the matching library options."""
+    import json
+    from fdtdsarsim_b200 import _native, tuning
+    from fdtdsarsim_b200.gpu.main_sim import native_geometry
+    from helpers import make_params
+    monkeypatch.setenv('FDTDSARSIM_B200_TUNING', str(tmp_path / 'tune.json'))
+    geom = native_geometry(make_params(41, 37, 29, 16, 12, 10))
+    assert tuning.choose(geom, device=0)['kernel'] == _native.FDTD_KERNEL_FUSED
+    key = tuning._key(geom, tuning._device_name(0))
+    (tmp_path / 'tune.json').write_text(json.dumps({key: {'kernel': 1, 'tile_y': 7, 'zchunk': 26,
+                                                          'slab': 1}}))
+    c = tuning.choose(geom, device=0)
+    assert (c['tile_y'], c['zchunk'], c['slab']) == (7, 26, 1)
+    assert tuning.choose(geom, kernel=_native.FDTD_KERNEL_SPLIT)['kernel'] == _native.FDTD_KERNEL_SPLIT
+
+    class Fake:
+        def __init__(self):
+            self.opts = {}
+
+        def set_option(self, k, v):
+            self.opts[k] = v
+    f = Fake()
+    tuning.apply(f, c)
+    assert f.opts == {_native.OPT_KERNEL: 1, _native.OPT_TILE_X: 32, _native.OPT_TILE_Y: 7,
+                      _native.OPT_ZCHUNK: 26, _native.OPT_FUSED_SLAB: 1}
+
+
+def test_incident_pulse_matches_reference():
+    """The package's create_pulse (host) against the reference's pulse and
+    spectrum (incidentbeam.py:174-199, fixture incident_hh_f32.npz)."""
+    from fdtdsarsim_b200.incident import create_pulse, taper_radius
+    from helpers import make_params
+    g = np.load(os.path.join(GOLDEN, 'incident_hh_f32.npz'))
+    pc = make_params(int(g['nx']), int(g['ny']), 60, 30, int(g['size_t_inc']), int(g['size_t_inc']))
+    pc.geom_params.timestep = float(g['dt'])
+    pc.geom_params.size_t_pulse = int(g['size_t_pulse'])
+    pc.inc_beam_params.duration = float(g['duration'])
+    pc.inc_beam_params.frequency = float(g['freq'])
+    pc.inc_beam_params.illumination_width = float(g['illumination_width'])
+    tv, pulse, pfft, pfreq = create_pulse(pc)
+    assert np.array_equal(tv, g['time_vals']) and np.array_equal(pfreq, g['pulse_freqs'])
+    assert np.max(np.abs(pulse - g['pulse'])) <= 1e-15
+    assert np.max(np.abs(pfft - g['pulse_fft'])) <= 1e-12 * np.max(np.abs(g['pulse_fft']))
+    assert taper_radius(pc) > 0
