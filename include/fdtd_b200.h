@@ -58,7 +58,9 @@ extern "C" {
                                     4 x cells each; 32 (128 cells) */
 #define FDTD_OPT_TILE_Y       4  /* fused kernel tile height in rows:
                                     4, 7, 8 (float, double), 15, 16 (float) */
-#define FDTD_OPT_GRAPH_CHUNK  5  /* steps per captured CUDA graph (0 = no graph) */
+#define FDTD_OPT_GRAPH_CHUNK  5  /* fdtd_run: steps per captured CUDA graph (0 = no
+                                    graph); used while timing and the non-finite
+                                    check are off */
 #define FDTD_OPT_CHECK_EVERY  6  /* non-finite check period in steps (0 = off) */
 #define FDTD_OPT_TIMING       7  /* 1: record CUDA events around every kernel */
 #define FDTD_OPT_ZCHUNK       8  /* fused kernel z planes per block (0 = automatic) */
@@ -120,8 +122,10 @@ int fdtd_get_option(fdtd_sim *sim, int option, int *value);
  * the same profiles tiled into 24 full 3-D arrays (absorbers.py:121-185). */
 int fdtd_set_absorbers(fdtd_sim *sim, const void *profiles);
 
-/* Uploads the update coefficient arrays Ca, Cb (nz, ny, nx) from host memory.
- * Replaces the Ca/Cb transfer at the top of MainSimGpu._sim_loop
+/* Uploads the update coefficient arrays Ca, Cb (nz, ny, nx) from host memory:
+ * one contiguous transfer each into a packed device buffer (allocated on the
+ * first call and kept: one more volume of device memory), re-pitched on the
+ * device. Replaces the Ca/Cb transfer at the top of MainSimGpu._sim_loop
  * (gpu/main_sim.py:200-202). */
 int fdtd_set_materials(fdtd_sim *sim, const void *ca, const void *cb);
 
