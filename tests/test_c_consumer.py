@@ -1,0 +1,51 @@
+"""The C-ABI from plain C: a C99 program including include/fdtd_b200.h,
+linked against libfdtd_b200.so, calls the entry points that need no device
+(version, error text, argument validation that precedes any device use)."""
+import os
+import shutil
+import subprocess
+
+import pytest
+
+from fdtdsarsim_b200 import _native
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+PROGRAM = r'''
+#include <stdio.h>
+#include <string.h>
+#include "fdtd_b200.h"
+
+int main(void) {
+    char msg[256];
+    if (fdtd_version() < 100) return 10;
+    fdtd_sim *sim = NULL;
+    fdtd_geometry g;
+    memset(&g, 0, sizeof(g));
+    g.nx = g.ny = g.nz = 5; g.npml = 10; g.tfsf_z = 2; g.nt = 10; g.nt_inc = 5;
+    g.dtype = FDTD_F32; g.cell_size = 1e-3; g.timestep = 1e-12; g.frequency = 5.4e9;
+    if (fdtd_create(&g, 0, &sim) != FDTD_ERR_INVALID || sim != NULL) return 11;
+    fdtd_last_error(msg, (int)sizeof(msg));
+    if (!strstr(msg, "too small")) return 12;
+    if (fdtd_run(NULL, 1) != FDTD_ERR_INVALID) return 13;
+    if (fdtd_batch_run(NULL, 1) == FDTD_OK) return 14;
+    int out[7 * 64], n = 0;
+    if (fdtd_fused_plan_boxes(761, 761, 203, 10, 156, 4, 0, 0, out, 64, &n) != FDTD_OK || n < 2) return 15;
+    printf("ok %d boxes\n", n);
+    return 0;
+}
+'''
+
+
+@pytest.mark.skipif(shutil.which('gcc') is None, reason='no C compiler')
+def test_c_program_links_and_calls(tmp_path):
+    src = tmp_path / 'consumer.c'
+    src.write_text(PROGRAM)
+    exe = tmp_path / 'consumer'
+    libdir = os.path.dirname(_native.LIB_PATH)
+    cmd = ['gcc', '-std=c99', '-Wall', '-Werror', '-I', os.path.join(ROOT, 'include'), str(src),
+           '-o', str(exe), '-L', libdir, '-l:libfdtd_b200.so', f'-Wl,-rpath,{libdir}']
+    subprocess.run(cmd, check=True, capture_output=True, text=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, (r.returncode, r.stdout, r.stderr)
+    assert r.stdout.startswith('ok')
