@@ -42,9 +42,10 @@ typedef struct oracle_state {
 } oracle_state;
 
 #define IDX(z, y, x) (((size_t)(z) * ny + (y)) * nx + (x))
+#define RS __restrict__
 
 #define DEFINE_STEP(T, NAME)                                                           \
-static void NAME(const oracle_state *s, int phase, int lo, int hi) {                                             \
+__attribute__((target_clones("avx2", "default"))) static void NAME(const oracle_state *s, int phase, int lo, int hi) {                                           \
   const int nx = s->nx, ny = s->ny, nz = s->nz, m = s->npml;                           \
   T *ex = (T *)s->ex, *ey = (T *)s->ey, *ez = (T *)s->ez;                              \
   T *hx = (T *)s->hx, *hy = (T *)s->hy, *hz = (T *)s->hz;                              \
@@ -54,68 +55,87 @@ static void NAME(const oracle_state *s, int phase, int lo, int hi) {            
   const T *bh[2] = {(const T *)s->prof[1], (const T *)s->prof[5]};                     \
   const T *cE[2] = {(const T *)s->prof[2], (const T *)s->prof[6]};                     \
   const T *cH[2] = {(const T *)s->prof[3], (const T *)s->prof[7]};                     \
-  /* ---- phase 0: H main update, planes [lo, hi) ---- */                              \
+  /* ---- phase 0: H main update, planes [lo, hi); per row, the x range of   \
+   * each component's update (no branch in the inner loops) ---- */                   \
   if (phase == 0)                                                                      \
-  for (int z = lo; z < hi; ++z)                                                        \
-    for (int y = 0; y < ny; ++y)                                                       \
-      for (int x = 0; x < nx; ++x) {                                                   \
-        const size_t i = IDX(z, y, x);                                                 \
-        if (z < nz - 1 && y < ny - 1 && x >= 1 && x < nx - 1) {                        \
-          T dez = ez[IDX(z, y + 1, x)] - ez[i];                                        \
-          T dey = ey[IDX(z + 1, y, x)] - ey[i];                                        \
-          hx[i] -= Db * (dez - dey);                                                   \
-        }                                                                              \
-        if (z < nz - 1 && y >= 1 && y < ny - 1 && x < nx - 1) {                        \
-          T dex = ex[IDX(z + 1, y, x)] - ex[i];                                        \
-          T dez = ez[IDX(z, y, x + 1)] - ez[i];                                        \
-          hy[i] -= Db * (dex - dez);                                                   \
-        }                                                                              \
-        if (z >= 1 && z < nz - 1 && y < ny - 1 && x < nx - 1) {                        \
-          T dex = ex[IDX(z, y + 1, x)] - ex[i];                                        \
-          T dey = ey[IDX(z, y, x + 1)] - ey[i];                                        \
-          hz[i] -= Db * (dey - dex);                                                   \
-        }                                                                              \
-      }                                                                                \
-  /* ---- phase 1: H CPML, z faces, then x, then y (per cell, that order) ---- */      \
-  if (phase == 1)                                                                      \
   for (int z = lo; z < hi && z < nz - 1; ++z)                                          \
+    for (int y = 0; y < ny - 1; ++y) {                                                 \
+      const size_t r = IDX(z, y, 0), rz = IDX(z + 1, y, 0), ry = IDX(z, y + 1, 0);     \
+      T *RS hxr = hx + r; T *RS hyr = hy + r; T *RS hzr = hz + r;                      \
+      const T *RS exr = ex + r; const T *RS eyr = ey + r; const T *RS ezr = ez + r;    \
+      const T *RS eyz = ey + rz; const T *RS exz = ex + rz;                            \
+      const T *RS ezy = ez + ry; const T *RS exy = ex + ry;                            \
+      for (int x = 1; x < nx - 1; ++x)                                                 \
+        hxr[x] -= Db * ((ezy[x] - ezr[x]) - (eyz[x] - eyr[x]));                        \
+      if (y >= 1)                                                                      \
+        for (int x = 0; x < nx - 1; ++x)                                               \
+          hyr[x] -= Db * ((exz[x] - exr[x]) - (ezr[x + 1] - ezr[x]));                  \
+      if (z >= 1)                                                                      \
+        for (int x = 0; x < nx - 1; ++x)                                               \
+          hzr[x] -= Db * ((eyr[x + 1] - eyr[x]) - (exy[x] - exr[x]));                  \
+    }                                                                                  \
+  /* ---- phase 1: H CPML over the face regions only: z faces, then x, then    \
+   * y (the reference's kernel order; a cell's corrections keep that order)     \
+   * ---- */                                                                            \
+  /* phase 7: the z faces, rows of the face planes [lo, hi) (planes           \
+   * z < m - 1 and nz - m <= z < nz - 1, (ny - 1) rows each), so that every     \
+   * thread gets an equal share; then phase 1: x and y faces per plane */       \
+  if (phase == 7)                                                                      \
+  for (int w = lo; w < hi; ++w) {                                                      \
+    const int j = w / (ny - 1), y = w % (ny - 1);                                      \
+    const int sd = j < m - 1 ? 0 : 1, q = sd ? j - (m - 1) : j;                        \
+    const int z = sd ? nz - m + q : q;                                                 \
+    const T b = bh[sd][q], c = cH[sd][q];                                              \
+    const size_t r = IDX(z, y, 0), rz = IDX(z + 1, y, 0);                              \
+    T *RS Pyz = (T *)s->psi[0][sd][3] + ((size_t)q * ny + y) * nx;                     \
+    T *RS Pxz = (T *)s->psi[0][sd][2] + ((size_t)q * ny + y) * nx;                     \
+    T *RS hxr = hx + r; T *RS hyr = hy + r;                                            \
+    const T *RS exr = ex + r; const T *RS eyr = ey + r;                                \
+    const T *RS exz = ex + rz; const T *RS eyz = ey + rz;                              \
+    for (int x = 0; x < nx - 1; ++x) {                                                 \
+      Pyz[x] = b * Pyz[x] + c * (exz[x] - exr[x]) / dx;                                \
+      Pxz[x] = b * Pxz[x] + c * (eyz[x] - eyr[x]) / dx;                                \
+      hyr[x] -= dtm0 * Pyz[x];                                                         \
+      hxr[x] += dtm0 * Pxz[x];                                                         \
+    }                                                                                  \
+  }                                                                                    \
+  if (phase == 1)                                                                      \
+  for (int z = lo; z < hi && z < nz - 1; ++z) {                                        \
     for (int y = 0; y < ny - 1; ++y)                                                   \
-      for (int x = 0; x < nx - 1; ++x) {                                               \
-        const size_t i = IDX(z, y, x);                                                 \
-        int sd = -1, q = 0;                                                            \
-        if (z < m - 1) { sd = 0; q = z; } else if (z >= nz - m) { sd = 1; q = z - (nz - m); } \
-        if (sd >= 0) {                                                                 \
-          T *Pyz = (T *)s->psi[0][sd][3], *Pxz = (T *)s->psi[0][sd][2];                \
-          const size_t k = ((size_t)q * ny + y) * nx + x;                              \
-          const T b = bh[sd][q], c = cH[sd][q];                                        \
-          Pyz[k] = b * Pyz[k] + c * (ex[IDX(z + 1, y, x)] - ex[i]) / dx;               \
-          Pxz[k] = b * Pxz[k] + c * (ey[IDX(z + 1, y, x)] - ey[i]) / dx;               \
-          hy[i] -= dtm0 * Pyz[k];                                                      \
-          hx[i] += dtm0 * Pxz[k];                                                      \
-        }                                                                              \
-        sd = -1;                                                                       \
-        if (x < m - 1) { sd = 0; q = x; } else if (x >= nx - m) { sd = 1; q = x - (nx - m); } \
-        if (sd >= 0) {                                                                 \
-          T *Pzx = (T *)s->psi[1][sd][3], *Pyx = (T *)s->psi[1][sd][2];                \
-          const size_t k = ((size_t)z * ny + y) * m + q;                               \
-          const T b = bh[sd][q], c = cH[sd][q];                                        \
-          Pzx[k] = b * Pzx[k] + c * (ey[IDX(z, y, x + 1)] - ey[i]) / dx;               \
-          Pyx[k] = b * Pyx[k] + c * (ez[IDX(z, y, x + 1)] - ez[i]) / dx;               \
+      for (int sx = 0; sx < 2; ++sx) {                                                 \
+        const int x0 = sx ? nx - m : 0, x1 = sx ? nx - 1 : m - 1;                      \
+        for (int x = x0; x < x1; ++x) {                                                \
+          const int qx = sx ? x - (nx - m) : x;                                        \
+          const size_t i = IDX(z, y, x);                                               \
+          T *Pzx = (T *)s->psi[1][sx][3], *Pyx = (T *)s->psi[1][sx][2];                \
+          const size_t k = ((size_t)z * ny + y) * m + qx;                              \
+          const T b = bh[sx][qx], c = cH[sx][qx];                                      \
+          Pzx[k] = b * Pzx[k] + c * (ey[i + 1] - ey[i]) / dx;                          \
+          Pyx[k] = b * Pyx[k] + c * (ez[i + 1] - ez[i]) / dx;                          \
           hz[i] -= dtm0 * Pzx[k];                                                      \
           hy[i] += dtm0 * Pyx[k];                                                      \
         }                                                                              \
-        sd = -1;                                                                       \
-        if (y < m - 1) { sd = 0; q = y; } else if (y >= ny - m) { sd = 1; q = y - (ny - m); } \
-        if (sd >= 0) {                                                                 \
-          T *Pxy = (T *)s->psi[2][sd][2], *Pzy = (T *)s->psi[2][sd][3];                \
-          const size_t k = ((size_t)z * m + q) * nx + x;                               \
-          const T b = bh[sd][q], c = cH[sd][q];                                        \
-          Pxy[k] = b * Pxy[k] + c * (ez[IDX(z, y + 1, x)] - ez[i]) / dx;               \
-          Pzy[k] = b * Pzy[k] + c * (ex[IDX(z, y + 1, x)] - ex[i]) / dx;               \
-          hx[i] -= dtm0 * Pxy[k];                                                      \
-          hz[i] += dtm0 * Pzy[k];                                                      \
+      }                                                                                \
+    for (int sy = 0; sy < 2; ++sy) {                                                   \
+      const int y0 = sy ? ny - m : 0, y1 = sy ? ny - 1 : m - 1;                        \
+      for (int y = y0; y < y1; ++y) {                                                  \
+        const int qy = sy ? y - (ny - m) : y;                                          \
+        const T b = bh[sy][qy], c = cH[sy][qy];                                        \
+        const size_t r = IDX(z, y, 0), ry = IDX(z, y + 1, 0);                          \
+        T *RS Pxy = (T *)s->psi[2][sy][2] + ((size_t)z * m + qy) * nx;                 \
+        T *RS Pzy = (T *)s->psi[2][sy][3] + ((size_t)z * m + qy) * nx;                 \
+        T *RS hxr = hx + r; T *RS hzr = hz + r;                                        \
+        const T *RS exr = ex + r; const T *RS ezr = ez + r;                            \
+        const T *RS exy = ex + ry; const T *RS ezy = ez + ry;                          \
+        for (int x = 0; x < nx - 1; ++x) {                                             \
+          Pxy[x] = b * Pxy[x] + c * (ezy[x] - ezr[x]) / dx;                            \
+          Pzy[x] = b * Pzy[x] + c * (exy[x] - exr[x]) / dx;                            \
+          hxr[x] -= dtm0 * Pxy[x];                                                     \
+          hzr[x] += dtm0 * Pzy[x];                                                     \
         }                                                                              \
       }                                                                                \
+    }                                                                                  \
+  }                                                                                    \
   const int inj = s->t < s->nt_inc;                                                    \
   /* ---- phase 2: E-field injection into H, rows [lo, hi) ---- */                     \
   if (phase == 2 && inj) {                                                             \
@@ -127,71 +147,91 @@ static void NAME(const oracle_state *s, int phase, int lo, int hi) {            
         hy[IDX(s->tfsf_z, y, x)] -= Db * iex[(size_t)y * nx + x];                      \
       }                                                                                \
   }                                                                                    \
-  /* ---- phase 3: E main update ---- */                                              \
+  /* ---- phase 3: E main update, per row as phase 0 ---- */                     \
   if (phase == 3)                                                                      \
-  for (int z = lo; z < hi; ++z)                                                        \
-    for (int y = 0; y < ny; ++y)                                                       \
-      for (int x = 0; x < nx; ++x) {                                                   \
-        const size_t i = IDX(z, y, x);                                                 \
-        if (z >= 1 && z < nz - 1 && y >= 1 && y < ny - 1 && x < nx - 1) {              \
-          T scaled = ex[i] * ca[i];                                                    \
-          T dhz = hz[i] - hz[IDX(z, y - 1, x)];                                        \
-          T dhy = hy[i] - hy[IDX(z - 1, y, x)];                                        \
-          ex[i] = scaled + (cb[i] * (dhz - dhy));                                      \
-        }                                                                              \
-        if (z >= 1 && z < nz - 1 && y < ny - 1 && x >= 1 && x < nx - 1) {              \
-          T scaled = ey[i] * ca[i];                                                    \
-          T dhx = hx[i] - hx[IDX(z - 1, y, x)];                                        \
-          T dhz = hz[i] - hz[IDX(z, y, x - 1)];                                        \
-          ey[i] = scaled + (cb[i] * (dhx - dhz));                                      \
-        }                                                                              \
-        if (z < nz - 1 && y >= 1 && y < ny - 1 && x >= 1 && x < nx - 1) {              \
-          T scaled = ez[i] * ca[i];                                                    \
-          T dhx = hx[i] - hx[IDX(z, y - 1, x)];                                        \
-          T dhy = hy[i] - hy[IDX(z, y, x - 1)];                                        \
-          ez[i] = scaled + (cb[i] * (dhy - dhx));                                      \
-        }                                                                              \
-      }                                                                                \
-  /* ---- phase 4: E CPML, z faces, then x, then y ---- */                            \
-  if (phase == 4)                                                                      \
   for (int z = lo; z < hi && z < nz - 1; ++z)                                          \
-    for (int y = 0; y < ny - 1; ++y)                                                   \
-      for (int x = 0; x < nx - 1; ++x) {                                               \
-        const size_t i = IDX(z, y, x);                                                 \
-        int sd = -1, q = 0;                                                            \
-        if (z >= 1 && z < m) { sd = 0; q = z; } else if (z >= nz - m) { sd = 1; q = z - (nz - m); } \
-        if (sd >= 0) {                                                                 \
-          T *Pyz = (T *)s->psi[0][sd][1], *Pxz = (T *)s->psi[0][sd][0];                \
-          const size_t k = ((size_t)q * ny + y) * nx + x;                              \
-          const T b = be[sd][q], c = cE[sd][q];                                        \
-          Pyz[k] = b * Pyz[k] + c * (hx[i] - hx[IDX(z - 1, y, x)]) / dx;               \
-          Pxz[k] = b * Pxz[k] + c * (hy[i] - hy[IDX(z - 1, y, x)]) / dx;               \
-          ey[i] += cb[i] * dx * Pyz[k];                                                \
-          ex[i] -= cb[i] * dx * Pxz[k];                                                \
+    for (int y = 0; y < ny - 1; ++y) {                                                 \
+      const size_t r = IDX(z, y, 0);                                                   \
+      T *RS exr = ex + r; T *RS eyr = ey + r; T *RS ezr = ez + r;                      \
+      const T *RS car = ca + r; const T *RS cbr = cb + r;                              \
+      const T *RS hxr = hx + r; const T *RS hyr = hy + r; const T *RS hzr = hz + r;    \
+      if (z >= 1) {                                                                    \
+        const T *RS hyz = hy + IDX(z - 1, y, 0); const T *RS hxz = hx + IDX(z - 1, y, 0); \
+        if (y >= 1) {                                                                  \
+          const T *RS hzy = hz + IDX(z, y - 1, 0);                                     \
+          for (int x = 0; x < nx - 1; ++x)                                             \
+            exr[x] = (exr[x] * car[x]) + (cbr[x] * ((hzr[x] - hzy[x]) - (hyr[x] - hyz[x]))); \
         }                                                                              \
-        sd = -1;                                                                       \
-        if (x >= 1 && x < m) { sd = 0; q = x; } else if (x >= nx - m) { sd = 1; q = x - (nx - m); } \
-        if (sd >= 0) {                                                                 \
-          T *Pzx = (T *)s->psi[1][sd][1], *Pyx = (T *)s->psi[1][sd][0];                \
-          const size_t k = ((size_t)z * ny + y) * m + q;                               \
-          const T b = be[sd][q], c = cE[sd][q];                                        \
-          Pzx[k] = b * Pzx[k] + c * (hy[i] - hy[IDX(z, y, x - 1)]) / dx;               \
-          Pyx[k] = b * Pyx[k] + c * (hz[i] - hz[IDX(z, y, x - 1)]) / dx;               \
+        for (int x = 1; x < nx - 1; ++x)                                               \
+          eyr[x] = (eyr[x] * car[x]) + (cbr[x] * ((hxr[x] - hxz[x]) - (hzr[x] - hzr[x - 1]))); \
+      }                                                                                \
+      if (y >= 1) {                                                                    \
+        const T *RS hxy = hx + IDX(z, y - 1, 0);                                       \
+        for (int x = 1; x < nx - 1; ++x)                                               \
+          ezr[x] = (ezr[x] * car[x]) + (cbr[x] * ((hyr[x] - hyr[x - 1]) - (hxr[x] - hxy[x]))); \
+      }                                                                                \
+    }                                                                                  \
+  /* ---- phase 4: E CPML over the face regions: z faces, then x, then y ---- */      \
+  /* phase 8: E z faces, rows of the face planes [lo, hi) (planes            \
+   * 1 <= z < m and nz - m <= z < nz - 1); then phase 4: x and y faces */        \
+  if (phase == 8)                                                                      \
+  for (int w = lo; w < hi; ++w) {                                                      \
+    const int j = w / (ny - 1), y = w % (ny - 1);                                      \
+    const int sd = j < m - 1 ? 0 : 1, q = sd ? j - (m - 1) : j + 1;                    \
+    const int z = sd ? nz - m + q : q;                                                 \
+    const T b = be[sd][q], c = cE[sd][q];                                              \
+    const size_t r = IDX(z, y, 0), rz = IDX(z - 1, y, 0);                              \
+    T *RS Pyz = (T *)s->psi[0][sd][1] + ((size_t)q * ny + y) * nx;                     \
+    T *RS Pxz = (T *)s->psi[0][sd][0] + ((size_t)q * ny + y) * nx;                     \
+    T *RS exr = ex + r; T *RS eyr = ey + r;                                            \
+    const T *RS cbr = cb + r;                                                          \
+    const T *RS hxr = hx + r; const T *RS hyr = hy + r;                                \
+    const T *RS hxz = hx + rz; const T *RS hyz = hy + rz;                              \
+    for (int x = 0; x < nx - 1; ++x) {                                                 \
+      Pyz[x] = b * Pyz[x] + c * (hxr[x] - hxz[x]) / dx;                                \
+      Pxz[x] = b * Pxz[x] + c * (hyr[x] - hyz[x]) / dx;                                \
+      eyr[x] += cbr[x] * dx * Pyz[x];                                                  \
+      exr[x] -= cbr[x] * dx * Pxz[x];                                                  \
+    }                                                                                  \
+  }                                                                                    \
+  if (phase == 4)                                                                      \
+  for (int z = lo; z < hi && z < nz - 1; ++z) {                                        \
+    for (int y = 0; y < ny - 1; ++y)                                                   \
+      for (int sx = 0; sx < 2; ++sx) {                                                 \
+        const int x0 = sx ? nx - m : 1, x1 = sx ? nx - 1 : m;                          \
+        for (int x = x0; x < x1; ++x) {                                                \
+          const int qx = sx ? x - (nx - m) : x;                                        \
+          const size_t i = IDX(z, y, x);                                               \
+          T *Pzx = (T *)s->psi[1][sx][1], *Pyx = (T *)s->psi[1][sx][0];                \
+          const size_t k = ((size_t)z * ny + y) * m + qx;                              \
+          const T b = be[sx][qx], c = cE[sx][qx];                                      \
+          Pzx[k] = b * Pzx[k] + c * (hy[i] - hy[i - 1]) / dx;                          \
+          Pyx[k] = b * Pyx[k] + c * (hz[i] - hz[i - 1]) / dx;                          \
           ez[i] += cb[i] * dx * Pzx[k];                                                \
           ey[i] -= cb[i] * dx * Pyx[k];                                                \
         }                                                                              \
-        sd = -1;                                                                       \
-        if (y >= 1 && y < m) { sd = 0; q = y; } else if (y >= ny - m) { sd = 1; q = y - (ny - m); } \
-        if (sd >= 0) {                                                                 \
-          T *Pxy = (T *)s->psi[2][sd][0], *Pzy = (T *)s->psi[2][sd][1];                \
-          const size_t k = ((size_t)z * m + q) * nx + x;                               \
-          const T b = be[sd][q], c = cE[sd][q];                                        \
-          Pxy[k] = b * Pxy[k] + c * (hz[i] - hz[IDX(z, y - 1, x)]) / dx;               \
-          Pzy[k] = b * Pzy[k] + c * (hx[i] - hx[IDX(z, y - 1, x)]) / dx;               \
-          ex[i] += cb[i] * dx * Pxy[k];                                                \
-          ez[i] -= cb[i] * dx * Pzy[k];                                                \
+      }                                                                                \
+    for (int sy = 0; sy < 2; ++sy) {                                                   \
+      const int y0 = sy ? ny - m : 1, y1 = sy ? ny - 1 : m;                            \
+      for (int y = y0; y < y1; ++y) {                                                  \
+        const int qy = sy ? y - (ny - m) : y;                                          \
+        const T b = be[sy][qy], c = cE[sy][qy];                                        \
+        const size_t r = IDX(z, y, 0), ry = IDX(z, y - 1, 0);                          \
+        T *RS Pxy = (T *)s->psi[2][sy][0] + ((size_t)z * m + qy) * nx;                 \
+        T *RS Pzy = (T *)s->psi[2][sy][1] + ((size_t)z * m + qy) * nx;                 \
+        T *RS exr = ex + r; T *RS ezr = ez + r;                                        \
+        const T *RS cbr = cb + r;                                                      \
+        const T *RS hxr = hx + r; const T *RS hzr = hz + r;                            \
+        const T *RS hxy = hx + ry; const T *RS hzy = hz + ry;                          \
+        for (int x = 0; x < nx - 1; ++x) {                                             \
+          Pxy[x] = b * Pxy[x] + c * (hzr[x] - hzy[x]) / dx;                            \
+          Pzy[x] = b * Pzy[x] + c * (hxr[x] - hxy[x]) / dx;                            \
+          exr[x] += cbr[x] * dx * Pxy[x];                                              \
+          ezr[x] -= cbr[x] * dx * Pzy[x];                                              \
         }                                                                              \
       }                                                                                \
+    }                                                                                  \
+  }                                                                                    \
   /* ---- phase 5: H-field injection into E ---- */                                   \
   if (phase == 5 && inj) {                                                             \
     const T *ihx = (const T *)s->inc[2] + (size_t)s->t * ny * nx;                      \
@@ -294,11 +334,14 @@ static int run_phase(const oracle_state *s, int phase, int n) {
 /* One time step of the state. Returns 0, or 1 for a bad element type. */
 int oracle_step(const oracle_state *s) {
   if (s->dtype != 0 && s->dtype != 1) return 1;
+  const int zrows = (s->npml - 1) * 2 * (s->ny - 1);   /* z-face rows of either kind */
   run_phase(s, 0, s->nz);   /* H main */
-  run_phase(s, 1, s->nz);   /* H CPML */
+  run_phase(s, 7, zrows);   /* H CPML, z faces */
+  run_phase(s, 1, s->nz);   /* H CPML, x and y faces */
   run_phase(s, 2, s->ny);   /* injection into H */
   run_phase(s, 3, s->nz);   /* E main */
-  run_phase(s, 4, s->nz);   /* E CPML */
+  run_phase(s, 8, zrows);   /* E CPML, z faces */
+  run_phase(s, 4, s->nz);   /* E CPML, x and y faces */
   run_phase(s, 5, s->ny);   /* injection into E */
   run_phase(s, 6, 6);       /* phasors */
   return 0;
