@@ -10,7 +10,9 @@ seeded coefficients and incident planes; per-step time is the difference
 between a run of ``2 + STEPS`` steps and a run of 2 steps, after a first
 run that compiles numba's kernels, on all host cores and on one.
 
-    python oracle/reference_speed.py
+    python oracle/reference_speed.py            # per-step rates, 8x8 wavelength geometry
+    python oracle/reference_speed.py --full     # whole solves of the 2x2 (31x39x39) and
+                                                # 4x4 (55x133x133) wavelength geometries
 """
 import json
 import os
@@ -99,5 +101,54 @@ def main():
     print(json.dumps(out))
 
 
+def full_solves():
+    """Wall time of whole reference solves (all size_t steps, all host cores,
+    numba compiled beforehand) of the two small benchmark geometries."""
+    import _refshims
+    _refshims.install()
+    sys.path.insert(0, REF)
+    import h5py
+    from fdtdsarsim.cpu.main_sim import MainSimCpu
+    from fdtdsarsim.parameters import ParameterCollection, inc_filename
+    from fdtdsarsim_b200 import synthetic
+    from fdtdsarsim_b200.materials import compute_material_arrays
+    out = {'cores': os.cpu_count()}
+    for name in ('plain_2x2', 'adjoint_4x4'):
+        pc = synthetic.config_params(name, 'float32')
+        g = pc.geom_params
+        rng = np.random.default_rng(7)
+        ca, cb = compute_material_arrays(pc, synthetic.uniform_rough_soil(pc, rng))
+        inc = synthetic.plane_wave_incident(pc, g.size_t_inc, 'float32')
+        rpc = ParameterCollection()
+        for grp in ('geom_params', 'inc_beam_params', 'processing_params'):
+            for k, v in vars(getattr(pc, grp)).items():
+                setattr(getattr(rpc, grp), k, v)
+        rpc.processing_params.processing_type = 'cpu'
+        rpc.processing_params.threads_per_proc = os.cpu_count()
+        nt = g.size_t
+        runs = {}
+        for tag, steps in (('compile', 2), ('full', nt)):
+            with tempfile.TemporaryDirectory() as proj:
+                rpc.processing_params.project_dir = proj
+                rpc.geom_params.size_t = steps
+                with h5py.File(inc_filename(rpc), 'w') as f:
+                    for c in ('ex', 'ey', 'hx', 'hy'):
+                        f.create_dataset(c, data=inc[c])
+                    grp = f.create_group('phasors')
+                    for c in ('ex', 'ey', 'hx', 'hy'):
+                        grp.create_dataset(f'{c}_inc_phasor', data=np.zeros(
+                            (g.size_y - 20, g.size_x - 20), np.complex64))
+                sim = MainSimCpu(rpc, mpi=True)
+                t0 = time.perf_counter()
+                sim.run(ca, cb, tag, {})
+                runs[tag] = time.perf_counter() - t0
+        out[name] = {'grid': [g.size_z, g.size_y, g.size_x], 'size_t': nt,
+                     'reference_solve_s': round(runs['full'], 2)}
+    print(json.dumps(out))
+
+
 if __name__ == '__main__':
-    main()
+    if '--full' in sys.argv:
+        full_solves()
+    else:
+        main()
