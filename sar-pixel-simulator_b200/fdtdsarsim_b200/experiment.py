@@ -1,4 +1,4 @@
-"""Experiment driver: the reference's entry points (fdtdsarsim/experiment.py:
+"""Experiment entry points: the reference's functions (fdtdsarsim/experiment.py:
 19-97) over the device simulator."""
 import logging
 import os

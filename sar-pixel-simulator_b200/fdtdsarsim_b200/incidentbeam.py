@@ -115,8 +115,8 @@ def write_incident_file(params: ParameterCollection, ex, ey, hx, hy, inc_phasors
     """Write an incident beam file with the reference's datasets and
     metadata (cpu/incident_sim.py:94-98,166-224)."""
     fname = inc_filename(params)
-    if os.path.exists(resultsio.storage_path(fname)):
-        os.remove(resultsio.storage_path(fname))
+    if os.path.exists(fname):
+        os.remove(fname)
     proc, inc, g = params.processing_params, params.inc_beam_params, params.geom_params
     with resultsio.File(fname, 'w') as f:
         for name, arr in (('ex', ex), ('ey', ey), ('hx', hx), ('hy', hy)):

@@ -20,10 +20,7 @@ THETAS = np.linspace(-80.0, 80.0, num=161, endpoint=True)
 
 def process_all_results(project_dir: str, debug_plots=False):
     """Process every result file of a project (processresults.py:15-22)."""
-    pattern = '*.hdf5' if resultsio.BACKEND == 'hdf5' else '*.npz'
-    for fname in sorted(glob.glob(os.path.join(project_dir, 'results', pattern))):
-        if resultsio.BACKEND == 'npz':
-            fname = fname[:-4] + '.hdf5'
+    for fname in sorted(glob.glob(os.path.join(project_dir, 'results', '*.hdf5'))):
         process_results(fname, debug_plots)
 
 
