@@ -76,6 +76,13 @@ def near_field_power(phasors: Mapping, dx: float, size_z_material: int):
     return power
 
 
+def scattering_coefficient(out_pwr_far, incident_power, nx_phasor, ny_phasor, dx):
+    """Far-field power normalised by the incident power through the
+    illuminated area, times 4 pi r^2 (processresults.py:103-119)."""
+    pwr = np.asarray(out_pwr_far) / incident_power
+    return pwr * 4.0 * np.pi * (RADIUS ** 2) / (nx_phasor * ny_phasor * dx * dx)
+
+
 def process_results(filename: str, debug_plots=False, device=0):
     """Far field, near-field power and scattering coefficient of one result
     file, written back into it (processresults.py:25-125)."""
@@ -110,11 +117,9 @@ def process_results(filename: str, debug_plots=False, device=0):
             else results.create_group('scattering_coefficient')
         if 'scattering_computed' not in sc_grp.attrs:
             inp = nf_grp.attrs['incident']
-            area = nx_ph * ny_ph * dx * dx
-            h = np.asarray(ff_grp['out_pwr_far_h'][()]) / inp
-            v = np.asarray(ff_grp['out_pwr_far_v'][()]) / inp
-            sc_grp.create_dataset('scattering_coeff_h', data=h * 4.0 * np.pi * RADIUS ** 2 / area)
-            sc_grp.create_dataset('scattering_coeff_v', data=v * 4.0 * np.pi * RADIUS ** 2 / area)
+            for pol in ('h', 'v'):
+                sc_grp.create_dataset(f'scattering_coeff_{pol}', data=scattering_coefficient(
+                    ff_grp[f'out_pwr_far_{pol}'][()], inp, nx_ph, ny_ph, dx))
             sc_grp.attrs['scattering_computed'] = True
 
 

@@ -199,3 +199,53 @@ def test_incident_pulse_matches_reference():
     assert np.max(np.abs(pulse - g['pulse'])) <= 1e-15
     assert np.max(np.abs(pfft - g['pulse_fft'])) <= 1e-12 * np.max(np.abs(g['pulse_fft']))
     assert taper_radius(pc) > 0
+
+
+def test_process_results_host_stages_match_reference(tmp_path):
+    """The host stages of process_results on a result file in the
+    reference's layout (written through resultsio): far-field power
+    (processresults.py:66-76), near-field Poynting power through every face
+    (:83-93,128-257) and the scattering coefficient (:97-119) equal the
+    reference's own values for the 31x39x39 flat-soil run bit for bit
+    (fixture pipeline_cfg1.npz; the far field itself is the device
+    transform's, tested on the GPU, so it is taken from the fixture)."""
+    from fdtdsarsim_b200.processresults import (THETAS, backscatter, farfield_power,
+                                                process_results)
+    g = np.load(os.path.join(GOLDEN, 'pipeline_cfg1.npz'))
+    for pol, (e, h) in (('h', ('e_phi', 'h_theta')), ('v', ('e_theta', 'h_phi'))):
+        ph_h, ph_v = farfield_power(g['ff_e_theta'], g['ff_e_phi'], g['ff_h_theta'], g['ff_h_phi'])
+        np.testing.assert_array_equal(ph_h if pol == 'h' else ph_v, g[f'ff_out_pwr_far_{pol}'])
+    fname = str(tmp_path / 'flat.hdf5')
+    planes = [k for k in g.files if '_ph_' in k or k.endswith('_inc_phasor')]
+    assert len(planes) == 28
+    with resultsio.File(fname, 'w') as f:
+        pg = f.create_group('phasors')
+        ny, nx = g['ex_ph_u'].shape
+        pg.attrs['nx_phasor'], pg.attrs['ny_phasor'] = nx, ny
+        pg.attrs['nz_phasor'] = g['ey_ph_l'].shape[0]
+        for k in planes:
+            pg.create_dataset(k, data=g[k])
+        par = f.create_group('parameters')
+        for k in g.files:
+            if k.startswith('param_'):
+                v = g[k][()]
+                par.attrs[k[6:]] = str(v) if isinstance(v, np.str_) else v
+        f.create_group('material_metadata')
+        ff = f.create_group('farfield')
+        for k in ('e_theta', 'e_phi', 'h_theta', 'h_phi', 'out_pwr_far_h', 'out_pwr_far_v'):
+            ff.create_dataset(k, data=g[f'ff_{k}'])
+        ff.attrs['theta_angles'] = THETAS
+        ff.attrs['farfields_computed'] = True
+    process_results(fname)
+    with resultsio.File(fname, 'r') as f:
+        nf = f['near_field_power'].attrs
+        for k in g.files:
+            if k.startswith('nfp_'):
+                assert nf[k[4:]] == g[k][()], k
+        for pol in ('h', 'v'):
+            np.testing.assert_array_equal(f['scattering_coefficient'][f'scattering_coeff_{pol}'][()],
+                                          g[f'scattering_coeff_{pol}'])
+    theta = float(g['param_theta_angle'])
+    key = 'ff_e_phi' if str(g['param_polarization']).upper() == 'HH' else 'ff_e_theta'
+    idx = int(np.where(THETAS == -theta)[0][0])
+    assert backscatter(fname) == complex(g[key][idx])
