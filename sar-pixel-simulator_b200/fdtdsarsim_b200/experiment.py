@@ -6,7 +6,6 @@ from typing import Iterable
 
 from .incidentbeam import IncidentBeam
 from .materials.materialmodel import MaterialModel
-from .materials.materials import compute_material_arrays
 from .parameters import ParameterCollection, set_geom_params
 from .processresults import process_all_results
 
@@ -48,7 +47,8 @@ def run_experiment(params: ParameterCollection, materials: Iterable[MaterialMode
                             params.geom_params.simulation_duration, dx, 'metre')
             sim = get_fdtd_simulator(params)(params)
             IncidentBeam(params).setup()
-        ca, cb = compute_material_arrays(params, material)
-        sim.run(ca, cb, material.name, material.metadata)
+        # Ca/Cb on the device: the values compute_material_arrays gives
+        sim.run_eps_sigma(material.relative_permittivity, material.conductivity,
+                          material.name, material.metadata)
     process_all_results(params.processing_params.project_dir,
                         params.display_params.debug_plots)

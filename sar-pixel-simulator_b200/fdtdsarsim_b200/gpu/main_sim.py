@@ -132,16 +132,46 @@ class MainSimGpu:
         self.native.run(self.params.geom_params.size_t)
         self.native.synchronize()
 
+    def simulate_eps_sigma(self, eps_r, sigma):
+        """As simulate, with Ca/Cb computed on the device from the material
+        block's relative permittivity and conductivity (vacuum above it),
+        bit-identical to compute_material_arrays."""
+        self.native.reset()
+        self.native.set_materials_eps_sigma(eps_r, sigma)
+        self._ensure_incident()
+        self.native.run(self.params.geom_params.size_t)
+        self.native.synchronize()
+
     def run(self, Ca: np.ndarray, Cb: np.ndarray, material_name: str, material_meta: dict):
         """Simulate one material model and save its phasors
         (gpu/main_sim.py:74-115)."""
+        self.Ca = np.asarray(Ca, dtype=self.dtype)
+        self.Cb = np.asarray(Cb, dtype=self.dtype)
+        self._run_and_save(lambda: self.simulate(self.Ca, self.Cb), material_name, material_meta)
+
+    def run_eps_sigma(self, eps_r: np.ndarray, sigma: np.ndarray, material_name: str,
+                      material_meta: dict):
+        """run() for a material block given as (size_z_material, ny, nx)
+        relative permittivity and conductivity: the update coefficients are
+        computed on the device instead of by compute_material_arrays on the
+        host (same values bit for bit, a fraction of the host's time and
+        0.7x the upload)."""
+        if np.shape(eps_r) != np.shape(sigma):
+            raise RuntimeError('Permittivity and conductivity arrays have different shapes')
+        g = self.params.geom_params
+        want = (g.size_z_material, g.size_y, g.size_x)
+        if tuple(np.shape(eps_r)) != want:
+            raise ValueError(f'material block is {tuple(np.shape(eps_r))}, expected {want}')
+        self.Ca = self.Cb = None
+        self._run_and_save(lambda: self.simulate_eps_sigma(eps_r, sigma), material_name,
+                           material_meta)
+
+    def _run_and_save(self, simulate, material_name, material_meta):
         logger.info('Starting a GPU FDTD simulation of %s on GPU %s', material_name, self.gpu_num)
         t0 = time.monotonic()
-        self.Ca = Ca.astype(self.dtype)
-        self.Cb = Cb.astype(self.dtype)
         out_name = results_filename(self.params, material_name)
         if not resultsio.exists(out_name):
-            self.simulate(self.Ca, self.Cb)
+            simulate()
             self.save_results(material_name, material_meta)
         else:
             logger.info('%s already exists, skipping', out_name)

@@ -212,3 +212,46 @@ def test_run_experiment_hands_the_beam_over_on_the_device(tmp_path):
             out.append({k: np.asarray(f['phasors'][k]) for k in _native.PHASOR_NAMES})
     for k in _native.PHASOR_NAMES:
         assert bits_equal(out[0][k], out[1][k]), k
+
+
+def test_run_eps_sigma_equals_run_with_host_coefficients(tmp_path):
+    """MainSimGpu.run_eps_sigma (Ca/Cb computed on the device, the path
+    run_experiment takes) writes the same result file as run() given the
+    host's compute_material_arrays (materials/materials.py:23-68), bit for
+    bit, on a rough two-material block; a block of the wrong shape is
+    rejected before anything runs."""
+    import fdtdsarsim_b200 as fdtd
+    from fdtdsarsim_b200 import resultsio
+    from fdtdsarsim_b200.gpu.main_sim import MainSimGpu
+    from fdtdsarsim_b200.materials import compute_material_arrays
+    from fdtdsarsim_b200.parameters import results_filename
+    ref = np.load(os.path.join(GOLDEN, 'pipeline_cfg1.npz'))
+    user = json.loads(str(ref['params_json']))
+    user.update({'processing_type': 'gpu', 'project_dir': str(tmp_path), 'gpu_num': 0})
+    path = tmp_path / 'params.json'
+    path.write_text(json.dumps(user))
+    pc = fdtd.load_from_json(str(path))
+    g = pc.geom_params
+    model = next(fdtd.materials.rough_dielectric(pc, 7.5, 0.03, 0.3 * g.cell_size * 4,
+                                                 0.5 * g.size_z_material * g.cell_size,
+                                                 4 * g.cell_size, 1, seed=11))
+    fdtd.IncidentBeam(pc).setup()
+    sim = MainSimGpu(pc)
+    try:
+        ca, cb = compute_material_arrays(pc, model)
+        sim.run(ca, cb, 'host', model.metadata)
+        sim.run_eps_sigma(model.relative_permittivity, model.conductivity, 'device',
+                          model.metadata)
+        with pytest.raises(ValueError):
+            sim.run_eps_sigma(model.relative_permittivity[1:], model.conductivity[1:], 'bad', {})
+        with pytest.raises(RuntimeError):
+            sim.run_eps_sigma(model.relative_permittivity, model.conductivity[1:], 'bad', {})
+    finally:
+        sim.close()
+    out = []
+    for name in ('host', 'device'):
+        with resultsio.File(results_filename(pc, name), 'r') as f:
+            out.append({k: np.asarray(f['phasors'][k]) for k in _native.PHASOR_NAMES})
+    for k in _native.PHASOR_NAMES:
+        assert bits_equal(out[0][k], out[1][k]), k
+    assert np.max(np.abs(out[0]['ex_ph_u'])) > 0
