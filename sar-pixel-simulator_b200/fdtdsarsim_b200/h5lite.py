@@ -596,6 +596,13 @@ class File(Group):
         self._eof = addr + len(data)
         return addr
 
+    def _place(self, addr, data):
+        """Append ``data``, which must land at ``addr`` (precomputed because
+        the structure refers to its own address)."""
+        got = self._append(data)
+        if got != addr:
+            raise RuntimeError(f'HDF5 structure placed at {got}, expected {addr}')
+
     def _reserve(self, nbytes):
         addr = _pad8(self._eof)
         self._eof = addr + nbytes
@@ -915,8 +922,8 @@ class File(Group):
             offs.append(len(seg))
             seg += _padded(name.encode('utf-8') + b'\0')
         haddr = _pad8(self._eof)
-        assert self._append(b'HEAP' + struct.pack('<B3xQQQ', 0, len(seg), HEAP_FREE_NULL,
-                                                  haddr + 32) + bytes(seg)) == haddr
+        self._place(haddr, b'HEAP' + struct.pack('<B3xQQQ', 0, len(seg), HEAP_FREE_NULL,
+                                                 haddr + 32) + bytes(seg))
         nodes = []                                   # (address, heap offset of the last name)
         for i in range(0, len(entries), 2 * LEAF_K):
             blob = bytearray(b'SNOD' + struct.pack('<BBH', 1, 0, len(entries[i:i + 2 * LEAF_K])))
@@ -941,7 +948,7 @@ class File(Group):
                 for caddr, last in kids:
                     blob += struct.pack('<QQ', caddr, last)
                 blob += b'\0' * (BTREE_SIZE - len(blob))
-                assert self._append(bytes(blob)) == addrs[j]
+                self._place(addrs[j], bytes(blob))
                 left_key = kids[-1][1] if kids else 0
                 upper.append((addrs[j], left_key))
             if len(upper) == 1:

@@ -402,3 +402,36 @@ def test_result_file_layout_through_resultsio(tmp_path):
         assert f['phasors'].attrs['nz_phasor'] == 7
         np.testing.assert_array_equal(f['material_metadata'].attrs['epsilon_r'], [5.0, 8.0])
         assert f['phasors/hz_ph_b'].dtype == np.complex64
+
+
+def test_large_writes_in_pieces_and_dataset_copies(tmp_path, monkeypatch):
+    """Raw data longer than one write piece is written in pieces; a dataset
+    created from another file's dataset (the reference copies the incident
+    phasors that way, cpu/main_sim.py:239-246) copies its values."""
+    monkeypatch.setattr(h5lite, 'WRITE_CHUNK', 1000)
+    src, dst = str(tmp_path / 'src.hdf5'), str(tmp_path / 'dst.hdf5')
+    data = np.random.default_rng(5).standard_normal((17, 33, 7)).astype(np.float32)
+    with h5lite.File(src, 'w') as f:
+        f.create_group('phasors').create_dataset('ex_inc_phasor', data=data[0] + 1j * data[1])
+        f.create_dataset('ex', data=data)
+    with h5lite.File(src, 'r') as s, h5lite.File(dst, 'w') as d:
+        d.create_group('phasors').create_dataset('ex_inc_phasor', data=s['phasors']['ex_inc_phasor'])
+        np.testing.assert_array_equal(s['ex'][()], data)
+    with h5lite.File(dst, 'r') as d:
+        np.testing.assert_array_equal(d['phasors/ex_inc_phasor'][()], data[0] + 1j * data[1])
+    SpecWalker(dst)
+
+
+def test_writes_survive_optimised_python(tmp_path):
+    """Writing does not depend on assert statements (python -O)."""
+    import subprocess
+    import sys
+    path = str(tmp_path / 'o.hdf5')
+    code = ('import sys, numpy as np; sys.path.insert(0, sys.argv[2]); '
+            'from fdtdsarsim_b200 import h5lite; f = h5lite.File(sys.argv[1], "w"); '
+            'g = f.create_group("g"); g.create_dataset("d", data=np.arange(5.0)); f.close()')
+    pkg = os.path.dirname(os.path.dirname(h5lite.__file__))
+    subprocess.run([sys.executable, '-O', '-c', code, path, pkg], check=True)
+    SpecWalker(path)
+    with h5lite.File(path, 'r') as f:
+        np.testing.assert_array_equal(f['g/d'][()], np.arange(5.0))
