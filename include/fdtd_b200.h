@@ -108,7 +108,8 @@ int fdtd_device_count(int *count);
  * _allocate_cuda_arrays (:512-640) and _clear_cuda_arrays (:691-787). */
 int fdtd_create(const fdtd_geometry *geom, int device, fdtd_sim **out);
 
-/* Frees every device resource of the handle. */
+/* Frees every device resource of the handle. Refused (FDTD_ERR_STATE, the
+ * handle stays valid) while the simulation is a member of a batch. */
 int fdtd_destroy(fdtd_sim *sim);
 
 /* Sets a tuning or behaviour option (FDTD_OPT_*). */
@@ -245,7 +246,8 @@ int fdtd_grad_backward(fdtd_sim *s, const double *dj_dre, const double *dj_dim, 
  * MainSimGpu.run (gpu/main_sim.py:74-115) and a separate time loop.
  * The members stay ordinary handles: set their absorbers, materials and
  * incident planes, run the batch, then read each member's phasors and
- * fields as usual. Members must outlive the batch; a member's own calls are
+ * fields as usual. Members must outlive the batch (fdtd_destroy refuses a
+ * member until its batches are destroyed); a member's own calls are
  * ordered after the batch's work. Each member advances nsteps from its own
  * step index, using its current field set in place (the split step). */
 typedef struct fdtd_batch fdtd_batch;

@@ -56,6 +56,7 @@ int fdtd::report_error(int code, const char* msg) { return fail(code, "%s", msg)
 struct fdtd_sim {
   fdtd_geometry g{};
   int device = 0;
+  int batch_refs = 0;                    // batches that hold this simulation as a member
   size_t esz = 4;
   int pitch = 0;
   long long plane = 0, vol = 0;          // elements
@@ -136,6 +137,7 @@ struct fdtd_sim {
 // and launches one kernel per phase for all of them.
 struct fdtd_batch {
   std::vector<fdtd_sim*> sims;
+  bool members_counted = false;  // the members' batch_refs include this batch
   int device = 0;
   int dtype = FDTD_F32;
   cudaStream_t stream = nullptr;
@@ -523,6 +525,9 @@ int fdtd_create(const fdtd_geometry* geom, int device, fdtd_sim** out) {
 
 int fdtd_destroy(fdtd_sim* s) {
   if (!s) return FDTD_OK;
+  if (s->batch_refs > 0)
+    return fail(FDTD_ERR_STATE, "simulation is a member of %d batch(es): destroy them first",
+                s->batch_refs);
   cudaSetDevice(s->device);
   if (s->own) cudaStreamSynchronize(s->own);
   for (auto& b : s->bufs) cudaFree(b.p);
@@ -1140,12 +1145,16 @@ int fdtd_batch_create(fdtd_sim* const* sims, int n, fdtd_batch** out) {
     cudaGetLastError();
     return fail(FDTD_ERR_CUDA, "batch set-up: %s", cudaGetErrorString(e));
   }
+  for (fdtd_sim* m : b->sims) ++m->batch_refs;
+  b->members_counted = true;
   *out = b;
   return FDTD_OK;
 }
 
 int fdtd_batch_destroy(fdtd_batch* b) {
   if (!b) return FDTD_OK;
+  if (b->members_counted)
+    for (fdtd_sim* m : b->sims) --m->batch_refs;
   cudaSetDevice(b->device);
   if (b->stream) cudaStreamSynchronize(b->stream);
   if (b->gexec) cudaGraphExecDestroy(b->gexec);

@@ -192,8 +192,10 @@ class NativeSim:
         self.nz_ph = geom.nz - 2 * geom.npml
 
     def close(self):
+        """Free the handle (FdtdError while it is a member of an open
+        Batch; the handle then stays valid)."""
         if getattr(self, 'h', None) is not None and self.h.value:
-            lib.fdtd_destroy(self.h)
+            check(lib.fdtd_destroy(self.h))
             self.h = None
 
     def __del__(self):

@@ -103,4 +103,9 @@ def test_batch_rejects_bad_members():
     with pytest.raises(_native.FdtdError) as ei:
         batch.run(1)   # materials not set
     assert ei.value.code == _native.FDTD_ERR_STATE
+    with pytest.raises(_native.FdtdError) as ei:
+        a.close()      # a member outlives its batch
+    assert ei.value.code == _native.FDTD_ERR_STATE and a.h is not None
     batch.close()
+    a.close()
+    assert a.h is None
