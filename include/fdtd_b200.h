@@ -66,6 +66,10 @@ extern "C" {
 #define FDTD_OPT_ZCHUNK       8  /* fused kernel z planes per block (0 = automatic) */
 #define FDTD_OPT_FUSED_SLAB   9  /* 1: the fused step marches the CPML z slabs too
                                     (default 0: the split passes sweep them) */
+#define FDTD_OPT_BATCH_STREAMS 10 /* fdtd_batch_set_option: 1 runs every member's
+                                    own step path on its own stream, side by
+                                    side; 0 (default) one launch per pass for
+                                    all members */
 
 /* kernel kinds of fdtd_get_kernel_time */
 #define FDTD_TIME_STEP    0   /* the field-update kernel(s) of a step */
@@ -254,7 +258,11 @@ typedef struct fdtd_batch fdtd_batch;
 
 int fdtd_batch_create(fdtd_sim *const *sims, int n, fdtd_batch **out);
 int fdtd_batch_destroy(fdtd_batch *b);
-/* FDTD_OPT_GRAPH_CHUNK: steps per captured graph (0: no graph; default 64). */
+/* FDTD_OPT_GRAPH_CHUNK: steps per captured graph (0: no graph; default 64).
+ * FDTD_OPT_BATCH_STREAMS = 1: each member advances by its own step path
+ * (its FDTD_OPT_KERNEL, its own graph chunks) on its own stream, forked from
+ * and joined to the batch stream; results are those of fdtd_run on each
+ * member. The all-or-nothing checks of fdtd_batch_run apply in both modes. */
 int fdtd_batch_set_option(fdtd_batch *b, int option, int value);
 int fdtd_batch_run(fdtd_batch *b, int nsteps);
 int fdtd_batch_synchronize(fdtd_batch *b);

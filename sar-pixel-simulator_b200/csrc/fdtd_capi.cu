@@ -151,6 +151,8 @@ struct fdtd_batch {
   int graph_chunk = 64;
   cudaGraphExec_t gexec = nullptr;
   int gexec_chunk = 0;
+  bool streams = false;            // FDTD_OPT_BATCH_STREAMS: members on their own streams
+  std::vector<cudaEvent_t> mev;    // one per member: the end of its work in a streams run
 };
 
 namespace {
@@ -1112,6 +1114,26 @@ int batch_run(fdtd_batch* b, int nsteps) {
   return FDTD_OK;
 }
 
+// FDTD_OPT_BATCH_STREAMS: every member advances by its own step path (its
+// kernel choice, its graph chunks) on its own stream, forked from the batch
+// stream after the batch's earlier work and joined back into it, so that the
+// members' small launches run side by side on the device. Each member's
+// results are those of fdtd_run on it alone.
+template <class T>
+int batch_run_streams(fdtd_batch* b, int nsteps) {
+  CK(cudaEventRecord(b->ev, b->stream));
+  for (fdtd_sim* s : b->sims) CK(cudaStreamWaitEvent(s->stream, b->ev, 0));
+  for (fdtd_sim* s : b->sims) {
+    const int rc = run_steps<T>(s, nsteps);
+    if (rc) return rc;
+  }
+  for (size_t m = 0; m < b->sims.size(); ++m) {
+    CK(cudaEventRecord(b->mev[m], b->sims[m]->stream));
+    CK(cudaStreamWaitEvent(b->stream, b->mev[m], 0));
+  }
+  return FDTD_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1140,6 +1162,9 @@ int fdtd_batch_create(fdtd_sim* const* sims, int n, fdtd_batch** out) {
   if (e == cudaSuccess) e = cudaMalloc(&b->d_models, msz * n);
   if (e == cudaSuccess) e = cudaMalloc(&b->d_start, sizeof(int) * (n + 1));
   if (e == cudaSuccess) e = cudaMalloc(&b->d_start_ph, sizeof(int) * (n + 1));
+  b->mev.assign(n, nullptr);
+  for (int i = 0; i < n && e == cudaSuccess; ++i)
+    e = cudaEventCreateWithFlags(&b->mev[i], cudaEventDisableTiming);
   if (e != cudaSuccess) {
     fdtd_batch_destroy(b);
     cudaGetLastError();
@@ -1162,6 +1187,8 @@ int fdtd_batch_destroy(fdtd_batch* b) {
   if (b->d_start) cudaFree(b->d_start);
   if (b->d_start_ph) cudaFree(b->d_start_ph);
   if (b->ev) cudaEventDestroy(b->ev);
+  for (cudaEvent_t ev : b->mev)
+    if (ev) cudaEventDestroy(ev);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
   cudaGetLastError();
@@ -1170,6 +1197,11 @@ int fdtd_batch_destroy(fdtd_batch* b) {
 
 int fdtd_batch_set_option(fdtd_batch* b, int option, int value) {
   if (!b) return fail(FDTD_ERR_INVALID, "null batch handle");
+  if (option == FDTD_OPT_BATCH_STREAMS) {
+    if (value != 0 && value != 1) return fail(FDTD_ERR_INVALID, "batch streams must be 0 or 1");
+    b->streams = value == 1;
+    return FDTD_OK;
+  }
   if (option != FDTD_OPT_GRAPH_CHUNK) return fail(FDTD_ERR_INVALID, "unknown batch option %d", option);
   if (value < 0) return fail(FDTD_ERR_INVALID, "bad graph chunk %d", value);
   b->graph_chunk = value;
@@ -1192,6 +1224,9 @@ int fdtd_batch_run(fdtd_batch* b, int nsteps) {
   if (nsteps == 0) return FDTD_OK;
   cudaError_t e = cudaSetDevice(b->device);
   if (e != cudaSuccess) return fail(FDTD_ERR_CUDA, "cudaSetDevice: %s", cudaGetErrorString(e));
+  if (b->streams)
+    return b->dtype == FDTD_F32 ? batch_run_streams<float>(b, nsteps)
+                                : batch_run_streams<double>(b, nsteps);
   return b->dtype == FDTD_F32 ? batch_run<float>(b, nsteps) : batch_run<double>(b, nsteps);
 }
 

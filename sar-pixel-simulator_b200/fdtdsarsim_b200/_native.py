@@ -37,6 +37,7 @@ OPT_CHECK_EVERY = 6
 OPT_TIMING = 7
 OPT_ZCHUNK = 8
 OPT_FUSED_SLAB = 9
+OPT_BATCH_STREAMS = 10
 
 TIME_STEP = 0
 TIME_PHASOR = 1
@@ -481,20 +482,27 @@ def fused_plan_boxes(nx, ny, nz, npml, tfsf_z, tile_y=4, zchunk=0, slab=False):
 
 
 class Batch:
-    """Several NativeSim members advanced together (fdtd_batch_*): one launch
-    per pass for all members each step, chunks of steps replayed from a
-    captured CUDA graph. Members keep their own state and readback calls."""
+    """Several NativeSim members advanced together (fdtd_batch_*): by
+    default one launch per pass for all members each step, chunks of steps
+    replayed from a captured CUDA graph; with ``streams=True`` every member
+    runs its own step path on its own stream, side by side. Members keep
+    their own state and readback calls."""
 
-    def __init__(self, sims, graph_chunk=None):
+    def __init__(self, sims, graph_chunk=None, streams=False):
         self.sims = list(sims)   # keeps the members alive while the batch exists
         arr = (_P * len(self.sims))(*[s.h for s in self.sims])
         self.h = _P()
         check(lib.fdtd_batch_create(arr, len(self.sims), ctypes.byref(self.h)))
         if graph_chunk is not None:
             self.set_graph_chunk(graph_chunk)
+        if streams:
+            self.set_streams(True)
 
     def set_graph_chunk(self, steps):
         check(lib.fdtd_batch_set_option(self.h, OPT_GRAPH_CHUNK, int(steps)))
+
+    def set_streams(self, on):
+        check(lib.fdtd_batch_set_option(self.h, OPT_BATCH_STREAMS, int(bool(on))))
 
     def run(self, nsteps):
         check(lib.fdtd_batch_run(self.h, int(nsteps)))

@@ -55,6 +55,34 @@ def test_batch_matches_oracle_for_every_member(chunk, calls):
         sim.close()
 
 
+@pytest.mark.parametrize('kernels', ['fused', 'mixed'])
+def test_streams_mode_matches_oracle_for_every_member(kernels):
+    """FDTD_OPT_BATCH_STREAMS: every member on its own stream with its own
+    kernel (all fused, or fused and split mixed) ends with the oracle's
+    fields and phasors; the all-or-nothing step check still applies; the
+    mode can be switched between calls."""
+    members = _members(MODELS, seed=560)
+    sims = [s for _, s in members]
+    if kernels == 'mixed':
+        for s in sims[::2]:
+            s.set_option(_native.OPT_KERNEL, _native.FDTD_KERNEL_SPLIT)
+    batch = _native.Batch(sims, graph_chunk=4, streams=True)
+    batch.run(7)
+    with pytest.raises(_native.FdtdError):
+        batch.run(24)             # would pass size_t: nothing runs
+    batch.set_streams(False)
+    batch.run(9)
+    batch.set_streams(True)
+    batch.run(14)
+    batch.synchronize()
+    for orc, sim in members:
+        assert sim.step_index() == 30
+        _assert_member(orc, sim)
+    with pytest.raises(_native.FdtdError):
+        _native.check(_native.lib.fdtd_batch_set_option(batch.h, _native.OPT_BATCH_STREAMS, 2))
+    batch.close()
+
+
 def test_batch_float64_members():
     members = _members(MODELS[:2], seed=520, dtype='float64')
     batch = _native.Batch([s for _, s in members], graph_chunk=8)
