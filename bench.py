@@ -466,12 +466,13 @@ def run_batch(a):
     cells = [pc.geom_params.size_x * pc.geom_params.size_y * pc.geom_params.size_z
              for pc, _, _, _ in models]
     total = int(sum(cells))
-    sims = []
+    sims, choices = [], []
     for pc, ca, cb, inc in models:
         geom = native_geometry(pc)
         sim = _native.NativeSim(geom, 0)
         sim.set_absorbers(packed_profiles(pc))
         choice = tuning.choose(geom)
+        choices.append(choice)
         sim.set_option(_native.OPT_KERNEL, choice['kernel'])
         sim.set_option(_native.OPT_TILE_X, choice['tile_x'])
         sim.set_option(_native.OPT_TILE_Y, choice['tile_y'])
@@ -489,16 +490,26 @@ def run_batch(a):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1)
 
-    # batched: every member each step, one launch per pass, graph chunks
+    # batched, two modes: (split) every member each step, one launch per
+    # pass, graph chunks; (streams) every member's own step path on its own
+    # stream, side by side. The faster is the batched result.
     batch = _native.Batch(sims)
     bstream = torch.cuda.ExternalStream(batch.stream())
     batch.run(a.warmup)
     batch.synchronize()
     clocks = ClockSampler(0)
     clocks.start()
-    ms_b = timed(bstream, lambda: batch.run(a.steps))
+    ms_split = timed(bstream, lambda: batch.run(a.steps))
+    for s in sims:
+        s.reset()
+    batch.set_streams(True)
+    batch.run(a.warmup)
+    batch.synchronize()
+    ms_streams = timed(bstream, lambda: batch.run(a.steps))
     clk = clocks.stop()
     batch.close()
+    mode = 'streams' if ms_streams < ms_split else 'split'
+    ms_b = min(ms_streams, ms_split)
 
     # one after another: each model's own time loop (its default kernel), on
     # one stream so the solves do not overlap
@@ -529,15 +540,22 @@ def run_batch(a):
                    'models': a.models, 'cells_total': total,
                    'nx_range': [int(min(nx)), int(max(nx))], 'nz_range': [int(min(nz)), int(max(nz))],
                    'l2': 'inputs larger than L2 (fields of all models)',
-                   'batched': 'split step of every model per launch, 64-step graph chunks'},
+                   'batched': ('every model on its own stream, its default kernel, side by side'
+                               if mode == 'streams' else
+                               'split step of every model per launch, 64-step graph chunks'),
+                   'modes_ms_per_step': {'split': round(ms_split / a.steps, 4),
+                                         'streams': round(ms_streams / a.steps, 4)}},
         'sequential': {'value': round(seq_value, 1), 'ms_per_step': round(ms_s / a.steps, 4),
                        'kernel': 'each model alone, its default kernel, one shared stream'},
         'speedup_vs_sequential': round(ms_s / ms_b, 3),
         'roofline': {'bound': 'hbm', 'achieved': round(achieved, 1), 'peak': peak, 'unit': 'GB/s',
                      'frac': round(achieved / peak, 4), 'traffic': None, 'peak_source': peak_kind,
-                     'kernel': 'batch_split_step'},
+                     'kernel': 'fused_step (member streams)' if mode == 'streams' else 'batch_split_step'},
         'cpu_baseline': None, 'e2e': None,
-        'gpu_launches': 3 * a.steps + 1 + (a.steps + 63) // 64, 'clocks': clk,
+        'gpu_launches': (sum(3 if c['kernel'] == _native.FDTD_KERNEL_SPLIT
+                             else 4 + int(bool(c.get('slab', 0))) for c in choices) * a.steps
+                         if mode == 'streams' else 3 * a.steps + 1 + (a.steps + 63) // 64),
+        'clocks': clk,
     }
     print(json.dumps(line))
 
