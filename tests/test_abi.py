@@ -65,3 +65,26 @@ def test_near2far_rejects_even_planes():
     with pytest.raises(_native.FdtdError) as ei:
         _native.near2far(z, z, z, z, 4, 4, 5, 0.01, 2000.0, [0.0], [0.0], 5.4e9)
     assert ei.value.code == _native.FDTD_ERR_INVALID
+
+
+def test_binding_constants_match_the_header():
+    """Every integer #define of the header that the ctypes binding mirrors
+    (FDTD_X as FDTD_X or X) has the header's value; every option is bound."""
+    src = open(os.path.join(ROOT, 'include', 'fdtd_b200.h')).read()
+    defines = dict((k, int(v)) for k, v in
+                   re.findall(r'^#define\s+(FDTD_\w+)\s+(-?\d+)\b', src, flags=re.M))
+    checked = 0
+    for name, value in defines.items():
+        short = name[len('FDTD_'):]
+        for attr in (name, short):
+            if hasattr(_native, attr):
+                assert getattr(_native, attr) == value, (name, attr)
+                checked += 1
+                break
+        else:
+            if short.startswith('OPT_'):
+                raise AssertionError(f'{name} has no binding constant')
+            if short.startswith('POL_'):
+                assert _native.POLARIZATIONS[short[4:]] == value, name
+                checked += 1
+    assert checked >= 20 and defines['FDTD_OPT_BATCH_STREAMS'] == _native.OPT_BATCH_STREAMS
