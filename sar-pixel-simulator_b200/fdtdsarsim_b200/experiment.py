@@ -2,7 +2,9 @@
 19-97) over the device simulator."""
 import logging
 import os
-from typing import Iterable
+import queue
+import threading
+from typing import Iterable, Iterator, TypeVar
 
 from .incidentbeam import IncidentBeam
 from .materials.materialmodel import MaterialModel
@@ -30,25 +32,89 @@ def get_fdtd_simulator(params: ParameterCollection):
     raise ValueError('Invalid processing type')
 
 
-def run_experiment(params: ParameterCollection, materials: Iterable[MaterialModel]):
+T = TypeVar('T')
+
+
+def prefetched(items: Iterable[T], depth: int = 1) -> Iterator[T]:
+    """``items`` in order, produced by a background thread up to ``depth``
+    ahead of the consumer, so that a host-side material generator makes the
+    next model while the device solves the current one (the solve waits in
+    the library with the GIL released). An exception of the producer is
+    raised in the consumer where the item would have been; closing the
+    iterator early stops the producer."""
+    q: queue.Queue = queue.Queue(maxsize=max(1, depth))
+    stop = threading.Event()
+    end = object()
+
+    def put(entry):
+        while not stop.is_set():
+            try:
+                q.put(entry, timeout=0.1)
+                return True
+            except queue.Full:
+                continue
+        return False
+
+    def produce():
+        try:
+            for item in items:
+                if not put((True, item)):
+                    return
+            put((True, end))
+        except BaseException as exc:  # handed to the consumer
+            put((False, exc))
+
+    worker = threading.Thread(target=produce, name='material-prefetch', daemon=True)
+    worker.start()
+    try:
+        while True:
+            try:
+                ok, item = q.get(timeout=0.5)
+            except queue.Empty:
+                if not worker.is_alive() and q.empty():
+                    raise RuntimeError('material prefetch thread ended without a result')
+                continue
+            if not ok:
+                raise item
+            if item is end:
+                return
+            yield item
+    finally:
+        stop.set()
+
+
+def run_experiment(params: ParameterCollection, materials: Iterable[MaterialModel],
+                   prefetch: int = 1):
     """Simulate every material model with one shared incident beam, then
-    post-process all results (experiment.py:41-97)."""
+    post-process all results (experiment.py:41-97). ``prefetch`` (this
+    package's addition; 0 turns it off) is how many models the host makes
+    ahead while the device runs."""
     g = params.geom_params
     geom_specified = not (g.size_x == 0 and g.size_y == 0 and g.size_z == 0)
+    it = iter(materials)
     sim = None
     if geom_specified:
         sim = get_fdtd_simulator(params)(params)
         IncidentBeam(params).setup()
-    for material in materials:
-        if sim is None:
-            nz_mat, ny, nx = material.conductivity.shape
-            dx = material.cell_size
+    else:
+        # the first model sets the geometry before any other model is made
+        first = next(it, None)
+        if first is not None:
+            nz_mat, ny, nx = first.conductivity.shape
+            dx = first.cell_size
             set_geom_params(params, nx * dx, ny * dx, nz_mat * dx,
                             params.geom_params.simulation_duration, dx, 'metre')
             sim = get_fdtd_simulator(params)(params)
             IncidentBeam(params).setup()
-        # Ca/Cb on the device: the values compute_material_arrays gives
-        sim.run_eps_sigma(material.relative_permittivity, material.conductivity,
-                          material.name, material.metadata)
+            _simulate(sim, first)
+    if sim is not None:
+        for material in (prefetched(it, prefetch) if prefetch > 0 else it):
+            _simulate(sim, material)
     process_all_results(params.processing_params.project_dir,
                         params.display_params.debug_plots)
+
+
+def _simulate(sim, material: MaterialModel):
+    # Ca/Cb on the device: the values compute_material_arrays gives
+    sim.run_eps_sigma(material.relative_permittivity, material.conductivity,
+                      material.name, material.metadata)
