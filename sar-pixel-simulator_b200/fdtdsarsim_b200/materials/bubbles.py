@@ -24,7 +24,7 @@ def material_volume(rel_permittivity, conductivity):
     return np.sum(np.logical_or(rel_permittivity != 1.0, conductivity != 0.0))
 
 
-@numba.njit(cache=False)
+@numba.njit(cache=False, nogil=True)
 def _paint(eps, cond, surf, rng, target, vol, r_min, r_max, fixed_radius, cell, eps_b, cond_b):
     nz, ny, nx = eps.shape
     while vol > target:
