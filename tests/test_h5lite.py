@@ -435,3 +435,47 @@ def test_writes_survive_optimised_python(tmp_path):
     SpecWalker(path)
     with h5lite.File(path, 'r') as f:
         np.testing.assert_array_equal(f['g/d'][()], np.arange(5.0))
+
+
+def test_reads_object_headers_continued_in_another_chunk(tmp_path):
+    """libhdf5 continues a version-1 object header in further chunks when
+    its messages outgrow the first one (h5py does this for the reference's
+    /parameters group of ~35 attributes). A written header is split here
+    into a first chunk that ends with a continuation message (0x10) and a
+    second chunk at the end of the file; both readers follow it."""
+    path = str(tmp_path / 'cont.hdf5')
+    with h5lite.File(path, 'w') as f:
+        g = f.create_group('parameters')
+        for k in range(12):
+            g.attrs[f'a{k:02d}'] = float(k)
+        g.attrs['polarization'] = 'VV'
+    w = SpecWalker(path)
+    raw = bytearray(open(path, 'rb').read())
+    # the group's header: the root SNOD's only entry
+    with h5lite.File(path, 'r') as f:
+        stab = [b for t, b in f._messages(w.root) if t == 0x11][0]
+        ((_, addr),) = f._walk(struct.unpack_from('<Q', stab)[0])
+    ver, _, nmsgs, refs, size = struct.unpack_from('<BBHII', raw, addr)
+    msgs, p = [], addr + 16
+    while p < addr + 16 + size:
+        t, sz = struct.unpack_from('<HH', raw, p)
+        msgs.append(bytes(raw[p:p + 8 + sz]))
+        p += 8 + sz
+    keep, move = msgs[:5], msgs[5:]
+    second = b''.join(move)
+    caddr = h5lite._pad8(len(raw))
+    cont = struct.pack('<HHB3x', 0x10, 16, 0) + struct.pack('<QQ', caddr, len(second))
+    first = b''.join(keep) + cont
+    gap = size - len(first)
+    assert gap >= 8
+    first += struct.pack('<HHB3x', 0, gap - 8, 0) + b'\0' * (gap - 8)    # NIL message
+    raw[addr + 16:addr + 16 + size] = first
+    struct.pack_into('<H', raw, addr + 2, len(keep) + 1 + 1 + len(move))
+    raw += b'\0' * (caddr - len(raw)) + second
+    struct.pack_into('<Q', raw, w.sb + 40, len(raw))                    # end-of-file address
+    open(path, 'wb').write(bytes(raw))
+    SpecWalker(path)
+    with h5lite.File(path, 'r') as f:
+        a = f['parameters'].attrs
+        assert [a[f'a{k:02d}'] for k in range(12)] == [float(k) for k in range(12)]
+        assert a['polarization'] == 'VV'
