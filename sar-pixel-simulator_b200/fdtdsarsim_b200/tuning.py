@@ -11,7 +11,6 @@ and element type (``$FDTDSARSIM_B200_TUNING``, else
 """
 import json
 import os
-from typing import Optional
 
 import numpy as np
 

@@ -3,7 +3,6 @@ differences of the float64 forward oracle: d P_h / d eps_r and d P_h / d sigma
 at material cells. This pins the CPU reference that the device adjoint is
 checked against."""
 import numpy as np
-import pytest
 
 from adjoint_ref import AdjointRef, ca_cb_partials
 from fdtdsarsim_b200.absorbers import cpml_profiles

@@ -2,7 +2,6 @@
 one launch per pass for all members, chunks replayed from a captured CUDA
 graph. Each member must end with the oracle's fields and phasors bit for
 bit, however the run is cut into calls and graph chunks."""
-import numpy as np
 import pytest
 
 from fdtdsarsim_b200 import _native

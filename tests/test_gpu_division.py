@@ -2,7 +2,6 @@
 rounded reciprocal and one FMA correction (Markstein's method). On the
 device it must give the IEEE quotient bit for bit: every float input is
 checked, and 2^30 sampled doubles."""
-import numpy as np
 import pytest
 import scipy.constants
 

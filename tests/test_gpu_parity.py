@@ -7,7 +7,6 @@ import os
 import numpy as np
 import pytest
 
-import fdtd_oracle as O
 from fdtdsarsim_b200 import _native
 from helpers import (GOLDEN, bits_equal, make_params, native_for, oracle_for, random_problem,
                      rel_err)
