@@ -92,7 +92,9 @@ def workload_desc(pc, name):
         'materials': 'synthetic seeded (snowpack of ice spheres over rough soil)'
         if name == 'plain_16x16' else 'synthetic seeded (rough lognormal soil)',
         'incident': 'tapered plane wave (geometry frequency, polarisation, angle), injected every timed step',
-        'l2': 'inputs larger than L2 (fields alone 2.8 GB)',
+        'l2': 'inputs larger than L2 (fields alone %.2f GB, L2 126 MB)' % (
+            6 * g.size_z * g.size_y * g.size_x
+            * (4 if pc.processing_params.datatype == 'float32' else 8) / 1e9),
     }
 
 

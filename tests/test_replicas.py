@@ -77,3 +77,20 @@ def test_rank_that_leaves_early_ends_peer_collective(tmp_path):
     res = run(tmp_path, True)
     assert len(res) == 1 and res[0]['rank'] == 0
     assert res[0]['barrier'].startswith('error')
+
+
+def test_reference_arm_line_on_the_host():
+    """bench.py --impl reference needs no GPU: it times the C restatement
+    on the host cores and prints one line with the contract's keys."""
+    import subprocess
+    out = subprocess.run([sys.executable, os.path.join(ROOT, 'bench.py'), '--impl', 'reference',
+                          '--workload', 'plain_8x8', '--steps', '1', '--warmup', '1'],
+                         capture_output=True, text=True, timeout=600, cwd=ROOT, check=True)
+    line = json.loads(out.stdout.strip().splitlines()[-1])
+    assert line['impl'] == 'reference' and line['metric'] == 'Mcell-updates/s'
+    assert line['value'] > 0 and line['higher_is_better'] is True and line['n_gpus'] == 1
+    assert line['cpu_baseline']['kind'] == 'port' and line['cpu_baseline']['cores'] >= 1
+    assert line['e2e'] == {'value': line['value'], 'unit': 'Mcell-updates/s',
+                           'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}
+    assert line['config']['grid'] == [101, 381, 381]
+    assert '0.35 GB' in line['config']['l2']
