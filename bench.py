@@ -156,7 +156,7 @@ def measured_peak_hbm():
     try:
         with open(path) as fh:
             return float(json.load(fh)['hbm_gbs']), 'measured'
-    except (OSError, KeyError, ValueError):
+    except (OSError, KeyError, ValueError, TypeError):
         return 6650.0, 'fallback'
 
 
