@@ -88,3 +88,21 @@ def test_binding_constants_match_the_header():
                 assert _native.POLARIZATIONS[short[4:]] == value, name
                 checked += 1
     assert checked >= 20 and defines['FDTD_OPT_BATCH_STREAMS'] == _native.OPT_BATCH_STREAMS
+
+
+def test_every_entry_point_rejects_null_handles():
+    """No entry point dereferences a NULL handle or output pointer: each
+    returns FDTD_ERR_INVALID with a message (the destroy calls accept NULL
+    and return FDTD_OK), before any device is touched."""
+    no_handle = {'fdtd_last_error', 'fdtd_version', 'fdtd_device_count', 'fdtd_fused_plan_boxes',
+                 'fdtd_check_cell_division'}
+    for name, argtypes in _native.SIGNATURES.items():
+        if name in no_handle:
+            continue
+        args = [0 if t is _native._I else 0.0 if t is _native._D else None for t in argtypes]
+        rc = getattr(_native.lib, name)(*args)
+        if name.endswith('_destroy'):
+            assert rc == _native.FDTD_OK, name
+        else:
+            assert rc == _native.FDTD_ERR_INVALID, name
+            assert 'null' in _native.last_error(), name
