@@ -15,7 +15,8 @@ from .experiment import get_fdtd_simulator, run_experiment
 from .incidentbeam import IncidentBeam
 from . import materials, near2far, processresults  # noqa: F401
 from .materials import MaterialModel, compute_material_arrays
+from .sweep import run_experiment_batched
 
-__all__ = list(_param_all) + ['get_fdtd_simulator', 'run_experiment', 'IncidentBeam',
-                              'materials', 'near2far', 'processresults', 'MaterialModel',
-                              'compute_material_arrays']
+__all__ = list(_param_all) + ['get_fdtd_simulator', 'run_experiment', 'run_experiment_batched',
+                              'IncidentBeam', 'materials', 'near2far', 'processresults',
+                              'MaterialModel', 'compute_material_arrays']

@@ -88,6 +88,23 @@ class MainSimGpu:
         self._incident_loaded = 'arrays'
         self._inc_phasors = inc_phasors
 
+    def use_incident_run(self, run, phasors) -> bool:
+        """Take the planes of an incident run still on the device (the
+        IncidentSimGpu that IncidentBeam.setup made) device to device; False,
+        with nothing changed, when its grid, element type or device does not
+        fit this simulation. The caller keeps and closes the run."""
+        g = run.native.geom
+        if (g.nx, g.ny, g.dtype) != (self.geom.nx, self.geom.ny, self.geom.dtype) or \
+                g.nt < self.geom.nt_inc:
+            return False
+        try:
+            self.native.set_incident_from(run.native)   # checks the device too
+        except _native.FdtdError:
+            return False   # another device: the caller reads the file
+        self._inc_phasors = {k: np.asarray(v) for k, v in phasors.items()}
+        self._incident_loaded = inc_filename(self.params)
+        return True
+
     def _ensure_incident(self):
         if self._incident_loaded is not None:
             return
@@ -99,17 +116,13 @@ class MainSimGpu:
             # planes device to device instead of reading the file back
             run, phasors = held
             try:
-                g = run.native.geom
-                if (g.nx, g.ny, g.dtype) == (self.geom.nx, self.geom.ny, self.geom.dtype) and \
-                        g.nt >= self.geom.nt_inc:
-                    self.native.set_incident_from(run.native)   # checks the device too
-                    self._inc_phasors = {k: np.asarray(v) for k, v in phasors.items()}
-                    self._incident_loaded = fname
+                if self.use_incident_run(run, phasors):
                     return
-            except _native.FdtdError:
-                pass   # another device: read the file
             finally:
                 run.close()
+        self._load_incident_file(fname)
+
+    def _load_incident_file(self, fname):
         with resultsio.File(fname, 'r') as f:
             comps = [np.asarray(f[c][:], dtype=self.dtype) for c in ('ex', 'ey', 'hx', 'hy')]
             self._inc_phasors = {f'{c}_inc_phasor': np.asarray(f['phasors'][f'{c}_inc_phasor'][:])
