@@ -22,7 +22,10 @@ fixed-length null-padded string, Python int / float int64 / float64.
 
 Writing: raw data goes to the end of the file when a dataset is created;
 the metadata of the whole tree follows it when the file is closed, and the
-superblock is written last. A file opened 'r+' or 'a' is read into the
+superblock is written last. A new file is written as ``<path>.partial`` and
+renamed onto its path when it is closed, so that a file at the path is
+always complete (a process that dies while writing leaves no result file
+for the simulator's skip-if-exists check to mistake for a finished one). A file opened 'r+' or 'a' is read into the
 same tree, new raw data is appended, and on close the tree's metadata is
 written again at the end (the earlier metadata stays in the file, unused).
 
@@ -315,7 +318,7 @@ class Dataset:
         mm = f._maps.get(id(self))
         if mm is None:
             f._fh.flush()
-            mm = np.memmap(f.filename, self.dtype, 'r' if f.mode == 'r' else 'r+',
+            mm = np.memmap(f._disk, self.dtype, 'r' if f.mode == 'r' else 'r+',
                            offset=f._base + self._addr, shape=self.shape or (1,))
             f._maps[id(self)] = mm
         return mm if self.shape else mm.reshape(())
@@ -327,7 +330,7 @@ class Dataset:
         if not self._stored():
             return np.zeros(self.shape, self.dtype)
         f._fh.flush()
-        return np.fromfile(f.filename, self.dtype, self.size,
+        return np.fromfile(f._disk, self.dtype, self.size,
                            offset=f._base + self._addr).reshape(self.shape)
 
     def __getitem__(self, idx):
@@ -560,7 +563,10 @@ class File(Group):
         self._gcols = {}
         self._base = 0
         self._dirty = mode == 'w'
-        self._fh = open(path, {'r': 'rb', 'r+': 'r+b', 'w': 'w+b'}[mode])
+        # a new file is written beside its path and renamed onto it when it is
+        # complete, so that a file at the path is always a whole HDF5 file
+        self._disk = path + '.partial' if mode == 'w' else path
+        self._fh = open(self._disk, {'r': 'rb', 'r+': 'r+b', 'w': 'w+b'}[mode])
         try:
             if mode == 'w':
                 self._fh.write(b'\0' * 96)          # the superblock, written on close
@@ -630,6 +636,7 @@ class File(Group):
     def close(self):
         if self._fh is None:
             return
+        complete = False
         try:
             for mm in self._maps.values():
                 mm.flush()
@@ -637,9 +644,13 @@ class File(Group):
             if self.mode != 'r' and self._dirty:
                 self._write_metadata()
                 self._dirty = False
+            complete = True
         finally:
             self._fh.close()
             self._fh = None
+        if complete and self._disk != self.filename:
+            os.replace(self._disk, self.filename)
+            self._disk = self.filename
 
     def __enter__(self):
         return self

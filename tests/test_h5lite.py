@@ -479,3 +479,28 @@ def test_reads_object_headers_continued_in_another_chunk(tmp_path):
         a = f['parameters'].attrs
         assert [a[f'a{k:02d}'] for k in range(12)] == [float(k) for k in range(12)]
         assert a['polarization'] == 'VV'
+
+
+def test_new_file_appears_only_when_complete(tmp_path):
+    """A file in 'w' mode is written beside its path and renamed onto it on
+    close: while it is being written (or after a writer died) nothing
+    partial sits at the path that skip-if-exists checks."""
+    path = str(tmp_path / 'm.hdf5')
+    f = h5lite.File(path, 'w')
+    ds = f.create_dataset('ex', shape=(4, 5), dtype='f4')
+    ds[1] = 2.0
+    np.testing.assert_array_equal(ds[1], [2.0] * 5)
+    assert not os.path.exists(path) and os.path.exists(path + '.partial')
+    f.close()
+    assert os.path.exists(path) and not os.path.exists(path + '.partial')
+    SpecWalker(path)
+    with h5lite.File(path, 'r') as g:
+        np.testing.assert_array_equal(g['ex'][()][1], [2.0] * 5)
+    # an older file at the path stays readable until the new one replaces it
+    f = h5lite.File(path, 'w')
+    f.create_group('other')
+    with h5lite.File(path, 'r') as g:
+        assert 'ex' in g
+    f.close()
+    with h5lite.File(path, 'r') as g:
+        assert g.keys() == ['other']
