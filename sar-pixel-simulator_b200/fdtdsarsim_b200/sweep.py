@@ -77,12 +77,17 @@ def run_experiment_batched(params: ParameterCollection, materials: Iterable[Mate
 
 def _run_batch(params, models, streams):
     members = []                                  # (model, params, simulator)
+    taken = set()
     try:
         for model in models:
             pc = model_params(params, model)
-            if resultsio.exists(results_filename(pc, model.name)):
-                logger.info('%s already exists, skipping', results_filename(pc, model.name))
+            out = results_filename(pc, model.name)
+            # a result file that exists, or that an earlier model of this
+            # batch will write, is skipped as run_experiment skips it
+            if resultsio.exists(out) or out in taken:
+                logger.info('%s already exists, skipping', out)
                 continue
+            taken.add(out)
             members.append((model, pc, MainSimGpu(pc)))
         if not members:
             return

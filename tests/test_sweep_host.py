@@ -223,3 +223,18 @@ def test_model_params_rejects_extents_set_geom_params_cannot_make(tmp_path):
         sweep.model_params(pc, bad)
     with pytest.raises(ValueError):
         sweep.run_experiment_batched(pc, [], batch_size=0)
+
+
+def test_a_repeated_name_is_skipped_as_run_experiment_skips_it(stand_ins, tmp_path):
+    """Two models of one name in one batch: the first is simulated, the
+    second skipped, as the sequential run_experiment skips a model whose
+    result file an earlier model wrote (gpu/main_sim.py:100-110)."""
+    pc = base(tmp_path)
+    first, again = model(pc, (7, 25, 27), 1, 'same'), model(pc, (7, 25, 27), 9, 'same')
+    sweep.run_experiment_batched(pc, [first, again], batch_size=4)
+    assert StandInBatch.made == [(1, True)]
+    mp = sweep.model_params(pc, first)
+    want = oracle_phasors(mp, first)
+    with resultsio.File(results_filename(mp, 'same'), 'r') as f:
+        assert np.array_equal(f['phasors']['ey_ph_u'][()], want['ey_ph_u'])
+        assert f['material_metadata'].attrs['seed'] == 1
