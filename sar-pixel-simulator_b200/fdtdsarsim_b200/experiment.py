@@ -6,6 +6,7 @@ import queue
 import threading
 from typing import Iterable, Iterator, TypeVar
 
+from .incident import wait_written
 from .incidentbeam import IncidentBeam
 from .materials.materialmodel import MaterialModel
 from .parameters import ParameterCollection, set_geom_params
@@ -112,6 +113,7 @@ def run_experiment(params: ParameterCollection, materials: Iterable[MaterialMode
             _simulate(sim, material)
     process_all_results(params.processing_params.project_dir,
                         params.display_params.debug_plots)
+    wait_written()       # every incident file of this experiment is on disk
 
 
 def _simulate(sim, material: MaterialModel):

@@ -123,6 +123,8 @@ class MainSimGpu:
         self._load_incident_file(fname)
 
     def _load_incident_file(self, fname):
+        from ..incident import wait_written
+        wait_written(fname)                 # a file this process is still writing
         with resultsio.File(fname, 'r') as f:
             comps = [np.asarray(f[c][:], dtype=self.dtype) for c in ('ex', 'ey', 'hx', 'hy')]
             self._inc_phasors = {f'{c}_inc_phasor': np.asarray(f['phasors'][f'{c}_inc_phasor'][:])

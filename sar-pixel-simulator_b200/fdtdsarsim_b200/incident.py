@@ -14,13 +14,15 @@ handed to a main simulation on the device (NativeSim.set_incident_from).
 """
 import copy
 import logging
+import os
+import threading
 
 import numpy as np
 import scipy.constants
 
 from . import _native
 from .absorbers import packed_profiles
-from .parameters import ParameterCollection
+from .parameters import ParameterCollection, inc_filename
 
 logger = logging.getLogger(__name__)
 
@@ -137,20 +139,76 @@ def take_resident(fname: str):
     return _RESIDENT.pop(os.path.abspath(fname), None)
 
 
-def generate_incident_beam(params: ParameterCollection, write: bool = True, device=None):
-    """Make the incident beam of a geometry on the device and, with
-    ``write``, store it as the reference's incident file. Returns
-    (planes, phasors, sim): the recorded planes and incident phasors as host
-    arrays, and the IncidentSimGpu (still holding the planes on the device,
-    for NativeSim.set_incident_from; close it when done)."""
+def make_incident_beam(params: ParameterCollection, device=None):
+    """The incident beam of a geometry made on the device: (planes, phasors,
+    sim), the recorded planes and incident phasors as host arrays and the
+    IncidentSimGpu (still holding the planes on the device, for
+    NativeSim.set_incident_from; close it when done)."""
     from .gpu.main_sim import _device_of
     dev = _device_of(params) if device is None else int(device)
     _, _, pulse_fft, pulse_freqs = create_pulse(params)
     sim = IncidentSimGpu(params, dev)
     sim.make_excitation(pulse_fft, pulse_freqs)
     sim.run()
-    planes, phasors = sim.planes(), sim.phasors()
+    return sim.planes(), sim.phasors(), sim
+
+
+def generate_incident_beam(params: ParameterCollection, write: bool = True, device=None):
+    """make_incident_beam and, with ``write``, the incident file in the
+    reference's layout, written before returning."""
+    planes, phasors, sim = make_incident_beam(params, device)
     if write:
-        from .incidentbeam import write_incident_file
-        write_incident_file(params, planes['ex'], planes['ey'], planes['hx'], planes['hy'], phasors)
+        store_incident_beam(params, planes, phasors)
     return planes, phasors, sim
+
+
+# Incident files being written on a thread: {absolute file name: thread}.
+# Readers in this process wait for the write (wait_written); the threads are
+# not daemons, so the interpreter also waits for them before it exits.
+_WRITES = {}
+
+
+def store_incident_beam(params: ParameterCollection, planes, phasors, background: bool = False):
+    """Write the incident file of a beam (and check it as IncidentBeam.setup
+    checks a new file, incidentbeam.py:57-62); with ``background`` on a
+    thread, so that the device can go on while the file is written."""
+    from .incidentbeam import IncidentBeam, write_incident_file
+    pc = copy.deepcopy(params)
+
+    def write():
+        write_incident_file(pc, planes['ex'], planes['ey'], planes['hx'], planes['hy'], phasors)
+        IncidentBeam(pc).check_file()
+
+    fname = os.path.abspath(inc_filename(pc))
+    wait_written(fname)                  # one writer per file at a time
+    if not background:
+        write()
+        return
+    errors = []
+
+    def run():
+        try:
+            write()
+        except BaseException as exc:   # handed to the thread that waits
+            errors.append(exc)
+
+    t = threading.Thread(target=run, name='incident-file-write')
+    t.errors = errors
+    _WRITES[fname] = t
+    t.start()
+
+
+def wait_written(fname=None):
+    """Wait for the background write of incident file ``fname`` (of every
+    such write when None) and raise the first error one of them met."""
+    keys = [os.path.abspath(fname)] if fname is not None else list(_WRITES)
+    first = None
+    for key in keys:
+        t = _WRITES.pop(key, None)
+        if t is None:
+            continue
+        t.join()
+        if t.errors and first is None:
+            first = t.errors[0]
+    if first is not None:
+        raise first

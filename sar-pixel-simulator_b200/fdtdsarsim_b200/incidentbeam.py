@@ -38,7 +38,10 @@ class IncidentBeam:
         self.processing_params = params.processing_params
 
     def inc_beam_exists(self):
-        return resultsio.exists(inc_filename(self.params))
+        from .incident import wait_written
+        fname = inc_filename(self.params)
+        wait_written(fname)                 # a file this process is still writing
+        return resultsio.exists(fname)
 
     def setup(self):
         """Load the geometry's incident file, or make the beam on the device
@@ -48,12 +51,13 @@ class IncidentBeam:
             self.load_existing()
             return
         logger.info('Generating new incident beam on the device')
-        from .incident import generate_incident_beam, keep_resident
-        _, phasors, sim = generate_incident_beam(self.params)
+        from .incident import keep_resident, make_incident_beam, store_incident_beam
+        planes, phasors, sim = make_incident_beam(self.params)
         # the planes stay on the device for the main simulation of this
-        # geometry (MainSimGpu takes them without reading the file back)
+        # geometry (MainSimGpu takes them without reading the file back);
+        # the file is written, then checked, on a thread meanwhile
         keep_resident(inc_filename(self.params), sim, phasors)
-        self.load_existing()
+        store_incident_beam(self.params, planes, phasors, background=True)
 
     def create_pulse(self):
         """The temporal pulse and its spectrum (incidentbeam.py:174-204):
@@ -78,6 +82,13 @@ class IncidentBeam:
             sim.close()
 
     def load_existing(self):
+        from .incident import wait_written
+        wait_written(inc_filename(self.params))
+        self.check_file()
+
+    def check_file(self):
+        """Shape, dtype and metadata checks of the incident file
+        (incidentbeam.py:74-165)."""
         with resultsio.File(inc_filename(self.params), 'r') as f:
             self.check_array_sizes(f['ex'], f['ey'], f['hx'], f['hy'])
             self.check_metadata(f.attrs)

@@ -22,7 +22,7 @@ import numpy as np
 from . import _native, resultsio
 from .experiment import prefetched
 from .gpu.main_sim import MainSimGpu
-from .incident import take_resident
+from .incident import take_resident, wait_written
 from .incidentbeam import IncidentBeam
 from .materials.materialmodel import MaterialModel
 from .parameters import ParameterCollection, inc_filename, results_filename, set_geom_params
@@ -73,6 +73,7 @@ def run_experiment_batched(params: ParameterCollection, materials: Iterable[Mate
     if pending:
         _run_batch(params, pending, streams)
     process_all_results(params.processing_params.project_dir, params.display_params.debug_plots)
+    wait_written()       # every incident file of this sweep is on disk
 
 
 def _run_batch(params, models, streams):
