@@ -318,6 +318,9 @@ class Dataset:
         mm = f._maps.get(id(self))
         if mm is None:
             f._fh.flush()
+            end = f._base + self._addr + self.nbytes
+            if f.mode == 'r' and os.path.getsize(f._disk) < end:
+                raise OSError(f'truncated HDF5 file: dataset {self.name} ends at byte {end}')
             mm = np.memmap(f._disk, self.dtype, 'r' if f.mode == 'r' else 'r+',
                            offset=f._base + self._addr, shape=self.shape or (1,))
             f._maps[id(self)] = mm
@@ -330,8 +333,11 @@ class Dataset:
         if not self._stored():
             return np.zeros(self.shape, self.dtype)
         f._fh.flush()
-        return np.fromfile(f._disk, self.dtype, self.size,
-                           offset=f._base + self._addr).reshape(self.shape)
+        data = np.fromfile(f._disk, self.dtype, self.size, offset=f._base + self._addr)
+        if data.size != self.size:
+            raise OSError(f'truncated HDF5 file: dataset {self.name} holds {data.size} of '
+                          f'{self.size} elements')
+        return data.reshape(self.shape)
 
     def __getitem__(self, idx):
         self.file._check_open()
