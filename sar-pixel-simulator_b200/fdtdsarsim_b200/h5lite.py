@@ -598,7 +598,7 @@ class File(Group):
         self._fh.seek(self._base + addr)
         data = self._fh.read(n)
         if len(data) != n:
-            raise ValueError(f'truncated HDF5 file: {n} bytes at address {addr}')
+            raise OSError(f'truncated HDF5 file: {n} bytes at address {addr}')
         return data
 
     def _append(self, data):

@@ -103,13 +103,14 @@ def test_truncated_incident_file(tmp_path):
     fname = inc_filename(pc)
     with resultsio.File(fname, 'r') as f:
         cut = f['ex']._addr + f['ex'].nbytes // 2        # inside the first plane set
-    with open(fname, 'r+b') as fh:
-        fh.truncate(cut)
-    with resultsio.File(fname, 'r') as f:
+        with open(fname, 'r+b') as fh:                    # the file shrinks while open
+            fh.truncate(cut)
         with pytest.raises(OSError, match='truncated'):
             np.asarray(f['ex'][:])
         with pytest.raises(OSError, match='truncated'):
             f['ex'][1]
+    with pytest.raises(OSError, match='truncated'):     # its metadata is gone too
+        IncidentBeam(pc).load_existing()
 
 
 def test_simulator_error_ends_the_experiment_and_the_prefetch(monkeypatch, tmp_path):
