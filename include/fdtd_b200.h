@@ -107,6 +107,10 @@ int fdtd_version(void);
 /* Number of visible CUDA devices (0 when none). */
 int fdtd_device_count(int *count);
 
+/* The device's name (as cudaGetDeviceProperties gives it), NUL-terminated
+ * into name[len]; the autotuner's cache key. No reference counterpart. */
+int fdtd_device_name(int device, char *name, int len);
+
 /* Creates a simulation on `device`, allocates all device state and zeroes it.
  * Replaces MainSimGpu.__init__ (gpu/main_sim.py:45-72): context creation,
  * _allocate_cuda_arrays (:512-640) and _clear_cuda_arrays (:691-787). */

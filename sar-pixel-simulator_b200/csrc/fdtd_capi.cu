@@ -399,6 +399,27 @@ int fdtd_device_count(int* count) {
   return FDTD_OK;
 }
 
+int fdtd_device_name(int device, char* name, int len) {
+  if (!name || len < 1) return fail(FDTD_ERR_INVALID, "null name buffer");
+  name[0] = 0;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(FDTD_ERR_CUDA, "no CUDA device available");
+  }
+  if (device < 0 || device >= ndev)
+    return fail(FDTD_ERR_INVALID, "device %d out of range (%d devices)", device, ndev);
+  cudaDeviceProp prop;
+  cudaError_t e = cudaGetDeviceProperties(&prop, device);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(FDTD_ERR_CUDA, "cudaGetDeviceProperties: %s", cudaGetErrorString(e));
+  }
+  strncpy(name, prop.name, (size_t)len - 1);
+  name[len - 1] = 0;
+  return FDTD_OK;
+}
+
 int fdtd_create(const fdtd_geometry* geom, int device, fdtd_sim** out) {
   if (!geom || !out) return fail(FDTD_ERR_INVALID, "null argument");
   *out = nullptr;

@@ -84,6 +84,7 @@ SIGNATURES = {
     'fdtd_last_error': [ctypes.c_char_p, _I],
     'fdtd_version': [],
     'fdtd_device_count': [ctypes.POINTER(_I)],
+    'fdtd_device_name': [_I, ctypes.c_char_p, _I],
     'fdtd_create': [ctypes.POINTER(Geometry), _I, ctypes.POINTER(_P)],
     'fdtd_destroy': [_P],
     'fdtd_set_option': [_P, _I, _I],
@@ -163,6 +164,13 @@ def device_count():
     n = ctypes.c_int(0)
     check(lib.fdtd_device_count(ctypes.byref(n)))
     return n.value
+
+
+def device_name(device=0):
+    """The CUDA device's name (fdtd_device_name)."""
+    buf = ctypes.create_string_buffer(256)
+    check(lib.fdtd_device_name(int(device), buf, len(buf)))
+    return buf.value.decode(errors='replace')
 
 
 def ptr(a: np.ndarray):

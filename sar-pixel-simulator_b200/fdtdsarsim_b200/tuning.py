@@ -44,9 +44,8 @@ def _key(geom, device_name):
 
 def _device_name(device):
     try:
-        import torch
-        return torch.cuda.get_device_name(device)
-    except Exception:   # pragma: no cover - no torch / no device
+        return _native.device_name(device)
+    except _native.FdtdError:   # no device here
         return f'device{device}'
 
 

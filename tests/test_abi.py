@@ -106,3 +106,19 @@ def test_every_entry_point_rejects_null_handles():
         else:
             assert rc == _native.FDTD_ERR_INVALID, name
             assert 'null' in _native.last_error(), name
+
+
+def test_device_name_or_a_clean_error():
+    """fdtd_device_name: the autotuner's cache key; without a device an
+    FDTD_ERR_CUDA, and the autotuner falls back to a placeholder key."""
+    from fdtdsarsim_b200 import tuning
+    if _native.device_count() == 0:
+        with pytest.raises(_native.FdtdError) as ei:
+            _native.device_name(0)
+        assert ei.value.code == _native.FDTD_ERR_CUDA
+        assert tuning._device_name(0) == 'device0'
+    else:
+        assert _native.device_name(0) and tuning._device_name(0) == _native.device_name(0)
+    with pytest.raises(_native.FdtdError) as ei:
+        _native.device_name(-1 if _native.device_count() else 0)
+    assert ei.value.code in (_native.FDTD_ERR_INVALID, _native.FDTD_ERR_CUDA)
