@@ -122,3 +122,17 @@ def test_device_name_or_a_clean_error():
     with pytest.raises(_native.FdtdError) as ei:
         _native.device_name(-1 if _native.device_count() else 0)
     assert ei.value.code in (_native.FDTD_ERR_INVALID, _native.FDTD_ERR_CUDA)
+
+
+def test_the_package_imports_without_torch():
+    """PyTorch belongs to the autograd wrapper only: importing the package
+    and its simulation, sweep, tuning and file modules loads no torch."""
+    import subprocess
+    import sys
+    code = ('import sys; sys.path.insert(0, sys.argv[1]); import fdtdsarsim_b200, '
+            'fdtdsarsim_b200.sweep, fdtdsarsim_b200.tuning, fdtdsarsim_b200.gpu.main_sim, '
+            'fdtdsarsim_b200.incident, fdtdsarsim_b200.h5lite; '
+            'print("torch" in sys.modules)')
+    out = subprocess.run([sys.executable, '-c', code, os.path.join(ROOT, 'sar-pixel-simulator_b200')],
+                         capture_output=True, text=True, check=True, timeout=300)
+    assert out.stdout.strip() == 'False'
