@@ -238,3 +238,19 @@ def test_a_repeated_name_is_skipped_as_run_experiment_skips_it(stand_ins, tmp_pa
     with resultsio.File(results_filename(mp, 'same'), 'r') as f:
         assert np.array_equal(f['phasors']['ey_ph_u'][()], want['ey_ph_u'])
         assert f['material_metadata'].attrs['seed'] == 1
+
+
+@pytest.mark.parametrize('name', ['plain_2x2', 'adjoint_4x4', 'plain_8x8', 'plain_16x16'])
+def test_model_params_gives_the_geometry_the_model_was_made_for(name):
+    """A model made for a configuration's geometry gets exactly that
+    geometry back (every field the result file stores in /parameters)."""
+    import dataclasses
+    pc = synthetic.config_params(name, 'float32')
+    g = pc.geom_params
+    shape = (g.size_z_material, g.size_y, g.size_x)
+    m = MaterialModel(np.ones(shape, np.float32), np.zeros(shape, np.float32), g.cell_size, 'm')
+    blank = synthetic.config_params(name, 'float32')
+    blank.geom_params.size_x = blank.geom_params.size_y = blank.geom_params.size_z = 0
+    got = sweep.model_params(blank, m).geom_params
+    for f in dataclasses.fields(g):
+        assert getattr(got, f.name) == getattr(g, f.name), f.name
