@@ -20,8 +20,7 @@ from typing import Iterable
 import numpy as np
 
 from . import _native, resultsio
-from .experiment import prefetched
-from .gpu.main_sim import MainSimGpu
+from .experiment import get_fdtd_simulator, prefetched
 from .incident import take_resident, wait_written
 from .incidentbeam import IncidentBeam
 from .materials.materialmodel import MaterialModel
@@ -63,20 +62,21 @@ def run_experiment_batched(params: ParameterCollection, materials: Iterable[Mate
     the device runs the current batch."""
     if batch_size < 1:
         raise ValueError('batch_size must be at least 1')
+    sim_class = get_fdtd_simulator(params)          # 'gpu' only, as run_experiment
     source = prefetched(materials, batch_size) if prefetch else iter(materials)
     pending = []
     for model in source:
         pending.append(model)
         if len(pending) == batch_size:
-            _run_batch(params, pending, streams)
+            _run_batch(sim_class, params, pending, streams)
             pending = []
     if pending:
-        _run_batch(params, pending, streams)
+        _run_batch(sim_class, params, pending, streams)
     process_all_results(params.processing_params.project_dir, params.display_params.debug_plots)
     wait_written()       # every incident file of this sweep is on disk
 
 
-def _run_batch(params, models, streams):
+def _run_batch(sim_class, params, models, streams):
     members = []                                  # (model, params, simulator)
     taken = set()
     try:
@@ -89,7 +89,7 @@ def _run_batch(params, models, streams):
                 logger.info('%s already exists, skipping', out)
                 continue
             taken.add(out)
-            members.append((model, pc, MainSimGpu(pc)))
+            members.append((model, pc, sim_class(pc)))
         if not members:
             return
         # materials, and each geometry's incident beam made or loaded once

@@ -130,7 +130,7 @@ class StandInBeam:
 def stand_ins(monkeypatch):
     StandInSim.created, StandInBatch.made, StandInBeam.made = [], [], []
     processed = []
-    monkeypatch.setattr(sweep, 'MainSimGpu', StandInSim)
+    monkeypatch.setattr(sweep, 'get_fdtd_simulator', lambda params: StandInSim)
     monkeypatch.setattr(sweep, 'IncidentBeam', StandInBeam)
     monkeypatch.setattr(_native, 'Batch', StandInBatch)
     monkeypatch.setattr(sweep, 'process_all_results', lambda d, p: processed.append(d))
@@ -223,6 +223,9 @@ def test_model_params_rejects_extents_set_geom_params_cannot_make(tmp_path):
         sweep.model_params(pc, bad)
     with pytest.raises(ValueError):
         sweep.run_experiment_batched(pc, [], batch_size=0)
+    pc.processing_params.processing_type = 'cpu'       # no CPU solver here, as run_experiment
+    with pytest.raises(ValueError):
+        sweep.run_experiment_batched(pc, [])
 
 
 def test_a_repeated_name_is_skipped_as_run_experiment_skips_it(stand_ins, tmp_path):
