@@ -49,3 +49,34 @@ def test_c_program_links_and_calls(tmp_path):
     r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, (r.returncode, r.stdout, r.stderr)
     assert r.stdout.startswith('ok')
+
+
+PRELUDE = r'''
+#include <stddef.h>
+#include "fdtd_b200.h"
+int nx, ny, nz, tfsf_z, nt, nt_inc, size_t_pulse, size_t_inc, i;
+double dx, dt, db, dtm0, dte0dx, theta, phi, radius;
+float *profiles, *ca, *cb, *ex, *ey, *hx, *hy, *ex_ph_u, *all24, *out;
+double *k_vals, *pulse_fft;
+fdtd_geometry g;
+fdtd_sim *sim;                  /* a main simulation of an earlier example */
+'''
+
+
+@pytest.mark.skipif(shutil.which('gcc') is None, reason='no C compiler')
+def test_integration_c_examples_compile_against_the_header(tmp_path):
+    """Every C block of INTEGRATION.md compiles (syntax and types) against
+    include/fdtd_b200.h, so the documented calls keep the header's names and
+    arguments."""
+    import re
+    text = open(os.path.join(ROOT, 'INTEGRATION.md')).read()
+    blocks = re.findall(r'```c\n(.*?)```', text, flags=re.S)
+    assert len(blocks) >= 3
+    for k, block in enumerate(blocks):
+        body = '\n'.join(line for line in block.splitlines() if not line.startswith('#include'))
+        src = tmp_path / f'example{k}.c'
+        src.write_text(PRELUDE + f'void example{k}(void) {{\n{body}\n}}\n')
+        r = subprocess.run(['gcc', '-std=c99', '-fsyntax-only', '-Werror=implicit-function-declaration',
+                            '-Werror=incompatible-pointer-types', '-I', os.path.join(ROOT, 'include'),
+                            str(src)], capture_output=True, text=True)
+        assert r.returncode == 0, (k, r.stderr)
