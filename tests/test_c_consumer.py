@@ -80,3 +80,15 @@ def test_integration_c_examples_compile_against_the_header(tmp_path):
                             '-Werror=incompatible-pointer-types', '-I', os.path.join(ROOT, 'include'),
                             str(src)], capture_output=True, text=True)
         assert r.returncode == 0, (k, r.stderr)
+
+
+def test_integration_python_examples_parse():
+    """INTEGRATION.md's Python blocks are valid Python (each read as the
+    body of a function, since the selector branch returns)."""
+    import re
+    text = open(os.path.join(ROOT, 'INTEGRATION.md')).read()
+    blocks = re.findall(r'```python\n(.*?)```', text, flags=re.S)
+    assert len(blocks) >= 3
+    for k, block in enumerate(blocks):
+        src = 'def _example():\n' + '\n'.join('    ' + line for line in block.splitlines())
+        compile(src, f'INTEGRATION.md python block {k}', 'exec')
