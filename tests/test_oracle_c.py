@@ -59,3 +59,16 @@ def test_c_oracle_reproduces_reference_fixture():
         assert _same(getattr(sim, c), g[f'field_{c}']), c
     for name in sim.ph:
         assert _same(sim.ph[name], g[name]), name
+
+
+def test_float32_against_float64_on_the_2x2_configuration():
+    """The accuracy statement's first row (oracle/fp64_error.py): a full
+    31x39x39 solve (720 steps) in float32 and in float64 -- the precisions
+    the device reproduces bit for bit -- agree on the backscatter power to
+    well inside the 1e-4 bar."""
+    import fp64_error
+    r = fp64_error.run('plain_2x2')
+    assert r['grid'] == [31, 39, 39] and r['size_t'] == 720
+    assert r['backscatter_power_rel_err'] < 1e-5
+    assert r['backscatter_phasor_rel_err'] < 1e-5
+    assert r['upper_plane_max_rel_err'] < 1e-4
