@@ -140,3 +140,12 @@ def test_run_experiment_propagates_a_generator_error(fake_device):
     with pytest.raises(RuntimeError, match='generator failed'):
         experiment.run_experiment(pc, broken())
     assert [c[0] for c in FakeSim.calls] == ['m0', 'm1']
+
+
+def test_run_experiment_with_no_models(fake_device):
+    """No models: no simulator is made when the geometry comes from the
+    models (experiment.py:61-84), and the project is still post-processed."""
+    pc = make_params(27, 25, 23, 14, 10, 5)
+    pc.geom_params.size_x = pc.geom_params.size_y = pc.geom_params.size_z = 0
+    experiment.run_experiment(pc, iter([]))
+    assert FakeSim.calls == [] and fake_device == [pc.processing_params.project_dir]

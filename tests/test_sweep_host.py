@@ -257,3 +257,9 @@ def test_model_params_gives_the_geometry_the_model_was_made_for(name):
     got = sweep.model_params(blank, m).geom_params
     for f in dataclasses.fields(g):
         assert getattr(got, f.name) == getattr(g, f.name), f.name
+
+
+def test_batched_sweep_with_no_models(stand_ins, tmp_path):
+    pc = base(tmp_path)
+    sweep.run_experiment_batched(pc, iter([]))
+    assert StandInSim.created == [] and StandInBatch.made == [] and stand_ins == [str(tmp_path)]
