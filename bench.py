@@ -248,6 +248,26 @@ def job_rate(units, steps, ms, world):
     return world * units * steps / (ms / 1e3) / 1e6
 
 
+def step_launches(choice):
+    """Kernel launches of one step: split H pass, E pass, phasors; fused
+    with the marched shell: interior march, shell march, phasors; fused with
+    the split-pass shell: interior march (and z-slab march), shell H pass,
+    shell E pass, phasors."""
+    from fdtdsarsim_b200 import _native
+    if choice['kernel'] == _native.FDTD_KERNEL_SPLIT:
+        return 3
+    if choice.get('shell', _native.SHELL_MARCH) == _native.SHELL_MARCH:
+        return 3
+    return 4 + int(bool(choice.get('slab', 0)))
+
+
+def shell_name(choice):
+    from fdtdsarsim_b200 import _native
+    if choice['kernel'] == _native.FDTD_KERNEL_SPLIT:
+        return None
+    return 'march' if choice.get('shell', _native.SHELL_MARCH) == _native.SHELL_MARCH else 'split_passes'
+
+
 def run_ours(a):
     import torch
     import torch.distributed as dist
@@ -307,9 +327,7 @@ def run_ours(a):
     ms = t_start.elapsed_time(t_end)
     ms_max = max_over_ranks(ms, world, 'cuda')
     value = job_rate(cells, a.steps, ms_max, world)
-    # split: H pass, E pass, phasors; fused: interior pass (and z-slab pass), shell H pass,
-    # shell E pass, phasors; plus one step-counter advance per run call
-    launches_per_step = 3 if choice['kernel'] == _native.FDTD_KERNEL_SPLIT else 4 + int(bool(choice.get('slab', 0)))
+    launches_per_step = step_launches(choice)
     gpu_launches = launches_per_step * a.steps + 1
 
     # live per-kernel timing for the roofline (separate pass, same state)
@@ -386,9 +404,11 @@ def run_ours(a):
                            kernel=kname, tile=[choice['tile_x'], choice['tile_y']]
                            if choice['kernel'] == _native.FDTD_KERNEL_FUSED else None,
                            zchunk=choice.get('zchunk', 0), z_slabs_fused=bool(choice.get('slab', 0)),
+                           shell=shell_name(choice),
                            autotuned=None if tuned is None else
                            [{'ms': t, 'kernel': 'fused' if c['kernel'] else 'split',
-                             'tile_y': c['tile_y'], 'zchunk': c['zchunk'], 'slab': c.get('slab', 0)}
+                             'tile_y': c['tile_y'], 'zchunk': c['zchunk'], 'slab': c.get('slab', 0),
+                             'shell': shell_name(c)}
                             for t, c in tuned]),
             'roofline': roofline, 'cpu_baseline': base, 'e2e': e2e,
             'gpu_launches': gpu_launches, 'clocks': clk,
@@ -554,8 +574,7 @@ def run_batch(a):
                      'frac': round(achieved / peak, 4), 'traffic': None, 'peak_source': peak_kind,
                      'kernel': 'fused_step (member streams)' if mode == 'streams' else 'batch_split_step'},
         'cpu_baseline': None, 'e2e': None,
-        'gpu_launches': (sum(3 if c['kernel'] == _native.FDTD_KERNEL_SPLIT
-                             else 4 + int(bool(c.get('slab', 0))) for c in choices) * a.steps
+        'gpu_launches': (sum(step_launches(c) for c in choices) * a.steps
                          if mode == 'streams' else 3 * a.steps + 1 + (a.steps + 63) // 64),
         'clocks': clk,
     }

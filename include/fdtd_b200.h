@@ -70,6 +70,15 @@ extern "C" {
                                     own step path on its own stream, side by
                                     side; 0 (default) one launch per pass for
                                     all members */
+#define FDTD_OPT_SHELL        11 /* how the fused step updates the shell around
+                                    its interior box: FDTD_SHELL_* */
+
+/* shell of the fused step (fdtd_set_option(FDTD_OPT_SHELL, ...)) */
+#define FDTD_SHELL_MARCH 0   /* (default) fused z-marches with the CPML faces,
+                                edges and injection in the march, beside the
+                                interior march */
+#define FDTD_SHELL_SPLIT 1   /* the split H pass beside the interior march,
+                                then the split E pass */
 
 /* kernel kinds of fdtd_get_kernel_time */
 #define FDTD_TIME_STEP    0   /* the field-update kernel(s) of a step */
@@ -283,11 +292,14 @@ int fdtd_check_cell_division(int dtype, double cell_size, int device, int64_t *t
 
 /* Diagnostic (no counterpart in the reference): the boxes of the fused
  * step's decomposition of a grid, host computation only (no device use).
- * Rows of 7 ints (kind, x0, x1, y0, y1, z0, z1), kind 0 the interior
- * z-march, 1 the CPML z slabs (with slab = 1, FDTD_OPT_FUSED_SLAB), 2 the
- * shell swept by the split passes; every cell lies in exactly one box. */
+ * mode 0: the shell by the split passes (FDTD_SHELL_SPLIT), 1: the same
+ * with the CPML z slabs marched (FDTD_OPT_FUSED_SLAB), 2: the shell marched
+ * (FDTD_SHELL_MARCH, the default step). Rows of 7 ints (kind, x0, x1, y0,
+ * y1, z0, z1), kind 0 the interior z-march, 1 the CPML z slabs, 2 a shell
+ * box swept by the split passes, 3 a shell box of the general march; every
+ * cell lies in exactly one box. */
 int fdtd_fused_plan_boxes(int nx, int ny, int nz, int npml, int tfsf_z, int tile_y, int zchunk,
-                          int slab, int *out, int cap, int *count);
+                          int mode, int *out, int cap, int *count);
 
 /* fdtd_near2far without any device allocation. This entry point has no
  * counterpart in the reference; it exists for callers that cannot call

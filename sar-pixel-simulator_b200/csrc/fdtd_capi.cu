@@ -101,15 +101,16 @@ struct fdtd_sim {
   int tile_x = 32, tile_y = 8;
   int zchunk = 0;
   int slab = 0;                          // FDTD_OPT_FUSED_SLAB
+  int shell = FDTD_SHELL_MARCH;          // FDTD_OPT_SHELL
   FusedPlan plan;
-  int plan_ok = 0, plan_tile_y = 0, plan_zchunk = 0, plan_slab = 0;
+  int plan_ok = 0, plan_tile_y = 0, plan_zchunk = 0, plan_slab = 0, plan_shell = 0;
   int graph_chunk = 0;
   int check_every = 0;
   // captured step chunks (FDTD_OPT_GRAPH_CHUNK), one per starting field set,
   // with the settings they were captured under; absorber uploads bump the
   // epoch (the profiles are captured by value)
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
-  int gsig[2][8] = {};
+  int gsig[2][9] = {};
   int graph_epoch = 0;
   // gradient (fdtd_grad_*): checkpoints of the forward solve, the segment
   // of recomputed states and the adjoint state; a state is the 6 fields
@@ -262,11 +263,13 @@ int enqueue_steps(fdtd_sim* s, int n, bool phasors = true) {
       if (!fused_supported_tile(s->tile_x, s->tile_y, (int)sizeof(T)))
         return fail(FDTD_ERR_INVALID, "unsupported fused tile %dx%d", s->tile_x, s->tile_y);
       if (!s->plan_ok || s->plan_tile_y != s->tile_y || s->plan_zchunk != s->zchunk ||
-          s->plan_slab != s->slab) {
+          s->plan_slab != s->slab || s->plan_shell != s->shell) {
         const fdtd_geometry& g = s->g;
-        s->plan = make_fused_plan(g.nx, g.ny, g.nz, g.npml, g.tfsf_z, s->tile_y, s->zchunk, s->slab != 0);
+        s->plan = make_fused_plan(g.nx, g.ny, g.nz, g.npml, g.tfsf_z, s->tile_y, s->zchunk, s->slab != 0,
+                                  s->shell == FDTD_SHELL_MARCH);
         s->plan_slab = s->slab;
-        if (s->plan.shell.dropped)
+        s->plan_shell = s->shell;
+        if (s->plan.shell.dropped || s->plan.mshell.dropped)
           return fail(FDTD_ERR_INVALID, "fused plan needs more than %d shell boxes", kMaxShellBoxes);
         s->plan_tile_y = s->tile_y;
         s->plan_zchunk = s->zchunk;
@@ -277,14 +280,23 @@ int enqueue_steps(fdtd_sim* s, int n, bool phasors = true) {
       State<T> st = make_state<T>(s, s->cur, nxt);
       CK(cudaEventRecord(s->fork, s->stream));
       CK(cudaStreamWaitEvent(s->side, s->fork, 0));
-      launch_shell_pass<T>(st, s->tdev, k, s->plan.shell, true, s->side);
-      launch_fused_interior<T>(st, s->plan, s->tile_y, s->stream);
-      launch_fused_slab<T>(st, s->plan, s->tile_y, s->stream);
-      CK(cudaEventRecord(s->join, s->side));
-      CK(cudaStreamWaitEvent(s->stream, s->join, 0));
-      State<T> se = st;
-      se.ihx = (const T*)s->fld[nxt][3]; se.ihy = (const T*)s->fld[nxt][4]; se.ihz = (const T*)s->fld[nxt][5];
-      launch_shell_pass<T>(se, s->tdev, k, s->plan.shell, false, s->stream);
+      if (s->plan.march) {
+        // the shell march and the interior march read the source set only
+        // and write disjoint cells of the destination set
+        launch_march<T>(st, s->tdev, k, s->plan.mshell, s->side);
+        launch_fused_interior<T>(st, s->plan, s->tile_y, s->stream);
+        CK(cudaEventRecord(s->join, s->side));
+        CK(cudaStreamWaitEvent(s->stream, s->join, 0));
+      } else {
+        launch_shell_pass<T>(st, s->tdev, k, s->plan.shell, true, s->side);
+        launch_fused_interior<T>(st, s->plan, s->tile_y, s->stream);
+        launch_fused_slab<T>(st, s->plan, s->tile_y, s->stream);
+        CK(cudaEventRecord(s->join, s->side));
+        CK(cudaStreamWaitEvent(s->stream, s->join, 0));
+        State<T> se = st;
+        se.ihx = (const T*)s->fld[nxt][3]; se.ihy = (const T*)s->fld[nxt][4]; se.ihz = (const T*)s->fld[nxt][5];
+        launch_shell_pass<T>(se, s->tdev, k, s->plan.shell, false, s->stream);
+      }
       s->cur = nxt;
       mark(s, e1);
       State<T> sp = make_state<T>(s, s->cur, s->cur);
@@ -315,7 +327,8 @@ int enqueue_steps(fdtd_sim* s, int n, bool phasors = true) {
 template <class T>
 int enqueue_graph_chunk(fdtd_sim* s, int chunk) {
   const int start = s->cur;
-  const int sig[8] = {chunk, s->kernel, s->tile_x, s->tile_y, s->zchunk, s->phasor_mode, s->graph_epoch, s->slab};
+  const int sig[9] = {chunk,          s->kernel,      s->tile_x,    s->tile_y, s->zchunk,
+                      s->phasor_mode, s->graph_epoch, s->slab, s->shell};
   if (!s->gexec[start] || memcmp(sig, s->gsig[start], sizeof(sig)) != 0) {
     if (s->gexec[start]) {
       cudaGraphExecDestroy(s->gexec[start]);
@@ -603,6 +616,11 @@ int fdtd_set_option(fdtd_sim* s, int option, int value) {
     case FDTD_OPT_FUSED_SLAB:
       s->slab = value ? 1 : 0;
       return FDTD_OK;
+    case FDTD_OPT_SHELL:
+      if (value != FDTD_SHELL_MARCH && value != FDTD_SHELL_SPLIT)
+        return fail(FDTD_ERR_INVALID, "unknown shell mode %d", value);
+      s->shell = value;
+      return FDTD_OK;
     case FDTD_OPT_GRAPH_CHUNK:
       if (value < 0) return fail(FDTD_ERR_INVALID, "bad graph chunk %d", value);
       s->graph_chunk = value;
@@ -627,6 +645,7 @@ int fdtd_get_option(fdtd_sim* s, int option, int* value) {
     case FDTD_OPT_TILE_Y: *value = s->tile_y; return FDTD_OK;
     case FDTD_OPT_ZCHUNK: *value = s->zchunk; return FDTD_OK;
     case FDTD_OPT_FUSED_SLAB: *value = s->slab; return FDTD_OK;
+    case FDTD_OPT_SHELL: *value = s->shell; return FDTD_OK;
     case FDTD_OPT_GRAPH_CHUNK: *value = s->graph_chunk; return FDTD_OK;
     case FDTD_OPT_CHECK_EVERY: *value = s->check_every; return FDTD_OK;
     case FDTD_OPT_TIMING: *value = s->timing; return FDTD_OK;
@@ -1636,13 +1655,15 @@ int fdtd_incident_destroy(fdtd_incident* b) {
   return FDTD_OK;
 }
 
-int fdtd_fused_plan_boxes(int nx, int ny, int nz, int npml, int tfsf_z, int tile_y, int zchunk, int slab,
+int fdtd_fused_plan_boxes(int nx, int ny, int nz, int npml, int tfsf_z, int tile_y, int zchunk, int mode,
                           int* out, int cap, int* count) {
   if (!out || !count || cap < 0) return fail(FDTD_ERR_INVALID, "null argument");
   if (npml < 2 || npml > kMaxPml || nx < 2 * npml + 3 || ny < 2 * npml + 3 || nz < 2 * npml + 3)
     return fail(FDTD_ERR_INVALID, "grid %dx%dx%d too small for npml %d", nz, ny, nx, npml);
-  const FusedPlan p = make_fused_plan(nx, ny, nz, npml, tfsf_z, tile_y, zchunk, slab != 0);
-  if (p.shell.dropped) return fail(FDTD_ERR_INVALID, "plan needs more than %d shell boxes", kMaxShellBoxes);
+  if (mode < 0 || mode > 2) return fail(FDTD_ERR_INVALID, "unknown plan mode %d", mode);
+  const FusedPlan p = make_fused_plan(nx, ny, nz, npml, tfsf_z, tile_y, zchunk, mode == 1, mode == 2);
+  if (p.shell.dropped || p.mshell.dropped)
+    return fail(FDTD_ERR_INVALID, "plan needs more than %d shell boxes", kMaxShellBoxes);
   int n = 0;
   auto put = [&](int kind, int x0, int x1, int y0, int y1, int z0, int z1) {
     if (n < cap) {
@@ -1660,6 +1681,10 @@ int fdtd_fused_plan_boxes(int nx, int ny, int nz, int npml, int tfsf_z, int tile
   for (int k = 0; k < p.shell.n; ++k) {
     const ShellBox& b = p.shell.b[k];
     put(2, b.x0, b.x1, b.y0, b.y1, b.z0, b.z1);
+  }
+  for (int k = 0; k < p.mshell.n; ++k) {
+    const MarchBox& b = p.mshell.b[k];
+    put(3, b.x0, b.x1, b.y0, b.y1, b.z0, b.z1);
   }
   *count = n;
   return n <= cap ? FDTD_OK : fail(FDTD_ERR_INVALID, "%d boxes, room for %d", n, cap);

@@ -123,6 +123,26 @@ struct ShellBoxes {
   ShellBox b[kMaxShellBoxes];
 };
 
+// A box of the fused step's shell marched in z by the general kernel
+// (fdtd_march.cu): [x0, x1) x [y0, y1) x [z0, z1), x0 a multiple of 4. A
+// block is kMarchThreads threads: `width` lanes (width * 4 x cells) by
+// kMarchThreads / width rows, the first row recomputing the row below the
+// tile; gx, gy tiles per plane, z cut into chunks of `zchunk` planes
+// (`nchunks` of them); `first` is the box's first block in the launch.
+constexpr int kMarchThreads = 160;
+struct MarchBox {
+  int x0, x1, y0, y1, z0, z1;
+  int width, gx, gy;
+  int zchunk, nchunks;
+  int first;
+};
+constexpr int kMaxMarchBoxes = 24;
+struct MarchBoxes {
+  int n, total_blocks;
+  int dropped;   // boxes that did not fit (a plan with any is rejected)
+  MarchBox b[kMaxMarchBoxes];
+};
+
 // The interior box of the fused step: no CPML face, domain edge or
 // injection plane touches any of its cells or the halo cells it recomputes.
 // x in [xa, xb) (xa a multiple of 32, xb of 4), y in [ya, yb), and up to

@@ -48,6 +48,9 @@ namespace {
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kLanes = 32;
 constexpr int kRowCells = kLanes * kVec;   // x cells of one tile row
+// z planes per block of the shell march (a box of up to 1.5 times this
+// height is one chunk)
+constexpr int kMarchZChunk = 48;
 
 template <class T, int TY>
 constexpr int interior_min_blocks() { return sizeof(T) == 4 && TY <= 8 ? 2 : 1; }
@@ -334,9 +337,11 @@ bool fused_supported_tile(int tile_x, int tile_y, int elem_bytes) {
 // injection plane tfsf_z (and tfsf_z + 1, whose recomputed plane below would
 // be the injection plane).
 FusedPlan make_fused_plan(int nx, int ny, int nz, int npml, int tfsf_z, int tile_y, int zchunk,
-                          bool use_slab) {
+                          bool use_slab, bool march) {
   FusedPlan p;
   memset(&p, 0, sizeof(p));
+  p.march = march ? 1 : 0;
+  if (march) use_slab = false;
   const int m = npml;
   InteriorBox& ib = p.interior;
   // rows start on a 128-byte line (starting at npml rounded up to 4 cells
@@ -357,7 +362,8 @@ FusedPlan make_fused_plan(int nx, int ny, int nz, int npml, int tfsf_z, int tile
   p.has_interior = m >= 1 && ib.xa < ib.xb && ib.ya < ib.yb && nzr > 0;
   ShellBoxes& bl = p.shell;
   if (!p.has_interior) {
-    add_shell_box(bl, 0, nx, 0, ny, 0, nz);
+    if (march) add_march_box(p.mshell, 0, nx, 0, ny, 0, nz, kMarchZChunk);
+    else add_shell_box(bl, 0, nx, 0, ny, 0, nz);
     return p;
   }
   // with use_slab, the z slabs of the same x-y box (CPML in z only):
@@ -408,17 +414,21 @@ FusedPlan make_fused_plan(int nx, int ny, int nz, int npml, int tfsf_z, int tile
   for (int k = 0; k < nzr; ++k) { cz0[nc] = ib.z0[k]; cz1[nc++] = ib.z1[k]; }
   for (int k = 0; k < sb.nz_ranges; ++k)
     if (sb.z0[k] != 0) { cz0[nc] = sb.z0[k]; cz1[nc++] = sb.z1[k]; }
+  auto add = [&](int x0, int x1, int y0, int y1, int z0, int z1) {
+    if (march) add_march_box(p.mshell, x0, x1, y0, y1, z0, z1, kMarchZChunk);
+    else add_shell_box(bl, x0, x1, y0, y1, z0, z1);
+  };
   int zc = 0;
   for (int k = 0; k < nc; ++k) {
-    add_shell_box(bl, 0, nx, 0, ny, zc, cz0[k]);
+    add(0, nx, 0, ny, zc, cz0[k]);
     zc = cz1[k];
   }
-  add_shell_box(bl, 0, nx, 0, ny, zc, nz);
+  add(0, nx, 0, ny, zc, nz);
   for (int k = 0; k < nc; ++k) {
-    add_shell_box(bl, 0, nx, 0, ib.ya, cz0[k], cz1[k]);
-    add_shell_box(bl, 0, nx, ib.yb, ny, cz0[k], cz1[k]);
-    add_shell_box(bl, 0, ib.xa, ib.ya, ib.yb, cz0[k], cz1[k]);
-    add_shell_box(bl, ib.xb, nx, ib.ya, ib.yb, cz0[k], cz1[k]);
+    add(0, nx, 0, ib.ya, cz0[k], cz1[k]);
+    add(0, nx, ib.yb, ny, cz0[k], cz1[k]);
+    add(0, ib.xa, ib.ya, ib.yb, cz0[k], cz1[k]);
+    add(ib.xb, nx, ib.ya, ib.yb, cz0[k], cz1[k]);
   }
   return p;
 }

@@ -40,13 +40,26 @@ struct FusedPlan {
   InteriorBox interior;
   int has_slab;
   InteriorBox slab;   // the z slabs [0, npml), [nz - npml, nz) of the same x-y box
-  ShellBoxes shell;
+  ShellBoxes shell;   // the shell swept by the split passes (shell mode 1)
+  int march;          // shell mode 0: the shell is marched by k_march
+  MarchBoxes mshell;  // the shell's boxes for k_march (shell mode 0)
 };
 
 // Interior box, z slabs (with use_slab) and shell boxes of a grid; zchunk 0
-// picks the z chunk.
+// picks the z chunk. With march, the shell goes to k_march boxes (mshell)
+// and use_slab is ignored; otherwise to the split passes (shell).
 FusedPlan make_fused_plan(int nx, int ny, int nz, int npml, int tfsf_z, int tile_y, int zchunk,
-                          bool use_slab);
+                          bool use_slab, bool march = false);
+
+// Appends the box [x0, x1) x [y0, y1) x [z0, z1) to a march box list: the
+// row width (32, 16 or 8 lanes) that pads the box least, z chunks of about
+// `zchunk` planes.
+void add_march_box(MarchBoxes& mb, int x0, int x1, int y0, int y1, int z0, int z1, int zchunk);
+
+// Fused step of the march boxes: source set -> destination set, every CPML
+// face, domain edge and injection plane handled in the march.
+template <class T>
+void launch_march(const State<T>& s, const int* tdev, int toff, const MarchBoxes& mb, cudaStream_t st);
 
 // Tile shapes the interior kernel is built for: 32 lanes wide, tile_y rows.
 bool fused_supported_tile(int tile_x, int tile_y, int elem_bytes);

@@ -1,0 +1,217 @@
+// fdtd_march.cu -- the general z-marching fused step: H^{n+1/2} and E^{n+1}
+// of a list of boxes, read from the source field set and written to the
+// destination set, with every CPML face, domain edge and the injection
+// plane handled inside the march.
+//
+// The fused step (fdtd_fused.cu) covers the interior box with a march that
+// has no boundary code at all; this kernel covers everything else (the CPML
+// z slabs, the x and y strips, the injection planes) in the same one-pass
+// form, so the shell no longer needs the split H pass and E pass (80 B per
+// cell-update plus psi, and an E pass that has to wait for the interior).
+// Both marches read only the source set and write only the destination set,
+// so they run side by side.
+//
+// A block is kMarchThreads threads: `width` lanes of 4 x cells by
+// kMarchThreads / width rows (width 32, 16 or 8 per box, whichever pads the
+// box least: 8-lane rows keep the narrow x strips dense). It marches up a
+// chunk of z planes. At plane z a thread holds E(z) of its vector (carried
+// from the previous plane), loads E(z+1) and H(z), and
+//   1. computes H^{n+1/2}(z) with the complete per-vector update (h_vec:
+//      main update inside its index ranges, z, x and y CPML faces,
+//      E-field injection); the +x neighbour comes by shuffle from the next
+//      lane, the +y neighbour through shared memory from the next row;
+//   2. computes E^{n+1}(z) (e_vec: main update, CPML faces, H-field
+//      injection); the -x neighbour by shuffle, the -y neighbour through
+//      shared memory, the -z neighbour is H^{n+1/2}(z-1) carried from the
+//      previous plane.
+// The first row recomputes H of the row below the tile, lane 0 of every row
+// recomputes H at the cell left of its vector (h_cell, any position), and a
+// chunk starts by recomputing the plane below it; recomputed values are
+// never stored, and psi is written only for the block's own cells. Warps
+// whose vectors are all plain interior vectors take the plain update.
+// Per-cell values equal the split passes' bit for bit: the same update
+// functions in the same order of operations, fed the same neighbours.
+#include <algorithm>
+#include <cstring>
+
+#include "fdtd_launch.h"
+#include "fdtd_vec.cuh"
+
+namespace fdtd {
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+// Resident blocks per SM the march asks for (registers per thread <=
+// 65536 / (160 * n)).
+template <class T>
+constexpr int march_min_blocks() { return sizeof(T) == 4 ? 3 : 1; }
+
+__device__ __forceinline__ const MarchBox& find_march_box(const MarchBoxes& mb, int bid) {
+  int k = 0;
+  while (k + 1 < mb.n && bid >= mb.b[k + 1].first) ++k;
+  return mb.b[k];
+}
+
+template <class T>
+__global__ void __launch_bounds__(kMarchThreads, march_min_blocks<T>())
+k_march(const __grid_constant__ State<T> s, const int* __restrict__ tp, int toff,
+        const __grid_constant__ MarchBoxes mb) {
+  // E(z) of every row (read by the row below as its +y neighbour) and
+  // H^{n+1/2}(z) (read by the row above as its -y neighbour), indexed
+  // [(row * width + lane) * 4 + j]
+  __shared__ __align__(32) T sEx[kMarchThreads * kVec];
+  __shared__ __align__(32) T sEz[kMarchThreads * kVec];
+  __shared__ __align__(32) T sHx[kMarchThreads * kVec];
+  __shared__ __align__(32) T sHz[kMarchThreads * kVec];
+
+  const MarchBox& b = find_march_box(mb, blockIdx.x);
+  const int width = b.width, rows = kMarchThreads / width;
+  int local = blockIdx.x - b.first;
+  const int bx = local % b.gx;
+  local /= b.gx;
+  const int by = local % b.gy;
+  const int c = local / b.gy;
+  const int lane = threadIdx.x % width, r = threadIdx.x / width;
+  const int x0 = b.x0 + (bx * width + lane) * kVec;
+  const int y = b.y0 + by * (rows - 1) + r - 1;   // row 0 is the row below the tile
+  const int z0 = b.z0 + c * b.zchunk;
+  const int z1 = min(b.z1, z0 + b.zchunk);
+  const int zs = max(z0 - 1, 0);                  // the plane below the chunk, if any
+  const int t = *tp + toff;
+  const int ny = s.ny, nz = s.nz;
+  // Rows outside the grid and lanes past the pitch only feed the shared
+  // memory exchange and the shuffles (as zeros).
+  const bool vin = x0 < s.pitch && y >= 0 && y < ny;
+  const bool own = vin && r >= 1 && y < b.y1 && x0 < b.x1;
+  const long long P = s.plane, W = s.pitch;
+  long long i = (long long)zs * P + (vin ? (long long)y * W + x0 : 0);
+  const int so = threadIdx.x * kVec;
+  const int su = so + width * kVec;   // the next row's slot
+  const int sd = so - width * kVec;   // the previous row's slot
+
+  EVec<T> e;
+  HVec<T> h;
+  T ezz[kVec];   // Ez(z+1)
+  if (vin) { ld4(e.ex, s.iex + i); ld4(e.ey, s.iey + i); ld4(e.ez, s.iez + i); }
+  else { zero4(e.ex); zero4(e.ey); zero4(e.ez); }
+  zero4(h.hxz); zero4(h.hyz);
+
+  for (int z = zs; z < z1; ++z, i += P) {
+    const bool work = own && z >= z0;   // this thread updates and stores plane z
+    const bool up = z + 1 < nz;
+    // ---- loads of plane z
+    if (vin && up) { ld4(e.exz, s.iex + i + P); ld4(e.eyz, s.iey + i + P); ld4(ezz, s.iez + i + P); }
+    else { zero4(e.exz); zero4(e.eyz); zero4(ezz); }
+    if (vin) { ld4(h.hx, s.ihx + i); ld4(h.hy, s.ihy + i); ld4(h.hz, s.ihz + i); }
+    else { zero4(h.hx); zero4(h.hy); zero4(h.hz); }
+    T ca[kVec], cb[kVec];
+    if (work) { ld4(ca, s.ca + i); ld4(cb, s.cb + i); }
+    else { zero4(ca); zero4(cb); }
+    if (r == rows - 1) {   // +y neighbour of the top row lies in the next tile
+      if (vin && y + 1 < ny) { ld4(e.exy, s.iex + i + W); ld4(e.ezy, s.iez + i + W); }
+      else { zero4(e.exy); zero4(e.ezy); }
+    }
+    T eyr = T(0), ezr = T(0);   // +x neighbour of the last lane lies in the next tile
+    if (lane == width - 1 && vin && x0 + kVec < s.pitch) { eyr = s.iey[i + kVec]; ezr = s.iez[i + kVec]; }
+    // lane 0: the source values H^{n+1/2} at (z, y, x0 - 1) needs
+    ENbr<T> g;
+    T ghy = T(0), ghz = T(0);
+    const bool left = work && lane == 0 && x0 >= 1;
+    if (left) {
+      const long long j = i - 1;
+      g.ex0 = s.iex[j]; g.ey0 = s.iey[j]; g.ez0 = s.iez[j];
+      g.exz = up ? s.iex[j + P] : T(0);
+      g.eyz = up ? s.iey[j + P] : T(0);
+      g.exy = y + 1 < ny ? s.iex[j + W] : T(0);
+      g.ezy = y + 1 < ny ? s.iez[j + W] : T(0);
+      ghy = s.ihy[j]; ghz = s.ihz[j];
+    }
+    // ---- H^{n+1/2}(z) -----------------------------------------------------
+    st4(&sEx[so], e.ex);
+    st4(&sEz[so], e.ez);
+    __syncthreads();
+    if (r < rows - 1) { ld4(e.exy, &sEx[su]); ld4(e.ezy, &sEz[su]); }
+    e.eyn = __shfl_down_sync(kFull, e.ey[0], 1, width);
+    e.ezn = __shfl_down_sync(kFull, e.ez[0], 1, width);
+    if (lane == width - 1) { e.eyn = eyr; e.ezn = ezr; }
+    // plain_h: every vector of the warp is a plain interior vector (for H
+    // and for E)
+    const bool plain_h = __all_sync(kFull, !vin || interior(s, z, y, x0, t));
+    if (vin) {
+      if (plain_h) h_vec_interior(s, e, h.hx, h.hy, h.hz);
+      else h_vec(s, e, z, y, x0, t, work, h.hx, h.hy, h.hz);
+    }
+    st4(&sHx[so], h.hx);
+    st4(&sHz[so], h.hz);
+    __syncthreads();
+    // ---- E^{n+1}(z) ---------------------------------------------------------
+    h.hyp = __shfl_up_sync(kFull, h.hy[kVec - 1], 1, width);
+    h.hzp = __shfl_up_sync(kFull, h.hz[kVec - 1], 1, width);
+    if (lane == 0) {   // H^{n+1/2} left of the vector (any position)
+      T hxl = T(0), hyl = ghy, hzl = ghz;
+      if (left) {
+        g.eyx = e.ey[0];
+        g.ezx = e.ez[0];
+        h_cell(s, g, z, y, x0 - 1, t, false, hxl, hyl, hzl);
+      }
+      h.hyp = hyl;
+      h.hzp = hzl;
+    }
+    if (work) {
+      ld4(h.hxy, &sHx[sd]);
+      ld4(h.hzy, &sHz[sd]);
+      if (plain_h) e_vec_interior(h, ca, cb, e.ex, e.ey, e.ez);
+      else e_vec(s, h, ca, cb, z, y, x0, t, true, e.ex, e.ey, e.ez);
+      st4(s.ohx + i, h.hx); st4(s.ohy + i, h.hy); st4(s.ohz + i, h.hz);
+      st4(s.oex + i, e.ex); st4(s.oey + i, e.ey); st4(s.oez + i, e.ez);
+    }
+    // ---- next plane: E(z+1) becomes E(z), H^{n+1/2}(z) becomes H(z-1) -----
+    copy4(e.ex, e.exz); copy4(e.ey, e.eyz); copy4(e.ez, ezz);
+    copy4(h.hxz, h.hx); copy4(h.hyz, h.hy);
+  }
+}
+
+}  // namespace
+
+void add_march_box(MarchBoxes& mb, int x0, int x1, int y0, int y1, int z0, int z1, int zchunk) {
+  if (x0 >= x1 || y0 >= y1 || z0 >= z1) return;
+  if (mb.n >= kMaxMarchBoxes) {
+    ++mb.dropped;
+    return;
+  }
+  MarchBox& b = mb.b[mb.n++];
+  b.x0 = x0; b.x1 = x1; b.y0 = y0; b.y1 = y1; b.z0 = z0; b.z1 = z1;
+  // row width with the least padded area (ties: the wider rows)
+  long long best = -1;
+  for (int w : {32, 16, 8}) {
+    const int ty = kMarchThreads / w - 1;
+    const long long gx = (x1 - x0 + 4 * w - 1) / (4 * w), gy = (y1 - y0 + ty - 1) / ty;
+    const long long padded = gx * 4 * w * gy * ty;
+    if (best < 0 || padded < best) { best = padded; b.width = w; }
+  }
+  const int ty = kMarchThreads / b.width - 1;
+  b.gx = (x1 - x0 + b.width * kVec - 1) / (b.width * kVec);
+  b.gy = (y1 - y0 + ty - 1) / ty;
+  // chunks of about zchunk planes, evenly cut (each recomputes the plane
+  // below it)
+  const int len = z1 - z0;
+  const int zc = std::max(zchunk, 1);
+  b.nchunks = std::max(1, (len + zc - 1) / zc);
+  b.zchunk = (len + b.nchunks - 1) / b.nchunks;
+  b.nchunks = (len + b.zchunk - 1) / b.zchunk;
+  b.first = mb.total_blocks;
+  mb.total_blocks += b.gx * b.gy * b.nchunks;
+}
+
+template <class T>
+void launch_march(const State<T>& s, const int* tdev, int toff, const MarchBoxes& mb, cudaStream_t st) {
+  if (mb.n == 0 || mb.total_blocks == 0) return;
+  k_march<T><<<mb.total_blocks, kMarchThreads, 0, st>>>(s, tdev, toff, mb);
+}
+
+template void launch_march<float>(const State<float>&, const int*, int, const MarchBoxes&, cudaStream_t);
+template void launch_march<double>(const State<double>&, const int*, int, const MarchBoxes&, cudaStream_t);
+
+}  // namespace fdtd

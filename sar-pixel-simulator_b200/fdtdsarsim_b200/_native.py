@@ -38,6 +38,9 @@ OPT_TIMING = 7
 OPT_ZCHUNK = 8
 OPT_FUSED_SLAB = 9
 OPT_BATCH_STREAMS = 10
+OPT_SHELL = 11
+SHELL_MARCH = 0
+SHELL_SPLIT = 1
 
 TIME_STEP = 0
 TIME_PHASOR = 1
@@ -479,13 +482,17 @@ def check_cell_division(dtype, cell_size, device=0):
     return tested.value, bad.value
 
 
-def fused_plan_boxes(nx, ny, nz, npml, tfsf_z, tile_y=4, zchunk=0, slab=False):
+def fused_plan_boxes(nx, ny, nz, npml, tfsf_z, tile_y=4, zchunk=0, slab=False, march=False):
     """(kind, x0, x1, y0, y1, z0, z1) rows of the fused step's boxes
-    (fdtd_fused_plan_boxes; host computation, no device needed)."""
+    (fdtd_fused_plan_boxes; host computation, no device needed): kind 0
+    interior march, 1 CPML z slab march, 2 split-pass shell box, 3 general
+    march shell box. ``march`` gives the default step's plan (shell marched);
+    otherwise the split-pass shell, with ``slab`` the z slabs marched."""
     out = np.zeros((64, 7), np.int32)
     n = ctypes.c_int(0)
+    mode = 2 if march else int(bool(slab))
     check(lib.fdtd_fused_plan_boxes(int(nx), int(ny), int(nz), int(npml), int(tfsf_z), int(tile_y),
-                                    int(zchunk), int(bool(slab)), ptr(out), out.shape[0], ctypes.byref(n)))
+                                    int(zchunk), mode, ptr(out), out.shape[0], ctypes.byref(n)))
     return out[:n.value].copy()
 
 

@@ -18,17 +18,23 @@ from . import _native
 
 DEFAULT_TILE = (32, 4)
 
-# (kernel, tile_y, zchunk, slab); zchunk 0 lets the library pick; slab 1
-# marches the CPML z slabs with the fused step too
+_MARCH, _SPLIT = _native.SHELL_MARCH, _native.SHELL_SPLIT
+
+# (kernel, tile_y, zchunk, slab, shell); zchunk 0 lets the library pick;
+# shell: the fused step's shell marched (_MARCH) or swept by the split
+# passes (_SPLIT), then slab 1 marches the CPML z slabs
 CANDIDATES = [
-    (_native.FDTD_KERNEL_SPLIT, 4, 0, 0),
-    (_native.FDTD_KERNEL_FUSED, 4, 0, 0),
-    (_native.FDTD_KERNEL_FUSED, 4, 26, 0),
-    (_native.FDTD_KERNEL_FUSED, 7, 0, 0),
-    (_native.FDTD_KERNEL_FUSED, 8, 0, 0),
-    (_native.FDTD_KERNEL_FUSED, 4, 0, 1),
-    (_native.FDTD_KERNEL_FUSED, 7, 0, 1),
+    (_native.FDTD_KERNEL_SPLIT, 4, 0, 0, _MARCH),
+    (_native.FDTD_KERNEL_FUSED, 4, 0, 0, _MARCH),
+    (_native.FDTD_KERNEL_FUSED, 4, 26, 0, _MARCH),
+    (_native.FDTD_KERNEL_FUSED, 8, 0, 0, _MARCH),
+    (_native.FDTD_KERNEL_FUSED, 4, 0, 0, _SPLIT),
+    (_native.FDTD_KERNEL_FUSED, 8, 0, 0, _SPLIT),
+    (_native.FDTD_KERNEL_FUSED, 4, 0, 1, _SPLIT),
 ]
+
+# cache entries measured with another candidate set are measured again
+_VERSION = 'v2'
 
 
 def cache_path():
@@ -39,7 +45,7 @@ def cache_path():
 
 def _key(geom, device_name):
     dt = 'f32' if geom.dtype == _native.FDTD_F32 else 'f64'
-    return f'{device_name}|{geom.nx}x{geom.ny}x{geom.nz}|npml{geom.npml}|{dt}'
+    return f'{device_name}|{geom.nx}x{geom.ny}x{geom.nz}|npml{geom.npml}|{dt}|{_VERSION}'
 
 
 def _device_name(device):
@@ -62,15 +68,16 @@ def lookup(geom, device=0):
 
 
 def choose(geom, kernel=None, tile=None, device=0, use_cache=True):
-    """{'kernel', 'tile_x', 'tile_y', 'zchunk', 'slab'} for a geometry."""
+    """{'kernel', 'tile_x', 'tile_y', 'zchunk', 'slab', 'shell'} for a geometry."""
     if kernel is None and tile is None and use_cache:
         hit = lookup(geom, device)
         if hit:
             return {'kernel': int(hit['kernel']), 'tile_x': 32, 'tile_y': int(hit['tile_y']),
-                    'zchunk': int(hit['zchunk']), 'slab': int(hit.get('slab', 0))}
+                    'zchunk': int(hit['zchunk']), 'slab': int(hit.get('slab', 0)),
+                    'shell': int(hit.get('shell', _MARCH))}
     k = _native.FDTD_KERNEL_FUSED if kernel is None else int(kernel)
     tx, ty = tile if tile is not None else DEFAULT_TILE
-    return {'kernel': k, 'tile_x': int(tx), 'tile_y': int(ty), 'zchunk': 0, 'slab': 0}
+    return {'kernel': k, 'tile_x': int(tx), 'tile_y': int(ty), 'zchunk': 0, 'slab': 0, 'shell': _MARCH}
 
 
 def apply(sim, choice):
@@ -81,6 +88,7 @@ def apply(sim, choice):
         sim.set_option(_native.OPT_TILE_Y, choice['tile_y'])
         sim.set_option(_native.OPT_ZCHUNK, choice.get('zchunk', 0))
         sim.set_option(_native.OPT_FUSED_SLAB, choice.get('slab', 0))
+        sim.set_option(_native.OPT_SHELL, choice.get('shell', _MARCH))
 
 
 def autotune(geom, device=0, steps=6, candidates=None, save=True):
@@ -103,8 +111,11 @@ def autotune(geom, device=0, steps=6, candidates=None, save=True):
     cb = np.full((g.nz, g.ny, g.nx), g.dte0dx, ft)
     sim.set_materials(ca, cb)
     timings = []
-    for kernel, ty, zc, slab in (candidates or CANDIDATES):
-        choice = {'kernel': kernel, 'tile_x': 32, 'tile_y': ty, 'zchunk': zc, 'slab': slab}
+    for cand in (candidates or CANDIDATES):
+        kernel, ty, zc, slab = cand[:4]
+        shell = cand[4] if len(cand) > 4 else _MARCH
+        choice = {'kernel': kernel, 'tile_x': 32, 'tile_y': ty, 'zchunk': zc, 'slab': slab,
+                  'shell': shell}
         try:
             apply(sim, choice)
             sim.reset()

@@ -1,11 +1,12 @@
 """Generate the golden fixtures in this folder by running the reference
 package ``fdtdsarsim`` (wyatt-sfu/sar-pixel-simulator) on its CPU path.
 
-The reference is imported from ``/root/reference`` with the in-memory
+The reference is imported from its checkout (``--reference PATH`` or the
+``FDTDSARSIM_REFERENCE`` environment variable) with the in-memory
 ``h5py``/``matplotlib`` stand-ins of ``_refshims.py``; nothing of it is
 copied. Run once, in a container that has the reference checked out:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py --reference PATH [geom abs mat main n2f pipe inc matgen]
 
 Outputs (all small, committed):
   geom_cases.json      set_geom_params results (parameters.py:242-305)
@@ -31,7 +32,18 @@ import tempfile
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = '/root/reference'
+# the reference checkout (fdtdsarsim), from --reference PATH or the
+# FDTDSARSIM_REFERENCE environment variable
+REF = None
+for _k, _a in enumerate(sys.argv[1:]):
+    if _a.startswith('--reference='):
+        REF = _a.split('=', 1)[1]
+    elif _a == '--reference' and _k + 2 < len(sys.argv):
+        REF = sys.argv[_k + 2]
+REF = REF or os.environ.get('FDTDSARSIM_REFERENCE')
+if not REF or not os.path.isdir(os.path.join(REF, 'fdtdsarsim')):
+    sys.exit('make_golden.py: pass --reference PATH (or set FDTDSARSIM_REFERENCE) to the '
+             'fdtdsarsim checkout')
 
 sys.path.insert(0, HERE)
 import _refshims  # noqa: E402
@@ -426,7 +438,9 @@ def gen_material_generators():
 
 
 if __name__ == '__main__':
-    which = sys.argv[1:] or ['geom', 'abs', 'mat', 'main', 'n2f', 'pipe', 'inc', 'matgen']
+    args = [a for k, a in enumerate(sys.argv[1:])
+            if not a.startswith('--reference') and not (k > 0 and sys.argv[k] == '--reference')]
+    which = args or ['geom', 'abs', 'mat', 'main', 'n2f', 'pipe', 'inc', 'matgen']
     if 'geom' in which:
         gen_geom()
     if 'abs' in which:

@@ -61,16 +61,23 @@ def oracle_for(pc):
                        pc.processing_params.datatype, cpml_profiles(pc))
 
 
-def native_for(pc, kernel=_native.FDTD_KERNEL_SPLIT, tile=(32, 8), phasor_mode=0, zchunk=0, slab=False):
+def native_for(pc, kernel=_native.FDTD_KERNEL_SPLIT, tile=(32, 8), phasor_mode=0, zchunk=0, slab=False,
+               shell=None):
+    """A NativeSim for pc with the given step path. The fused step's shell
+    is marched (SHELL_MARCH) unless ``shell`` says otherwise; ``slab`` (the
+    z slabs marched beside split-pass strips) implies the split-pass shell."""
     from fdtdsarsim_b200.gpu.main_sim import native_geometry
     sim = _native.NativeSim(native_geometry(pc), 0)
     sim.set_absorbers(packed_profiles(pc))
     sim.set_option(_native.OPT_KERNEL, kernel)
     if kernel == _native.FDTD_KERNEL_FUSED:
+        if shell is None:
+            shell = _native.SHELL_SPLIT if slab else _native.SHELL_MARCH
         sim.set_option(_native.OPT_TILE_X, tile[0])
         sim.set_option(_native.OPT_TILE_Y, tile[1])
         sim.set_option(_native.OPT_ZCHUNK, zchunk)
         sim.set_option(_native.OPT_FUSED_SLAB, int(slab))
+        sim.set_option(_native.OPT_SHELL, shell)
     sim.set_option(_native.OPT_PHASOR_MODE, phasor_mode)
     return sim
 

@@ -63,32 +63,35 @@ fdtd_sim *sim;                  /* a main simulation of an earlier example */
 '''
 
 
+EXAMPLES = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'examples')
+
+
 @pytest.mark.skipif(shutil.which('gcc') is None, reason='no C compiler')
-def test_integration_c_examples_compile_against_the_header(tmp_path):
-    """Every C block of INTEGRATION.md compiles (syntax and types) against
-    include/fdtd_b200.h, so the documented calls keep the header's names and
-    arguments."""
-    import re
-    text = open(os.path.join(ROOT, 'INTEGRATION.md')).read()
-    blocks = re.findall(r'```c\n(.*?)```', text, flags=re.S)
-    assert len(blocks) >= 3
-    for k, block in enumerate(blocks):
+def test_c_call_examples_compile_against_the_header(tmp_path):
+    """The C call sequences of tests/examples (those a reference-side
+    integration makes) compile, syntax and types, against
+    include/fdtd_b200.h, so they keep the header's names and arguments."""
+    import glob
+    files = sorted(glob.glob(os.path.join(EXAMPLES, '*.c')))
+    assert len(files) >= 3
+    for k, path in enumerate(files):
+        block = open(path).read()
         body = '\n'.join(line for line in block.splitlines() if not line.startswith('#include'))
         src = tmp_path / f'example{k}.c'
         src.write_text(PRELUDE + f'void example{k}(void) {{\n{body}\n}}\n')
         r = subprocess.run(['gcc', '-std=c99', '-fsyntax-only', '-Werror=implicit-function-declaration',
                             '-Werror=incompatible-pointer-types', '-I', os.path.join(ROOT, 'include'),
                             str(src)], capture_output=True, text=True)
-        assert r.returncode == 0, (k, r.stderr)
+        assert r.returncode == 0, (path, r.stderr)
 
 
-def test_integration_python_examples_parse():
-    """INTEGRATION.md's Python blocks are valid Python (each read as the
-    body of a function, since the selector branch returns)."""
-    import re
-    text = open(os.path.join(ROOT, 'INTEGRATION.md')).read()
-    blocks = re.findall(r'```python\n(.*?)```', text, flags=re.S)
-    assert len(blocks) >= 3
-    for k, block in enumerate(blocks):
+def test_python_call_examples_parse():
+    """The Python call sequences of tests/examples are valid Python (each
+    read as the body of a function, since the selector branch returns)."""
+    import glob
+    files = sorted(glob.glob(os.path.join(EXAMPLES, '*.py')))
+    assert len(files) >= 3
+    for path in files:
+        block = open(path).read()
         src = 'def _example():\n' + '\n'.join('    ' + line for line in block.splitlines())
-        compile(src, f'INTEGRATION.md python block {k}', 'exec')
+        compile(src, path, 'exec')

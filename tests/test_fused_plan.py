@@ -17,12 +17,19 @@ GRIDS = [
 ]
 
 
-@pytest.mark.parametrize('slab', [False, True], ids=['shell', 'slab'])
+@pytest.mark.parametrize('mode', ['shell', 'slab', 'march'])
 @pytest.mark.parametrize('tile_y', [4, 8])
 @pytest.mark.parametrize('grid', GRIDS)
-def test_boxes_partition_the_grid(grid, tile_y, slab):
+def test_boxes_partition_the_grid(grid, tile_y, mode):
     nx, ny, nz, m, tfsf = grid
-    boxes = _native.fused_plan_boxes(nx, ny, nz, m, tfsf, tile_y, slab=slab)
+    boxes = _native.fused_plan_boxes(nx, ny, nz, m, tfsf, tile_y, slab=mode == 'slab',
+                                     march=mode == 'march')
+    # the march plan sends the whole shell to the general march, the others
+    # to the split passes
+    shell_kind = 3 if mode == 'march' else 2
+    assert set(boxes[:, 0]) <= {0, 1, shell_kind}
+    if mode != 'slab':
+        assert 1 not in boxes[:, 0]
     count = np.zeros((nz, ny, nx), np.int32)
     for kind, x0, x1, y0, y1, z0, z1 in boxes:
         assert x0 % 4 == 0

@@ -38,17 +38,20 @@ WIDE = [
     # upper CPML slab (nz - npml - 1): neither box may march through it
     (41, 37, 29, 9, 20, 15, 'float32'),
     (41, 37, 29, 18, 20, 15, 'float32'),
+    # tall grid: the shell march cuts its x and y strips into several z
+    # chunks (each recomputing the plane below it)
+    (140, 45, 200, 100, 10, 8, 'float32'),
 ]
 
 
-def _run_both(case, seed, kernel=SPLIT, tile=(32, 8), phasor_mode=0, steps=None, zchunk=0):
+def _run_both(case, seed, kernel=SPLIT, tile=(32, 8), phasor_mode=0, steps=None, zchunk=0, shell=None):
     nx, ny, nz, tfsf, nt, ntp, dtype = case
     pc = make_params(nx, ny, nz, tfsf, nt, ntp, dtype=dtype)
     _, _, ca, cb, inc = random_problem(pc, seed)
     orc = oracle_for(pc)
     steps = nt if steps is None else steps
     orc.run(ca, cb, inc, steps)
-    sim = native_for(pc, kernel, tile, phasor_mode, zchunk)
+    sim = native_for(pc, kernel, tile, phasor_mode, zchunk, shell=shell)
     sim.set_materials(ca, cb)
     sim.set_incident(inc['ex'], inc['ey'], inc['hx'], inc['hy'])
     sim.run(steps)
@@ -73,11 +76,27 @@ def _assert_matches(orc, sim):
         assert bits_equal(sim.get_phasor(k), orc.ph[name]), name
 
 
+@pytest.mark.parametrize('shell', [_native.SHELL_MARCH, _native.SHELL_SPLIT], ids=['march', 'split'])
 @pytest.mark.parametrize('case', CASES + WIDE)
-def test_fused_matches_oracle_bit_exact(case):
-    orc, sim = _run_both(case, seed=202, kernel=FUSED)
+def test_fused_matches_oracle_bit_exact(case, shell):
+    """The fused step with its shell marched (the default: CPML faces,
+    domain edges and the injection plane inside a z-march beside the
+    interior march) or swept by the split passes."""
+    orc, sim = _run_both(case, seed=202, kernel=FUSED, shell=shell)
     _assert_matches(orc, sim)
     sim.close()
+
+
+@pytest.mark.parametrize('tile_y', [4, 8])
+def test_march_shell_tiles(tile_y):
+    """The shell march beside interior tiles of other heights, and a grid
+    whose interior is narrower than one 128-cell row (8- and 16-lane rows
+    in the strips and slabs)."""
+    for case in (WIDE[0], (67, 91, 43, 30, 16, 12, 'float32')):
+        orc, sim = _run_both(case, seed=404 + tile_y, kernel=FUSED, tile=(32, tile_y),
+                             shell=_native.SHELL_MARCH)
+        _assert_matches(orc, sim)
+        sim.close()
 
 
 @pytest.mark.parametrize('case', CASES + WIDE)

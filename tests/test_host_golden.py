@@ -165,9 +165,9 @@ def test_tuning_cache_choose_and_apply(tmp_path, monkeypatch):
     assert tuning.choose(geom, device=0)['kernel'] == _native.FDTD_KERNEL_FUSED
     key = tuning._key(geom, tuning._device_name(0))
     (tmp_path / 'tune.json').write_text(json.dumps({key: {'kernel': 1, 'tile_y': 7, 'zchunk': 26,
-                                                          'slab': 1}}))
+                                                          'slab': 1, 'shell': 1}}))
     c = tuning.choose(geom, device=0)
-    assert (c['tile_y'], c['zchunk'], c['slab']) == (7, 26, 1)
+    assert (c['tile_y'], c['zchunk'], c['slab'], c['shell']) == (7, 26, 1, _native.SHELL_SPLIT)
     assert tuning.choose(geom, kernel=_native.FDTD_KERNEL_SPLIT)['kernel'] == _native.FDTD_KERNEL_SPLIT
 
     class Fake:
@@ -179,7 +179,10 @@ def test_tuning_cache_choose_and_apply(tmp_path, monkeypatch):
     f = Fake()
     tuning.apply(f, c)
     assert f.opts == {_native.OPT_KERNEL: 1, _native.OPT_TILE_X: 32, _native.OPT_TILE_Y: 7,
-                      _native.OPT_ZCHUNK: 26, _native.OPT_FUSED_SLAB: 1}
+                      _native.OPT_ZCHUNK: 26, _native.OPT_FUSED_SLAB: 1,
+                      _native.OPT_SHELL: _native.SHELL_SPLIT}
+    # the default choice marches the shell
+    assert tuning.choose(geom, kernel=_native.FDTD_KERNEL_FUSED)['shell'] == _native.SHELL_MARCH
 
 
 def test_incident_pulse_matches_reference():
