@@ -47,6 +47,8 @@ def parse():
     ap.add_argument('--models', type=int, default=64, help='batch64: number of models')
     ap.add_argument('--kernel', default='auto', choices=['auto', 'split', 'fused'])
     ap.add_argument('--tile-y', type=int, default=None, help='fused kernel rows per tile')
+    ap.add_argument('--shell', default=None, choices=['march', 'split'],
+                    help='fused kernel: shell marched or swept by the split passes')
     ap.add_argument('--zchunk', type=int, default=0, help='fused kernel z planes per block (0: auto)')
     ap.add_argument('--dtype', default='float32', choices=['float32', 'float64'])
     ap.add_argument('--no-e2e', action='store_true')
@@ -292,6 +294,8 @@ def run_ours(a):
         choice = tuning.choose(geom, kernel=kernel,
                                tile=None if a.tile_y is None else (32, a.tile_y))
         choice['zchunk'] = a.zchunk
+        if a.shell is not None:
+            choice['shell'] = _native.SHELL_MARCH if a.shell == 'march' else _native.SHELL_SPLIT
 
     def new_sim():
         sim = _native.NativeSim(geom, local)

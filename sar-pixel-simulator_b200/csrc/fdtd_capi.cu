@@ -101,7 +101,7 @@ struct fdtd_sim {
   int tile_x = 32, tile_y = 8;
   int zchunk = 0;
   int slab = 0;                          // FDTD_OPT_FUSED_SLAB
-  int shell = FDTD_SHELL_MARCH;          // FDTD_OPT_SHELL
+  int shell = FDTD_SHELL_SPLIT;          // FDTD_OPT_SHELL
   FusedPlan plan;
   int plan_ok = 0, plan_tile_y = 0, plan_zchunk = 0, plan_slab = 0, plan_shell = 0;
   int graph_chunk = 0;

@@ -125,14 +125,17 @@ struct ShellBoxes {
 
 // A box of the fused step's shell marched in z by the general kernel
 // (fdtd_march.cu): [x0, x1) x [y0, y1) x [z0, z1), x0 a multiple of 4. A
-// block is kMarchThreads threads: `width` lanes (width * 4 x cells) by
+// block is kMarchThreads threads: `width` lanes of 4 x cells by
 // kMarchThreads / width rows, the first row recomputing the row below the
-// tile; gx, gy tiles per plane, z cut into chunks of `zchunk` planes
-// (`nchunks` of them); `first` is the box's first block in the launch.
+// tile. Lane 0 of a tile is a halo lane (recomputes the vector left of the
+// tile) except in the first tile of a box that starts at x = 0; `lead` own
+// vectors in the first tile, width - 1 in the others; gx, gy tiles per
+// plane, z cut into chunks of `zchunk` planes (`nchunks` of them); `first`
+// is the box's first block in the launch.
 constexpr int kMarchThreads = 160;
 struct MarchBox {
   int x0, x1, y0, y1, z0, z1;
-  int width, gx, gy;
+  int width, lead, gx, gy;
   int zchunk, nchunks;
   int first;
 };

@@ -362,8 +362,12 @@ FusedPlan make_fused_plan(int nx, int ny, int nz, int npml, int tfsf_z, int tile
   p.has_interior = m >= 1 && ib.xa < ib.xb && ib.ya < ib.yb && nzr > 0;
   ShellBoxes& bl = p.shell;
   if (!p.has_interior) {
-    if (march) add_march_box(p.mshell, 0, nx, 0, ny, 0, nz, kMarchZChunk);
-    else add_shell_box(bl, 0, nx, 0, ny, 0, nz);
+    if (march) {
+      add_march_box(p.mshell, 0, nx, 0, ny, 0, nz, kMarchZChunk);
+      finish_march_boxes(p.mshell);
+    } else {
+      add_shell_box(bl, 0, nx, 0, ny, 0, nz);
+    }
     return p;
   }
   // with use_slab, the z slabs of the same x-y box (CPML in z only):
@@ -430,6 +434,7 @@ FusedPlan make_fused_plan(int nx, int ny, int nz, int npml, int tfsf_z, int tile
     add(0, ib.xa, ib.ya, ib.yb, cz0[k], cz1[k]);
     add(ib.xb, nx, ib.ya, ib.yb, cz0[k], cz1[k]);
   }
+  if (march) finish_march_boxes(p.mshell);
   return p;
 }
 

@@ -56,6 +56,10 @@ FusedPlan make_fused_plan(int nx, int ny, int nz, int npml, int tfsf_z, int tile
 // `zchunk` planes.
 void add_march_box(MarchBoxes& mb, int x0, int x1, int y0, int y1, int z0, int z1, int zchunk);
 
+// Orders a march box list longest z chunk first (the long blocks start
+// first and the short ones fill the tail) and numbers the blocks.
+void finish_march_boxes(MarchBoxes& mb);
+
 // Fused step of the march boxes: source set -> destination set, every CPML
 // face, domain edge and injection plane handled in the march.
 template <class T>

@@ -25,10 +25,12 @@
 //      shared memory, the -z neighbour is H^{n+1/2}(z-1) carried from the
 //      previous plane.
 // The first row recomputes H of the row below the tile, lane 0 of every row
-// recomputes H at the cell left of its vector (h_cell, any position), and a
-// chunk starts by recomputing the plane below it; recomputed values are
-// never stored, and psi is written only for the block's own cells. Warps
-// whose vectors are all plain interior vectors take the plain update.
+// H of the vector left of the tile (a halo lane: the same vector update as
+// every other lane, so nothing diverges; not in the first tile of a box
+// that starts at x = 0, which has no left neighbour), and a chunk starts by
+// recomputing the plane below it; recomputed values are never stored, and
+// psi is written only for the block's own cells. Warps whose vectors are
+// all plain interior vectors take the plain update.
 // Per-cell values equal the split passes' bit for bit: the same update
 // functions in the same order of operations, fed the same neighbours.
 #include <algorithm>
@@ -74,7 +76,11 @@ k_march(const __grid_constant__ State<T> s, const int* __restrict__ tp, int toff
   const int by = local % b.gy;
   const int c = local / b.gy;
   const int lane = threadIdx.x % width, r = threadIdx.x / width;
-  const int x0 = b.x0 + (bx * width + lane) * kVec;
+  // own vectors start at vector `first_own` of the box; a halo lane 0 sits
+  // one vector before
+  const int halo = (bx == 0 && b.x0 == 0) ? 0 : 1;
+  const int first_own = bx == 0 ? 0 : b.lead + (bx - 1) * (width - 1);
+  const int x0 = b.x0 + (first_own + lane - halo) * kVec;
   const int y = b.y0 + by * (rows - 1) + r - 1;   // row 0 is the row below the tile
   const int z0 = b.z0 + c * b.zchunk;
   const int z1 = min(b.z1, z0 + b.zchunk);
@@ -83,8 +89,8 @@ k_march(const __grid_constant__ State<T> s, const int* __restrict__ tp, int toff
   const int ny = s.ny, nz = s.nz;
   // Rows outside the grid and lanes past the pitch only feed the shared
   // memory exchange and the shuffles (as zeros).
-  const bool vin = x0 < s.pitch && y >= 0 && y < ny;
-  const bool own = vin && r >= 1 && y < b.y1 && x0 < b.x1;
+  const bool vin = x0 >= 0 && x0 < s.pitch && y >= 0 && y < ny;
+  const bool own = vin && r >= 1 && lane >= halo && y < b.y1 && x0 < b.x1;
   const long long P = s.plane, W = s.pitch;
   long long i = (long long)zs * P + (vin ? (long long)y * W + x0 : 0);
   const int so = threadIdx.x * kVec;
@@ -115,19 +121,6 @@ k_march(const __grid_constant__ State<T> s, const int* __restrict__ tp, int toff
     }
     T eyr = T(0), ezr = T(0);   // +x neighbour of the last lane lies in the next tile
     if (lane == width - 1 && vin && x0 + kVec < s.pitch) { eyr = s.iey[i + kVec]; ezr = s.iez[i + kVec]; }
-    // lane 0: the source values H^{n+1/2} at (z, y, x0 - 1) needs
-    ENbr<T> g;
-    T ghy = T(0), ghz = T(0);
-    const bool left = work && lane == 0 && x0 >= 1;
-    if (left) {
-      const long long j = i - 1;
-      g.ex0 = s.iex[j]; g.ey0 = s.iey[j]; g.ez0 = s.iez[j];
-      g.exz = up ? s.iex[j + P] : T(0);
-      g.eyz = up ? s.iey[j + P] : T(0);
-      g.exy = y + 1 < ny ? s.iex[j + W] : T(0);
-      g.ezy = y + 1 < ny ? s.iez[j + W] : T(0);
-      ghy = s.ihy[j]; ghz = s.ihz[j];
-    }
     // ---- H^{n+1/2}(z) -----------------------------------------------------
     st4(&sEx[so], e.ex);
     st4(&sEz[so], e.ez);
@@ -136,11 +129,13 @@ k_march(const __grid_constant__ State<T> s, const int* __restrict__ tp, int toff
     e.eyn = __shfl_down_sync(kFull, e.ey[0], 1, width);
     e.ezn = __shfl_down_sync(kFull, e.ez[0], 1, width);
     if (lane == width - 1) { e.eyn = eyr; e.ezn = ezr; }
-    // plain_h: every vector of the warp is a plain interior vector (for H
-    // and for E)
+    // warp-uniform paths: every vector of the warp a plain interior vector
+    // (for H and for E), or one whose only boundary term is the z face
     const bool plain_h = __all_sync(kFull, !vin || interior(s, z, y, x0, t));
+    const bool zface_h = !plain_h && __all_sync(kFull, !vin || zface_only(s, z, y, x0, t));
     if (vin) {
       if (plain_h) h_vec_interior(s, e, h.hx, h.hy, h.hz);
+      else if (zface_h) h_vec_zface(s, e, z, y, x0, work, h.hx, h.hy, h.hz);
       else h_vec(s, e, z, y, x0, t, work, h.hx, h.hy, h.hz);
     }
     st4(&sHx[so], h.hx);
@@ -149,20 +144,15 @@ k_march(const __grid_constant__ State<T> s, const int* __restrict__ tp, int toff
     // ---- E^{n+1}(z) ---------------------------------------------------------
     h.hyp = __shfl_up_sync(kFull, h.hy[kVec - 1], 1, width);
     h.hzp = __shfl_up_sync(kFull, h.hz[kVec - 1], 1, width);
-    if (lane == 0) {   // H^{n+1/2} left of the vector (any position)
-      T hxl = T(0), hyl = ghy, hzl = ghz;
-      if (left) {
-        g.eyx = e.ey[0];
-        g.ezx = e.ez[0];
-        h_cell(s, g, z, y, x0 - 1, t, false, hxl, hyl, hzl);
-      }
-      h.hyp = hyl;
-      h.hzp = hzl;
+    if (lane == 0) {   // own only at x0 = 0, whose E update reads no x - 1 value
+      h.hyp = T(0);
+      h.hzp = T(0);
     }
     if (work) {
       ld4(h.hxy, &sHx[sd]);
       ld4(h.hzy, &sHz[sd]);
       if (plain_h) e_vec_interior(h, ca, cb, e.ex, e.ey, e.ez);
+      else if (zface_h) e_vec_zface(s, h, ca, cb, z, y, x0, e.ex, e.ey, e.ez);
       else e_vec(s, h, ca, cb, z, y, x0, t, true, e.ex, e.ey, e.ez);
       st4(s.ohx + i, h.hx); st4(s.ohy + i, h.hy); st4(s.ohz + i, h.hz);
       st4(s.oex + i, e.ex); st4(s.oey + i, e.ey); st4(s.oez + i, e.ez);
@@ -183,16 +173,24 @@ void add_march_box(MarchBoxes& mb, int x0, int x1, int y0, int y1, int z0, int z
   }
   MarchBox& b = mb.b[mb.n++];
   b.x0 = x0; b.x1 = x1; b.y0 = y0; b.y1 = y1; b.z0 = z0; b.z1 = z1;
-  // row width with the least padded area (ties: the wider rows)
+  // tiles of a row width: `lead` own vectors in the first (the whole row
+  // when the box starts at x = 0, else all lanes but the halo lane), then
+  // width - 1 per tile
+  const int nv = (x1 - x0 + kVec - 1) / kVec;
+  auto tiles = [&](int w, int& lead) {
+    lead = x0 == 0 ? w : w - 1;
+    return nv <= lead ? 1 : 1 + (nv - lead + w - 2) / (w - 1);
+  };
+  // row width with the fewest threads (ties: the wider rows)
   long long best = -1;
   for (int w : {32, 16, 8}) {
     const int ty = kMarchThreads / w - 1;
-    const long long gx = (x1 - x0 + 4 * w - 1) / (4 * w), gy = (y1 - y0 + ty - 1) / ty;
-    const long long padded = gx * 4 * w * gy * ty;
-    if (best < 0 || padded < best) { best = padded; b.width = w; }
+    int lead = 0;
+    const long long threads = (long long)tiles(w, lead) * ((y1 - y0 + ty - 1) / ty) * kMarchThreads;
+    if (best < 0 || threads < best) { best = threads; b.width = w; }
   }
   const int ty = kMarchThreads / b.width - 1;
-  b.gx = (x1 - x0 + b.width * kVec - 1) / (b.width * kVec);
+  b.gx = tiles(b.width, b.lead);
   b.gy = (y1 - y0 + ty - 1) / ty;
   // chunks of about zchunk planes, evenly cut (each recomputes the plane
   // below it)
@@ -203,6 +201,15 @@ void add_march_box(MarchBoxes& mb, int x0, int x1, int y0, int y1, int z0, int z
   b.nchunks = (len + b.zchunk - 1) / b.zchunk;
   b.first = mb.total_blocks;
   mb.total_blocks += b.gx * b.gy * b.nchunks;
+}
+
+void finish_march_boxes(MarchBoxes& mb) {
+  std::stable_sort(mb.b, mb.b + mb.n, [](const MarchBox& a, const MarchBox& c) { return a.zchunk > c.zchunk; });
+  mb.total_blocks = 0;
+  for (int k = 0; k < mb.n; ++k) {
+    mb.b[k].first = mb.total_blocks;
+    mb.total_blocks += mb.b[k].gx * mb.b[k].gy * mb.b[k].nchunks;
+  }
 }
 
 template <class T>

@@ -115,6 +115,77 @@ __device__ __forceinline__ void e_vec_interior(const HVec<T>& h, const T (&ca)[k
   }
 }
 
+// True when the only boundary term of the vector (for H and for E) is the
+// z-face CPML: every cell inside both update ranges in x and y, away from
+// the x and y faces, z inside [1, nz - 1) and in an H or E z face, no
+// injection. The update is then the plain curl update plus the z-face
+// terms, whose coefficients are uniform over the plane.
+template <class T>
+__device__ __forceinline__ bool zface_only(const State<T>& s, int z, int y, int x0, int t) {
+  const int m = s.npml;
+  return z >= 1 && z < s.nz - 1 && (z < m || z >= s.nz - m) && y >= m && y < s.ny - m && x0 >= m &&
+         x0 + kVec <= s.nx - m && !injects(s, z, t);
+}
+
+// H update of a vector for which zface_only holds: the plain update, then
+// the z-face terms in h_vec's order (cpml_h_down/up, cpu/field_updates.py:243-282).
+template <class T>
+__device__ __forceinline__ void h_vec_zface(const State<T>& s, const EVec<T>& e, int z, int y, int x0,
+                                            bool wpsi, T (&hx)[kVec], T (&hy)[kVec], T (&hz)[kVec]) {
+  using M = R<T>;
+  const int nz = s.nz, m = s.npml;
+  h_vec_interior(s, e, hx, hy, hz);
+  if (z < m - 1 || z >= nz - m) {
+    const int side = z < m - 1 ? 0 : 1;
+    const int q = side ? z - (nz - m) : z;
+    const T b = s.prof[side ? BH_U : BH_D][q];
+    const T c = s.prof[side ? CH_U : CH_D][q];
+    const long long k = ((long long)q * s.ny + y) * s.pitch + x0;
+    T p3[kVec], p2[kVec];
+    ld4(p3, s.ps.z[side][3] + k);
+    ld4(p2, s.ps.z[side][2] + k);
+#pragma unroll
+    for (int j = 0; j < kVec; ++j) {
+      p3[j] = M::add(M::mul(b, p3[j]), div_dx(s, M::mul(c, M::sub(e.exz[j], e.ex[j]))));   // psi_Hyz
+      p2[j] = M::add(M::mul(b, p2[j]), div_dx(s, M::mul(c, M::sub(e.eyz[j], e.ey[j]))));   // psi_Hxz
+      hy[j] = M::sub(hy[j], M::mul(s.dtm0, p3[j]));
+      hx[j] = M::add(hx[j], M::mul(s.dtm0, p2[j]));
+    }
+    if (wpsi) { st4(s.pd.z[side][3] + k, p3); st4(s.pd.z[side][2] + k, p2); }
+  }
+}
+
+// E update of a vector for which zface_only holds: the plain update, then
+// the z-face terms in e_vec's order (cpml_e_down/up, cpu/field_updates.py:66-105).
+template <class T>
+__device__ __forceinline__ void e_vec_zface(const State<T>& s, const HVec<T>& h, const T (&ca)[kVec],
+                                            const T (&cb)[kVec], int z, int y, int x0, T (&ex)[kVec],
+                                            T (&ey)[kVec], T (&ez)[kVec]) {
+  using M = R<T>;
+  const int nz = s.nz, m = s.npml;
+  e_vec_interior(h, ca, cb, ex, ey, ez);
+  if (z < m || z >= nz - m) {   // z >= 1 holds (zface_only)
+    const int side = z < m ? 0 : 1;
+    const int q = side ? z - (nz - m) : z;
+    const T b = s.prof[side ? BE_U : BE_D][q];
+    const T c = s.prof[side ? CE_U : CE_D][q];
+    const long long k = ((long long)q * s.ny + y) * s.pitch + x0;
+    T p1[kVec], p0[kVec];
+    ld4(p1, s.ps.z[side][1] + k);
+    ld4(p0, s.ps.z[side][0] + k);
+#pragma unroll
+    for (int j = 0; j < kVec; ++j) {
+      const T cbdx = M::mul(cb[j], s.dx);
+      p1[j] = M::add(M::mul(b, p1[j]), div_dx(s, M::mul(c, M::sub(h.hx[j], h.hxz[j]))));   // psi_Eyz
+      p0[j] = M::add(M::mul(b, p0[j]), div_dx(s, M::mul(c, M::sub(h.hy[j], h.hyz[j]))));   // psi_Exz
+      ey[j] = M::add(ey[j], M::mul(cbdx, p1[j]));
+      ex[j] = M::sub(ex[j], M::mul(cbdx, p0[j]));
+    }
+    st4(s.pd.z[side][1] + k, p1);
+    st4(s.pd.z[side][0] + k, p0);
+  }
+}
+
 // Complete H update of the vector at (z, y, x0..x0+3), any position.
 // psi is read from s.ps and, when wpsi, written to s.pd.
 template <class T>
