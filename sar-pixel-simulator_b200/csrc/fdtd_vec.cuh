@@ -129,9 +129,12 @@ __device__ __forceinline__ bool zface_only(const State<T>& s, int z, int y, int 
 
 // H update of a vector for which zface_only holds: the plain update, then
 // the z-face terms in h_vec's order (cpml_h_down/up, cpu/field_updates.py:243-282).
+// src3, src2: psi_Hyz, psi_Hxz of the vector (a staged copy of the source
+// psi, or the source psi itself).
 template <class T>
 __device__ __forceinline__ void h_vec_zface(const State<T>& s, const EVec<T>& e, int z, int y, int x0,
-                                            bool wpsi, T (&hx)[kVec], T (&hy)[kVec], T (&hz)[kVec]) {
+                                            bool wpsi, const T* src3, const T* src2, T (&hx)[kVec],
+                                            T (&hy)[kVec], T (&hz)[kVec]) {
   using M = R<T>;
   const int nz = s.nz, m = s.npml;
   h_vec_interior(s, e, hx, hy, hz);
@@ -142,8 +145,8 @@ __device__ __forceinline__ void h_vec_zface(const State<T>& s, const EVec<T>& e,
     const T c = s.prof[side ? CH_U : CH_D][q];
     const long long k = ((long long)q * s.ny + y) * s.pitch + x0;
     T p3[kVec], p2[kVec];
-    ld4(p3, s.ps.z[side][3] + k);
-    ld4(p2, s.ps.z[side][2] + k);
+    ld4(p3, src3);
+    ld4(p2, src2);
 #pragma unroll
     for (int j = 0; j < kVec; ++j) {
       p3[j] = M::add(M::mul(b, p3[j]), div_dx(s, M::mul(c, M::sub(e.exz[j], e.ex[j]))));   // psi_Hyz
@@ -157,10 +160,12 @@ __device__ __forceinline__ void h_vec_zface(const State<T>& s, const EVec<T>& e,
 
 // E update of a vector for which zface_only holds: the plain update, then
 // the z-face terms in e_vec's order (cpml_e_down/up, cpu/field_updates.py:66-105).
+// src1, src0: psi_Eyz, psi_Exz of the vector (staged or source).
 template <class T>
 __device__ __forceinline__ void e_vec_zface(const State<T>& s, const HVec<T>& h, const T (&ca)[kVec],
-                                            const T (&cb)[kVec], int z, int y, int x0, T (&ex)[kVec],
-                                            T (&ey)[kVec], T (&ez)[kVec]) {
+                                            const T (&cb)[kVec], int z, int y, int x0, const T* src1,
+                                            const T* src0, T (&ex)[kVec], T (&ey)[kVec],
+                                            T (&ez)[kVec]) {
   using M = R<T>;
   const int nz = s.nz, m = s.npml;
   e_vec_interior(h, ca, cb, ex, ey, ez);
@@ -171,8 +176,8 @@ __device__ __forceinline__ void e_vec_zface(const State<T>& s, const HVec<T>& h,
     const T c = s.prof[side ? CE_U : CE_D][q];
     const long long k = ((long long)q * s.ny + y) * s.pitch + x0;
     T p1[kVec], p0[kVec];
-    ld4(p1, s.ps.z[side][1] + k);
-    ld4(p0, s.ps.z[side][0] + k);
+    ld4(p1, src1);
+    ld4(p0, src0);
 #pragma unroll
     for (int j = 0; j < kVec; ++j) {
       const T cbdx = M::mul(cb[j], s.dx);
