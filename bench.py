@@ -60,7 +60,10 @@ def parse():
 # ---------------------------------------------------------------------------
 # workload
 # ---------------------------------------------------------------------------
-def build_workload(name, dtype, nsteps_inc, seed=2024):
+def build_workload(name, dtype, nsteps_inc, seed=2024, with_model=False):
+    """(params, Ca, Cb, incident planes) of a plain-solve workload, and the
+    material model (eps_r, sigma of the material planes) with with_model.
+    Host modules only: the device library is not loaded here."""
     from fdtdsarsim_b200 import synthetic
     from fdtdsarsim_b200.materials import compute_material_arrays
     pc = synthetic.config_params(name, dtype)
@@ -78,6 +81,8 @@ def build_workload(name, dtype, nsteps_inc, seed=2024):
     n = min(g.size_t_inc, nsteps_inc)
     inc = synthetic.plane_wave_incident(pc, n, dtype)
     g.size_t_inc = n
+    if with_model:
+        return pc, ca, cb, inc, model
     return pc, ca, cb, inc
 
 
@@ -280,7 +285,7 @@ def run_ours(a):
     from fdtdsarsim_b200.gpu.main_sim import native_geometry
     from fdtdsarsim_b200 import tuning
 
-    pc, ca, cb, inc = build_workload(a.workload, a.dtype, a.warmup + a.steps + 1)
+    pc, ca, cb, inc, model = build_workload(a.workload, a.dtype, a.warmup + a.steps + 1, with_model=True)
     g = pc.geom_params
     cells = g.size_x * g.size_y * g.size_z
     geom = native_geometry(pc)
@@ -360,15 +365,19 @@ def run_ours(a):
     sim.close()
     del sim
 
-    # end to end through the C-ABI with host buffers
+    # end to end through the C-ABI with host buffers, as run_experiment
+    # drives it (MainSimGpu.run_eps_sigma): the material block's eps_r and
+    # sigma go up and the device makes Ca, Cb; the incident planes stream
+    # from pinned memory beside the steps; the 24 phasor planes come back
     e2e = None
     if not a.no_e2e:
         pin = {}
         for k, v in inc.items():
             t = torch.from_numpy(v).pin_memory()
             pin[k] = t.numpy()
-        ca_p = torch.from_numpy(ca).pin_memory().numpy()
-        cb_p = torch.from_numpy(cb).pin_memory().numpy()
+        dt = np.dtype(a.dtype)
+        eps_p = torch.from_numpy(np.ascontiguousarray(model.relative_permittivity, dt)).pin_memory().numpy()
+        sig_p = torch.from_numpy(np.ascontiguousarray(model.conductivity, dt)).pin_memory().numpy()
         sim2 = new_sim()
         ph_buf = torch.empty(2 * sim2.phasors_size(), dtype=torch.float32 if a.dtype == 'float32'
                              else torch.float64).pin_memory().numpy().view(sim2.cdtype)
@@ -376,17 +385,22 @@ def run_ours(a):
         barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        sim2.set_materials(ca_p, cb_p)
+        sim2.set_materials_eps_sigma(eps_p, sig_p)
         sim2.run_streamed(a.steps, pin['ex'], pin['ey'], pin['hx'], pin['hy'])
         phs = sim2.get_phasors(ph_buf)
         t1 = time.perf_counter()
         el = max_over_ranks(t1 - t0, world, 'cuda')
         esz = np.dtype(a.dtype).itemsize
-        h2d = 2 * cells * esz + 4 * g.size_t_inc * g.size_x * g.size_y * esz
+        # bytes copied: the material block once, then the incident planes of
+        # the steps that ran (t < size_t_inc), four components each
+        streamed = min(a.steps, g.size_t_inc)
+        h2d = eps_p.nbytes + sig_p.nbytes + 4 * streamed * g.size_x * g.size_y * esz
         d2h = sum(p.nbytes for p in phs.values())
         e2e = {'value': round(world * cells * a.steps / el / 1e6, 1), 'unit': 'Mcell-updates/s',
                'h2d_bytes_per_step': int(h2d / a.steps), 'd2h_bytes_per_step': int(d2h / a.steps),
-               'includes': 'Ca/Cb upload, incident planes from pinned host memory, '
+               'includes': f'eps_r/sigma upload of the {eps_p.shape[0]}-plane material block (Ca/Cb '
+                           f'made on the device, as run_experiment does), incident planes of '
+                           f'{streamed} steps from pinned host memory beside the stepping, '
                            f'{a.steps} steps, 24 phasor planes read back into pinned memory; '
                            'wall clock'}
         sim2.close()

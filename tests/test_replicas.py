@@ -83,9 +83,18 @@ def test_reference_arm_line_on_the_host():
     """bench.py --impl reference needs no GPU: it times the C restatement
     on the host cores and prints one line with the contract's keys."""
     import subprocess
-    out = subprocess.run([sys.executable, os.path.join(ROOT, 'bench.py'), '--impl', 'reference',
-                          '--workload', 'plain_8x8', '--steps', '1', '--warmup', '1'],
-                         capture_output=True, text=True, timeout=600, cwd=ROOT, check=True)
+    # run bench.py in a process that then reports whether the product
+    # library was ever mapped: the reference arm must not load it
+    code = ('import runpy, sys\n'
+            f'sys.argv = [{os.path.join(ROOT, "bench.py")!r}, "--impl", "reference", '
+            '"--workload", "plain_8x8", "--steps", "1", "--warmup", "1"]\n'
+            f'runpy.run_path({os.path.join(ROOT, "bench.py")!r}, run_name="__main__")\n'
+            'maps = open("/proc/self/maps").read()\n'
+            'print("MAPPED", "libfdtd_b200" in maps, "fdtdsarsim_b200._native" in sys.modules, '
+            'file=sys.stderr)\n')
+    out = subprocess.run([sys.executable, '-c', code], capture_output=True, text=True, timeout=600,
+                         cwd=ROOT, check=True)
+    assert 'MAPPED False False' in out.stderr, out.stderr[-2000:]
     line = json.loads(out.stdout.strip().splitlines()[-1])
     assert line['impl'] == 'reference' and line['metric'] == 'Mcell-updates/s'
     assert line['value'] > 0 and line['higher_is_better'] is True and line['n_gpus'] == 1
