@@ -54,6 +54,8 @@ def parse():
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--cpu-steps', type=int, default=4)
+    ap.add_argument('--no-extras', action='store_true',
+                    help='plain_16x16 at N=1: skip the batch64, adjoint_4x4 and fp64_error records')
     return ap.parse_args()
 
 
@@ -404,10 +406,26 @@ def run_ours(a):
                            f'{a.steps} steps, 24 phasor planes read back into pinned memory; '
                            'wall clock'}
         sim2.close()
+        pin = eps_p = sig_p = ph_buf = phs = None   # page-locked buffers
 
     base = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         base = cpu_baseline(pc, ca, cb, inc, a.cpu_steps)
+
+    # the batched, adjoint and float64 claims, measured in the same run
+    # (after the timed region; each with its own clock record)
+    extras = {}
+    if rank == 0 and world == 1 and a.workload == 'plain_16x16' and not a.no_extras:
+        del ca, cb, inc, model
+        for key, fn in (('batch64', lambda: batch_record(a, 64, a.steps, a.warmup)),
+                        ('adjoint_4x4', lambda: adjoint_record(a, 32)),
+                        ('fp64_error', lambda: fp64_record('plain_16x16'))):
+            t0 = time.perf_counter()
+            try:
+                extras[key] = fn()
+            except Exception as ex:   # recorded in the line, the headline stands
+                extras[key] = {'error': f'{type(ex).__name__}: {ex}'}
+            extras[key]['wall_s'] = round(time.perf_counter() - t0, 1)
 
     if rank == 0:
         line = {
@@ -431,6 +449,7 @@ def run_ours(a):
             'roofline': roofline, 'cpu_baseline': base, 'e2e': e2e,
             'gpu_launches': gpu_launches, 'clocks': clk,
         }
+        line.update(extras)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
@@ -495,14 +514,18 @@ def batch_models(n, nsteps_inc, seed=4040, dtype='float32'):
     return out
 
 
-def run_batch(a):
+def batch_record(a, n_models, steps, warmup, check_members=(0, 21, 42)):
+    """batch64: n_models uneven models advanced together (both batch modes,
+    the faster is the result) and one after another (each model's own time
+    loop on one stream). Members of the batched run are compared bit for
+    bit with the same models' sequential solves."""
     import torch
     torch.cuda.set_device(0)
     from fdtdsarsim_b200 import _native, tuning
     from fdtdsarsim_b200.absorbers import packed_profiles
     from fdtdsarsim_b200.gpu.main_sim import native_geometry
 
-    models = batch_models(a.models, a.warmup + a.steps + 1, dtype=a.dtype)
+    models = batch_models(n_models, warmup + steps + 1, dtype=a.dtype)
     cells = [pc.geom_params.size_x * pc.geom_params.size_y * pc.geom_params.size_z
              for pc, _, _, _ in models]
     total = int(sum(cells))
@@ -513,12 +536,11 @@ def run_batch(a):
         sim.set_absorbers(packed_profiles(pc))
         choice = tuning.choose(geom)
         choices.append(choice)
-        sim.set_option(_native.OPT_KERNEL, choice['kernel'])
-        sim.set_option(_native.OPT_TILE_X, choice['tile_x'])
-        sim.set_option(_native.OPT_TILE_Y, choice['tile_y'])
+        tuning.apply(sim, choice)
         sim.set_materials(ca, cb)
         sim.set_incident(inc['ex'], inc['ey'], inc['hx'], inc['hy'])
         sims.append(sim)
+    check_members = [k for k in check_members if k < len(sims)]
 
     def timed(stream, fn):
         torch.cuda.synchronize()
@@ -530,23 +552,27 @@ def run_batch(a):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1)
 
+    def snapshot():
+        return {k: {c: sims[k].get_field(c) for c in ('ex', 'hz')} for k in check_members}
+
     # batched, two modes: (split) every member each step, one launch per
     # pass, graph chunks; (streams) every member's own step path on its own
     # stream, side by side. The faster is the batched result.
     batch = _native.Batch(sims)
     bstream = torch.cuda.ExternalStream(batch.stream())
-    batch.run(a.warmup)
+    batch.run(warmup)
     batch.synchronize()
     clocks = ClockSampler(0)
     clocks.start()
-    ms_split = timed(bstream, lambda: batch.run(a.steps))
+    ms_split = timed(bstream, lambda: batch.run(steps))
+    snap_split = snapshot()
     for s in sims:
         s.reset()
     batch.set_streams(True)
-    batch.run(a.warmup)
+    batch.run(warmup)
     batch.synchronize()
-    ms_streams = timed(bstream, lambda: batch.run(a.steps))
-    clk = clocks.stop()
+    ms_streams = timed(bstream, lambda: batch.run(steps))
+    snap_streams = snapshot()
     batch.close()
     mode = 'streams' if ms_streams < ms_split else 'split'
     ms_b = min(ms_streams, ms_split)
@@ -558,51 +584,63 @@ def run_batch(a):
     seq = torch.cuda.Stream()
     for s in sims:
         s.set_stream(seq.cuda_stream)
-        s.run(a.warmup)
-    ms_s = timed(seq, lambda: [s.run(a.steps) for s in sims])
+        s.run(warmup)
+    ms_s = timed(seq, lambda: [s.run(steps) for s in sims])
+    clk = clocks.stop()
+    snap_seq = snapshot()
+    same = all(np.array_equal(snap[k][c].view(np.uint8), snap_seq[k][c].view(np.uint8))
+               for snap in (snap_split, snap_streams) for k in check_members for c in ('ex', 'hz'))
     for s in sims:
         s.close()
 
-    value = total * a.steps / (ms_b / 1e3) / 1e6
-    seq_value = total * a.steps / (ms_s / 1e3) / 1e6
+    value = total * steps / (ms_b / 1e3) / 1e6
+    seq_value = total * steps / (ms_s / 1e3) / 1e6
     peak, peak_kind = measured_peak_hbm()
-    achieved = total * BYTES_PER_CELL[a.dtype] * a.steps / (ms_b / 1e3) / 1e9
+    achieved = total * BYTES_PER_CELL[a.dtype] * steps / (ms_b / 1e3) / 1e9
     nx = [pc.geom_params.size_x for pc, _, _, _ in models]
     nz = [pc.geom_params.size_z for pc, _, _, _ in models]
-    line = {
+    return {
         'metric': 'Mcell-updates/s', 'value': round(value, 1), 'unit': 'Mcell-updates/s',
-        'n_gpus': 1, 'steps': a.steps, 'warmup': a.warmup, 'ms_per_step': round(ms_b / a.steps, 4),
+        'n_gpus': 1, 'steps': steps, 'warmup': warmup, 'ms_per_step': round(ms_b / steps, 4),
         'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
         'dtype': 'f32' if a.dtype == 'float32' else 'f64',
         'data': 'synthetic (seeded vegetation models, tapered plane-wave incident planes)',
-        'config': {'workload': f'batch{a.models}: {a.models} vegetation models, x-y 2-8 wl, depth '
+        'config': {'workload': f'batch{n_models}: {n_models} vegetation models, x-y 2-8 wl, depth '
                                f'0.5-2 wl, cell 0.03 wl, HH/VV, 5.4 GHz',
-                   'models': a.models, 'cells_total': total,
+                   'models': n_models, 'cells_total': total,
                    'nx_range': [int(min(nx)), int(max(nx))], 'nz_range': [int(min(nz)), int(max(nz))],
                    'l2': 'inputs larger than L2 (fields of all models)',
                    'batched': ('every model on its own stream, its default kernel, side by side'
                                if mode == 'streams' else
                                'split step of every model per launch, 64-step graph chunks'),
-                   'modes_ms_per_step': {'split': round(ms_split / a.steps, 4),
-                                         'streams': round(ms_streams / a.steps, 4)}},
-        'sequential': {'value': round(seq_value, 1), 'ms_per_step': round(ms_s / a.steps, 4),
+                   'modes_ms_per_step': {'split': round(ms_split / steps, 4),
+                                         'streams': round(ms_streams / steps, 4)}},
+        'sequential': {'value': round(seq_value, 1), 'ms_per_step': round(ms_s / steps, 4),
                        'kernel': 'each model alone, its default kernel, one shared stream'},
         'speedup_vs_sequential': round(ms_s / ms_b, 3),
+        'members_equal_sequential': {'members': check_members, 'fields': ['ex', 'hz'],
+                                     'modes': ['split', 'streams'], 'bit_exact': bool(same)},
         'roofline': {'bound': 'hbm', 'achieved': round(achieved, 1), 'peak': peak, 'unit': 'GB/s',
                      'frac': round(achieved / peak, 4), 'traffic': None, 'peak_source': peak_kind,
                      'kernel': 'fused_step (member streams)' if mode == 'streams' else 'batch_split_step'},
         'cpu_baseline': None, 'e2e': None,
-        'gpu_launches': (sum(step_launches(c) for c in choices) * a.steps
-                         if mode == 'streams' else 3 * a.steps + 1 + (a.steps + 63) // 64),
+        'gpu_launches': (sum(step_launches(c) for c in choices) * steps
+                         if mode == 'streams' else 3 * steps + 1 + (steps + 63) // 64),
         'clocks': clk,
     }
-    print(json.dumps(line))
+
+
+def run_batch(a):
+    print(json.dumps(batch_record(a, a.models, a.steps, a.warmup)))
 
 
 # ---------------------------------------------------------------------------
 # adjoint: cost of the gradient against one forward solve, and its accuracy
 # ---------------------------------------------------------------------------
-def run_adjoint(a):
+def adjoint_record(a, fd_cells):
+    """adjoint_4x4: the gradient's cost against one forward solve and its
+    accuracy against central differences of float64 solves and against the
+    float64 adjoint."""
     import torch
     torch.cuda.set_device(0)
     from fdtdsarsim_b200 import synthetic
@@ -625,6 +663,8 @@ def run_adjoint(a):
     run = BackscatterGradient(pc, inc, checkpoint_every=64)
     run.value(eps, sig)   # warm-up
     run.value_and_grad(eps, sig)
+    clocks = ClockSampler(0)
+    clocks.start()
 
     def wall(fn, reps):
         torch.cuda.synchronize()
@@ -635,6 +675,7 @@ def run_adjoint(a):
         return (time.perf_counter() - t0) / reps, out
     t_fwd, J = wall(lambda: run.value(eps, sig), 3)
     t_adj, (J2, ge, gs) = wall(lambda: run.value_and_grad(eps, sig), 3)
+    clk = clocks.stop()
     if a.profile_region:
         # one more gradient between cudaProfilerStart/Stop, for
         # `ncu --profile-from-start off` (no effect without a profiler)
@@ -651,7 +692,7 @@ def run_adjoint(a):
     rng = np.random.default_rng(7)
     mask = np.abs(ge64) > 1e-3 * np.abs(ge64).max()
     cells = np.argwhere(mask)
-    picks = cells[rng.choice(len(cells), size=min(a.fd_cells, len(cells)), replace=False)]
+    picks = cells[rng.choice(len(cells), size=min(fd_cells, len(cells)), replace=False)]
     err32, err64 = [], []
     for z, y, x in picks:
         for base, g32, g64, is_eps in ((eps, ge, ge64, True), (sig, gs, gs64, False)):
@@ -688,11 +729,15 @@ def run_adjoint(a):
                      'max_rel_err_f64_adjoint': float(max(err64)) if err64 else None},
         'f32_vs_f64_adjoint_rel_l2': norm_rel, 'gradients_finite': finite,
         'nonfinite_f32': int((~np.isfinite(ge)).sum() + (~np.isfinite(gs)).sum()),
-        'kernel': tuned,
+        'kernel': tuned, 'clocks': clk,
     }
     run.close()
     run64.close()
-    print(json.dumps(line))
+    return line
+
+
+def run_adjoint(a):
+    print(json.dumps(adjoint_record(a, a.fd_cells)))
 
 
 # ---------------------------------------------------------------------------
@@ -775,6 +820,77 @@ def run_incident(a):
         'gpu_launches': 4 * steps,
     }
     print(json.dumps(line))
+
+
+def fp64_record(name='plain_16x16', seed=2024):
+    """float32 against float64 for a full solve of a benchmark geometry on
+    the device: the same seeded material model (eps_r, sigma rounded to each
+    type, Ca/Cb made on the device), each precision's own incident beam made
+    on the device (tapered-wave excitation and vacuum run, handed over device
+    to device, as run_experiment does), all size_t steps; then the
+    backscatter far field (theta = -theta_inc, r = 2 km) and its power."""
+    import torch
+    torch.cuda.set_device(0)
+    from fdtdsarsim_b200 import _native, synthetic, tuning
+    from fdtdsarsim_b200.absorbers import packed_profiles
+    from fdtdsarsim_b200.gpu.main_sim import native_geometry
+    from fdtdsarsim_b200.incident import IncidentSimGpu, create_pulse
+    from fdtdsarsim_b200.near2far import FarFieldTransform
+    from fdtdsarsim_b200.processresults import farfield_power
+    pc = synthetic.config_params(name, 'float64')
+    rng = np.random.default_rng(seed)
+    model = (synthetic.snowpack_over_rough_soil(pc, rng) if name == 'plain_16x16'
+             else synthetic.rough_lognormal_soil(pc, rng))
+    out = {}
+    clocks = ClockSampler(0)
+    clocks.start()
+    for dtype in ('float32', 'float64'):
+        p = synthetic.config_params(name, dtype)
+        g, b = p.geom_params, p.inc_beam_params
+        t0 = time.perf_counter()
+        inc = IncidentSimGpu(p, 0)
+        _, _, pulse_fft, pulse_freqs = create_pulse(p)
+        inc.make_excitation(pulse_fft, pulse_freqs)
+        inc.run()
+        geom = native_geometry(p)
+        sim = _native.NativeSim(geom, 0)
+        sim.set_absorbers(packed_profiles(p))
+        tuning.apply(sim, tuning.choose(geom))
+        sim.set_materials_eps_sigma(model.relative_permittivity.astype(dtype),
+                                    model.conductivity.astype(dtype))
+        sim.set_incident_from(inc.native)
+        inc.close()
+        sim.run(g.size_t)
+        ph = sim.get_phasors()
+        sim.synchronize()
+        sim.close()
+        el = time.perf_counter() - t0
+        ff = FarFieldTransform(0)(ph, g.size_x - 2 * g.size_pml, g.size_y - 2 * g.size_pml,
+                                  g.size_z - 2 * g.size_pml, g.cell_size, 2.0e3,
+                                  np.array([-b.theta_angle]), np.array([b.phi_angle]), b.frequency)
+        p_h, p_v = farfield_power(ff['E_theta'], ff['E_phi'], ff['H_theta'], ff['H_phi'])
+        hh = str(b.polarization).upper() == 'HH'
+        out[dtype] = {'e': complex(np.ravel(ff['E_phi'] if hh else ff['E_theta'])[0]),
+                      'p': float(np.ravel(p_h if hh else p_v)[0]),
+                      'u': {k: np.asarray(ph[k], np.complex128) for k in
+                            ('ex_ph_u', 'ey_ph_u', 'hx_ph_u', 'hy_ph_u')},
+                      'seconds': round(el, 2), 'steps': g.size_t}
+    clk = clocks.stop()
+    a32, a64 = out['float32'], out['float64']
+    plane_err = max(float(np.max(np.abs(a32['u'][k] - a64['u'][k])) / max(np.max(np.abs(a64['u'][k])), 1e-300))
+                    for k in a64['u'])
+    g = pc.geom_params
+    return {
+        'workload': f'{name}: full solve {g.size_z}x{g.size_y}x{g.size_x}, {g.size_t} steps, '
+                    f'{pc.inc_beam_params.polarization}, the geometry\'s own incident beam made on '
+                    'the device in each precision',
+        'backscatter_power': {'float32': a32['p'], 'float64': a64['p'],
+                              'rel_err': abs(a32['p'] - a64['p']) / abs(a64['p'])},
+        'backscatter_phasor_rel_err': abs(a32['e'] - a64['e']) / abs(a64['e']),
+        'upper_phasor_planes_max_err_of_peak': plane_err,
+        'seconds': {'float32': a32['seconds'], 'float64': a64['seconds']},
+        'clocks': clk,
+    }
 
 
 def native_cb(params):
