@@ -265,7 +265,7 @@ def step_launches(choice):
     from fdtdsarsim_b200 import _native
     if choice['kernel'] == _native.FDTD_KERNEL_SPLIT:
         return 3
-    if choice.get('shell', _native.SHELL_MARCH) == _native.SHELL_MARCH:
+    if choice.get('shell', _native.SHELL_SPLIT) == _native.SHELL_MARCH:
         return 3
     return 4 + int(bool(choice.get('slab', 0)))
 
@@ -274,7 +274,7 @@ def shell_name(choice):
     from fdtdsarsim_b200 import _native
     if choice['kernel'] == _native.FDTD_KERNEL_SPLIT:
         return None
-    return 'march' if choice.get('shell', _native.SHELL_MARCH) == _native.SHELL_MARCH else 'split_passes'
+    return 'march' if choice.get('shell', _native.SHELL_SPLIT) == _native.SHELL_MARCH else 'split_passes'
 
 
 def run_ours(a):
@@ -387,8 +387,11 @@ def run_ours(a):
         barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        sim2.set_materials_eps_sigma(eps_p, sig_p)
+        sim2.set_materials_eps_sigma(eps_p, sig_p)          # returns when Ca/Cb are made
+        t_mat = time.perf_counter()
         sim2.run_streamed(a.steps, pin['ex'], pin['ey'], pin['hx'], pin['hy'])
+        sim2.synchronize()
+        t_run = time.perf_counter()
         phs = sim2.get_phasors(ph_buf)
         t1 = time.perf_counter()
         el = max_over_ranks(t1 - t0, world, 'cuda')
@@ -400,6 +403,9 @@ def run_ours(a):
         d2h = sum(p.nbytes for p in phs.values())
         e2e = {'value': round(world * cells * a.steps / el / 1e6, 1), 'unit': 'Mcell-updates/s',
                'h2d_bytes_per_step': int(h2d / a.steps), 'd2h_bytes_per_step': int(d2h / a.steps),
+               'phases_ms': {'materials': round((t_mat - t0) * 1e3, 2),
+                             'steps_with_incident_streaming': round((t_run - t_mat) * 1e3, 2),
+                             'phasor_readback': round((t1 - t_run) * 1e3, 2)},
                'includes': f'eps_r/sigma upload of the {eps_p.shape[0]}-plane material block (Ca/Cb '
                            f'made on the device, as run_experiment does), incident planes of '
                            f'{streamed} steps from pinned host memory beside the stepping, '

@@ -74,11 +74,11 @@ extern "C" {
                                     its interior box: FDTD_SHELL_* */
 
 /* shell of the fused step (fdtd_set_option(FDTD_OPT_SHELL, ...)) */
-#define FDTD_SHELL_MARCH 0   /* (default) fused z-marches with the CPML faces,
-                                edges and injection in the march, beside the
-                                interior march */
-#define FDTD_SHELL_SPLIT 1   /* the split H pass beside the interior march,
-                                then the split E pass */
+#define FDTD_SHELL_MARCH 0   /* fused z-marches with the CPML faces, edges and
+                                injection in the march, beside the interior
+                                march (fewer bytes, lower occupancy) */
+#define FDTD_SHELL_SPLIT 1   /* (default) the split H pass beside the
+                                interior march, then the split E pass */
 
 /* kernel kinds of fdtd_get_kernel_time */
 #define FDTD_TIME_STEP    0   /* the field-update kernel(s) of a step */

@@ -93,6 +93,7 @@ struct fdtd_sim {
   // packed (nz, ny, nx) device copy of a host volume, re-pitched on the
   // device by upload_volume (created on first use)
   void* packed = nullptr;
+  void* packed2 = nullptr;               // second one for fdtd_set_materials_eps_sigma
   size_t stage_bytes = 0;
   bool have_abs = false, have_mat = false;
   std::vector<unsigned char> prof;       // 8 * npml values of the element type
@@ -705,10 +706,13 @@ int fdtd_set_materials_eps_sigma(fdtd_sim* s, const void* eps_r, const void* sig
   const fdtd_geometry& g = s->g;
   if (nz_mat < 0 || nz_mat > g.nz) return fail(FDTD_ERR_INVALID, "nz_mat %d outside [0, %d]", nz_mat, g.nz);
   const size_t n = (size_t)nz_mat * g.ny * g.nx;
-  void* de = nullptr;
-  void* ds = nullptr;
-  CK(cudaMallocAsync(&de, std::max<size_t>(n, 1) * s->esz, s->stream));
-  CK(cudaMallocAsync(&ds, std::max<size_t>(n, 1) * s->esz, s->stream));
+  // the two packed volume buffers of the handle (made on first use, kept)
+  // stage eps_r and sigma; no allocation per call
+  const size_t vol_bytes = (size_t)g.nx * g.ny * g.nz * s->esz;
+  if (!s->packed && (rc = alloc(s, vol_bytes, &s->packed))) return rc;
+  if (!s->packed2 && (rc = alloc(s, vol_bytes, &s->packed2))) return rc;
+  void* de = s->packed;
+  void* ds = s->packed2;
   CK(cudaMemcpyAsync(de, eps_r, n * s->esz, cudaMemcpyHostToDevice, s->stream));
   CK(cudaMemcpyAsync(ds, sigma, n * s->esz, cudaMemcpyHostToDevice, s->stream));
   // eps0 as hard-coded in materials/materials.py:45, rounded to the dtype
@@ -722,8 +726,6 @@ int fdtd_set_materials_eps_sigma(fdtd_sim* s, const void* eps_r, const void* sig
                              (const double*)ds, eps0, g.timestep, g.cell_size, (double*)s->ca,
                              (double*)s->cb, s->stream);
   CK(cudaGetLastError());
-  CK(cudaFreeAsync(de, s->stream));
-  CK(cudaFreeAsync(ds, s->stream));
   CK(cudaStreamSynchronize(s->stream));
   s->have_mat = true;
   return FDTD_OK;

@@ -74,10 +74,10 @@ def choose(geom, kernel=None, tile=None, device=0, use_cache=True):
         if hit:
             return {'kernel': int(hit['kernel']), 'tile_x': 32, 'tile_y': int(hit['tile_y']),
                     'zchunk': int(hit['zchunk']), 'slab': int(hit.get('slab', 0)),
-                    'shell': int(hit.get('shell', _MARCH))}
+                    'shell': int(hit.get('shell', _SPLIT))}
     k = _native.FDTD_KERNEL_FUSED if kernel is None else int(kernel)
     tx, ty = tile if tile is not None else DEFAULT_TILE
-    return {'kernel': k, 'tile_x': int(tx), 'tile_y': int(ty), 'zchunk': 0, 'slab': 0, 'shell': _MARCH}
+    return {'kernel': k, 'tile_x': int(tx), 'tile_y': int(ty), 'zchunk': 0, 'slab': 0, 'shell': _SPLIT}
 
 
 def apply(sim, choice):
@@ -88,7 +88,7 @@ def apply(sim, choice):
         sim.set_option(_native.OPT_TILE_Y, choice['tile_y'])
         sim.set_option(_native.OPT_ZCHUNK, choice.get('zchunk', 0))
         sim.set_option(_native.OPT_FUSED_SLAB, choice.get('slab', 0))
-        sim.set_option(_native.OPT_SHELL, choice.get('shell', _MARCH))
+        sim.set_option(_native.OPT_SHELL, choice.get('shell', _SPLIT))
 
 
 def autotune(geom, device=0, steps=6, candidates=None, save=True):

@@ -181,8 +181,8 @@ def test_tuning_cache_choose_and_apply(tmp_path, monkeypatch):
     assert f.opts == {_native.OPT_KERNEL: 1, _native.OPT_TILE_X: 32, _native.OPT_TILE_Y: 7,
                       _native.OPT_ZCHUNK: 26, _native.OPT_FUSED_SLAB: 1,
                       _native.OPT_SHELL: _native.SHELL_SPLIT}
-    # the default choice marches the shell
-    assert tuning.choose(geom, kernel=_native.FDTD_KERNEL_FUSED)['shell'] == _native.SHELL_MARCH
+    # the default choice sweeps the shell with the split passes
+    assert tuning.choose(geom, kernel=_native.FDTD_KERNEL_FUSED)['shell'] == _native.SHELL_SPLIT
 
 
 def test_incident_pulse_matches_reference():
