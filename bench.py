@@ -579,9 +579,17 @@ def batch_record(a, n_models, steps, warmup, check_members=(0, 21, 42)):
     batch.synchronize()
     ms_streams = timed(bstream, lambda: batch.run(steps))
     snap_streams = snapshot()
+    for s in sims:
+        s.reset()
+    batch.set_mode(_native.BATCH_QUEUE)
+    batch.run(warmup)
+    batch.synchronize()
+    ms_queue = timed(bstream, lambda: batch.run(steps))
+    snap_queue = snapshot()
     batch.close()
-    mode = 'streams' if ms_streams < ms_split else 'split'
-    ms_b = min(ms_streams, ms_split)
+    times = {'split': ms_split, 'streams': ms_streams, 'queue': ms_queue}
+    mode = min(times, key=times.get)
+    ms_b = times[mode]
 
     # one after another: each model's own time loop (its default kernel), on
     # one stream so the solves do not overlap
@@ -595,7 +603,8 @@ def batch_record(a, n_models, steps, warmup, check_members=(0, 21, 42)):
     clk = clocks.stop()
     snap_seq = snapshot()
     same = all(np.array_equal(snap[k][c].view(np.uint8), snap_seq[k][c].view(np.uint8))
-               for snap in (snap_split, snap_streams) for k in check_members for c in ('ex', 'hz'))
+               for snap in (snap_split, snap_streams, snap_queue) for k in check_members
+               for c in ('ex', 'hz'))
     for s in sims:
         s.close()
 
@@ -616,22 +625,25 @@ def batch_record(a, n_models, steps, warmup, check_members=(0, 21, 42)):
                    'models': n_models, 'cells_total': total,
                    'nx_range': [int(min(nx)), int(max(nx))], 'nz_range': [int(min(nz)), int(max(nz))],
                    'l2': 'inputs larger than L2 (fields of all models)',
-                   'batched': ('every model on its own stream, its default kernel, side by side'
-                               if mode == 'streams' else
-                               'split step of every model per launch, 64-step graph chunks'),
-                   'modes_ms_per_step': {'split': round(ms_split / steps, 4),
-                                         'streams': round(ms_streams / steps, 4)}},
+                   'batched': {'streams': 'every model on its own stream, its default kernel, side by side',
+                               'split': 'split step of every model per launch, 64-step graph chunks',
+                               'queue': 'one persistent launch per step walking a tile queue over every '
+                                        "model's fused step (interior and shell z-march tiles), then one "
+                                        'phasor launch; 64-step graph chunks'}[mode],
+                   'modes_ms_per_step': {k: round(v / steps, 4) for k, v in times.items()}},
         'sequential': {'value': round(seq_value, 1), 'ms_per_step': round(ms_s / steps, 4),
                        'kernel': 'each model alone, its default kernel, one shared stream'},
         'speedup_vs_sequential': round(ms_s / ms_b, 3),
         'members_equal_sequential': {'members': check_members, 'fields': ['ex', 'hz'],
-                                     'modes': ['split', 'streams'], 'bit_exact': bool(same)},
+                                     'modes': ['split', 'streams', 'queue'], 'bit_exact': bool(same)},
         'roofline': {'bound': 'hbm', 'achieved': round(achieved, 1), 'peak': peak, 'unit': 'GB/s',
                      'frac': round(achieved / peak, 4), 'traffic': None, 'peak_source': peak_kind,
-                     'kernel': 'fused_step (member streams)' if mode == 'streams' else 'batch_split_step'},
+                     'kernel': {'streams': 'fused_step (member streams)', 'split': 'batch_split_step',
+                                'queue': 'batch_queue'}[mode]},
         'cpu_baseline': None, 'e2e': None,
-        'gpu_launches': (sum(step_launches(c) for c in choices) * steps
-                         if mode == 'streams' else 3 * steps + 1 + (steps + 63) // 64),
+        'gpu_launches': {'streams': sum(step_launches(c) for c in choices) * steps,
+                         'split': 3 * steps + 1,
+                         'queue': 2 * steps + 1}[mode],
         'clocks': clk,
     }
 

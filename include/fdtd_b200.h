@@ -72,6 +72,17 @@ extern "C" {
                                     all members */
 #define FDTD_OPT_SHELL        11 /* how the fused step updates the shell around
                                     its interior box: FDTD_SHELL_* */
+#define FDTD_OPT_BATCH_MODE   12 /* fdtd_batch_set_option: FDTD_BATCH_* */
+
+/* batched sweep (fdtd_batch_set_option(FDTD_OPT_BATCH_MODE, ...)) */
+#define FDTD_BATCH_SPLIT   0   /* (default) one launch per pass (H, E, phasors)
+                                  for all members, in place */
+#define FDTD_BATCH_STREAMS 1   /* every member's own step path on its own
+                                  stream, side by side */
+#define FDTD_BATCH_QUEUE   2   /* one persistent launch per step walks a tile
+                                  queue over every member's fused step
+                                  (interior and shell z-march tiles), then
+                                  one phasor launch */
 
 /* shell of the fused step (fdtd_set_option(FDTD_OPT_SHELL, ...)) */
 #define FDTD_SHELL_MARCH 0   /* fused z-marches with the CPML faces, edges and

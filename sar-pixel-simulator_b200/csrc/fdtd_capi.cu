@@ -90,6 +90,10 @@ struct fdtd_sim {
   cudaStream_t copy = nullptr;
   cudaEvent_t copy_ev[2] = {nullptr, nullptr};
   void* stage[2] = {nullptr, nullptr};
+  // device staging of fdtd_run_streamed: one packed group of planes per
+  // slot, re-pitched into the incident buffers on the copy stream
+  void* dstage = nullptr;
+  size_t dstage_bytes = 0;
   // packed (nz, ny, nx) device copy of a host volume, re-pitched on the
   // device by upload_volume (created on first use)
   void* packed = nullptr;
@@ -153,8 +157,21 @@ struct fdtd_batch {
   int graph_chunk = 64;
   cudaGraphExec_t gexec = nullptr;
   int gexec_chunk = 0;
-  bool streams = false;            // FDTD_OPT_BATCH_STREAMS: members on their own streams
+  int mode = FDTD_BATCH_SPLIT;     // FDTD_OPT_BATCH_MODE
   std::vector<cudaEvent_t> mev;    // one per member: the end of its work in a streams run
+  // FDTD_BATCH_QUEUE: per member a State for each step parity (2 n
+  // entries: source = current set, then the other), the members' fused
+  // plans, the tile list, its counter, the phasor blocks and the graph
+  void* d_qtab = nullptr;
+  QueueMember* d_qm = nullptr;
+  QueueTile* d_tiles = nullptr;
+  int* d_counter = nullptr;
+  int* d_qstart_ph = nullptr;
+  int ntiles = 0, qblocks = 0, qblocks_ph = 0;
+  std::vector<int> qsig;
+  bool qtable_ok = false;
+  cudaGraphExec_t qgexec = nullptr;
+  int qgexec_chunk = 0;
 };
 
 namespace {
@@ -838,6 +855,20 @@ int fdtd_run_streamed(fdtd_sim* s, int nsteps, const void* ex, const void* ey, c
     for (int k = 0; k < 2; ++k) CK(cudaHostAlloc(&s->stage[k], 4 * hb * chunk, cudaHostAllocDefault));
     s->stage_bytes = 4 * hb * chunk;
   }
+  // Each group's planes cross as one contiguous transfer per component into
+  // a device staging slot, then a kernel on the copy stream re-pitches them
+  // into the incident buffers (pitched 2-D transfers of short rows ran well
+  // below the link's bandwidth). A slot is reused two groups later, after
+  // its re-pitch (same stream). Without room for the slots, 2-D transfers.
+  const size_t dslot = 4 * hb * chunk;
+  if (!s->dstage && alloc(s, 2 * dslot, &s->dstage) == FDTD_OK) s->dstage_bytes = 2 * dslot;
+  if (s->dstage && s->dstage_bytes < 2 * dslot) {
+    release(s, s->dstage);
+    s->dstage = nullptr;
+    s->dstage_bytes = 0;
+    if (alloc(s, 2 * dslot, &s->dstage) == FDTD_OK) s->dstage_bytes = 2 * dslot;
+  }
+  cudaGetLastError();
   // the first group is short, so that the stepping starts early
   for (int c0 = t0, slot = 0, grp = std::min(2, chunk); c0 < t1; c0 += grp, slot ^= 1, grp = chunk) {
     const int n = std::min(grp, t1 - c0);
@@ -852,8 +883,18 @@ int fdtd_run_streamed(fdtd_sim* s, int nsteps, const void* ex, const void* ey, c
           memcpy(st, from, np * hb);
           from = st;
         }
-        CK(cudaMemcpy2DAsync(static_cast<unsigned char*>(s->inc[c]) + (size_t)c0 * pb, (size_t)s->pitch * s->esz,
-                             from, row, row, (size_t)g.ny * np, cudaMemcpyHostToDevice, s->copy));
+        unsigned char* to = static_cast<unsigned char*>(s->inc[c]) + (size_t)c0 * pb;
+        if (s->dstage) {
+          unsigned char* d = static_cast<unsigned char*>(s->dstage) + slot * dslot + (size_t)c * hb * chunk;
+          CK(cudaMemcpyAsync(d, from, np * hb, cudaMemcpyHostToDevice, s->copy));
+          if (g.dtype == FDTD_F32)
+            launch_repitch<float>((float*)to, (const float*)d, g.nx, (long long)g.ny * np, s->pitch, s->copy);
+          else
+            launch_repitch<double>((double*)to, (const double*)d, g.nx, (long long)g.ny * np, s->pitch, s->copy);
+        } else {
+          CK(cudaMemcpy2DAsync(to, (size_t)s->pitch * s->esz, from, row, row, (size_t)g.ny * np,
+                               cudaMemcpyHostToDevice, s->copy));
+        }
       }
       CK(cudaEventRecord(s->copy_ev[slot], s->copy));
       CK(cudaStreamWaitEvent(s->stream, s->copy_ev[slot], 0));
@@ -1156,7 +1197,169 @@ int batch_run(fdtd_batch* b, int nsteps) {
   return FDTD_OK;
 }
 
-// FDTD_OPT_BATCH_STREAMS: every member advances by its own step path (its
+// FDTD_BATCH_QUEUE: the tiles of every member's fused step, longest first
+// (interior z chunks of kQueueZChunk planes; the shell march's boxes as the
+// fused plan cuts them), and per member a State for each parity of the
+// step within a run (parity 0 reads the member's current set).
+constexpr int kQueueZChunk = 32;
+constexpr double kMarchTileCost = 3.0;   // a shell-march cell costs about 3 interior cells
+
+template <class T>
+int batch_build_queue(fdtd_batch* b) {
+  const int n = (int)b->sims.size();
+  std::vector<BatchModel<T>> tab(2 * (size_t)n);
+  std::vector<QueueMember> qm(n);
+  std::vector<QueueTile> tiles;
+  std::vector<double> cost;
+  std::vector<int> start_ph(n + 1);
+  long long blk_ph = 0;
+  for (int m = 0; m < n; ++m) {
+    fdtd_sim* s = b->sims[m];
+    const fdtd_geometry& g = s->g;
+    const int ph_n = std::max(s->ny_ph * s->nx_ph, std::max(s->nz_ph * s->ny_ph, s->nz_ph * s->nx_ph));
+    for (int p = 0; p < 2; ++p) {
+      const int src = p == 0 ? s->cur : 1 - s->cur;
+      BatchModel<T>& bm = tab[(size_t)p * n + m];
+      memset(&bm, 0, sizeof(bm));
+      bm.s = make_state<T>(s, src, 1 - src);
+      bm.tdev = s->tdev;
+      bm.ph_n = ph_n;
+    }
+    const FusedPlan plan = make_fused_plan(g.nx, g.ny, g.nz, g.npml, g.tfsf_z, 4, kQueueZChunk, false, true);
+    if (plan.mshell.dropped) return fail(FDTD_ERR_INVALID, "member %d: too many shell boxes", m);
+    QueueMember& q = qm[m];
+    memset(&q, 0, sizeof(q));
+    q.has_interior = plan.has_interior;
+    q.ib = plan.interior;
+    q.mb = plan.mshell;
+    if (plan.has_interior) {
+      const InteriorBox& ib = plan.interior;
+      const int gx = (ib.xb - ib.xa + 127) / 128, gy = (ib.yb - ib.ya + 3) / 4;
+      for (int c = 0; c < ib.chunks; ++c) {
+        const int k = c < ib.chunks0 ? 0 : 1, cc = k ? c - ib.chunks0 : c;
+        const int z0 = ib.z0[k] + cc * ib.zchunk, z1 = std::min(ib.z1[k], z0 + ib.zchunk);
+        for (int by = 0; by < gy; ++by)
+          for (int bx = 0; bx < gx; ++bx) {
+            tiles.push_back({m, 0, 0, bx, by, c});
+            cost.push_back(512.0 * (z1 - z0 + 1));
+          }
+      }
+    }
+    for (int k = 0; k < q.mb.n; ++k) {
+      const MarchBox& mb = q.mb.b[k];
+      const double own = (double)(mb.width - 1) * 4 * (kMarchThreads / mb.width - 1);
+      for (int c = 0; c < mb.nchunks; ++c) {
+        const int z0 = mb.z0 + c * mb.zchunk, z1 = std::min(mb.z1, z0 + mb.zchunk);
+        for (int by = 0; by < mb.gy; ++by)
+          for (int bx = 0; bx < mb.gx; ++bx) {
+            tiles.push_back({m, 1, k, bx, by, c});
+            cost.push_back(kMarchTileCost * own * (z1 - z0 + 1));
+          }
+      }
+    }
+    start_ph[m] = (int)blk_ph;
+    blk_ph += 6LL * ((ph_n + 255) / 256);
+    if (tiles.size() > (size_t)INT32_MAX / 2 || blk_ph > INT32_MAX) return fail(FDTD_ERR_INVALID, "batch too large");
+  }
+  start_ph[n] = (int)blk_ph;
+  // longest first: the long tiles start early, the short ones fill the end
+  std::vector<int> order(tiles.size());
+  for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost[x] > cost[y]; });
+  std::vector<QueueTile> sorted(tiles.size());
+  for (size_t i = 0; i < order.size(); ++i) sorted[i] = tiles[order[i]];
+  const size_t tab_bytes = sizeof(BatchModel<T>) * 2 * (size_t)n;
+  if (!b->d_qtab) {
+    CK(cudaMalloc(&b->d_qtab, tab_bytes));
+    CK(cudaMalloc(&b->d_qm, sizeof(QueueMember) * n));
+    CK(cudaMalloc(&b->d_qstart_ph, sizeof(int) * (n + 1)));
+    CK(cudaMalloc(&b->d_counter, sizeof(int)));
+  }
+  if (b->d_tiles && (int)sorted.size() != b->ntiles) {
+    cudaFree(b->d_tiles);
+    b->d_tiles = nullptr;
+  }
+  if (!b->d_tiles) CK(cudaMalloc(&b->d_tiles, sizeof(QueueTile) * std::max<size_t>(sorted.size(), 1)));
+  CK(cudaMemcpy(b->d_qtab, tab.data(), tab_bytes, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(b->d_qm, qm.data(), sizeof(QueueMember) * n, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(b->d_tiles, sorted.data(), sizeof(QueueTile) * sorted.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(b->d_qstart_ph, start_ph.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
+  CK(cudaMemset(b->d_counter, 0, sizeof(int)));
+  b->ntiles = (int)sorted.size();
+  b->qblocks_ph = (int)blk_ph;
+  int sms = 0;
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device));
+  const int per_sm = batch_queue_blocks_per_sm<T>();
+  if (per_sm < 1) return fail(FDTD_ERR_CUDA, "tile-queue kernel does not fit on an SM");
+  b->qblocks = std::max(1, std::min(b->ntiles, per_sm * sms));
+  b->qsig.resize(n);
+  for (int m = 0; m < n; ++m) b->qsig[m] = b->sims[m]->cur;
+  b->qtable_ok = true;
+  if (b->qgexec) { cudaGraphExecDestroy(b->qgexec); b->qgexec = nullptr; }
+  return FDTD_OK;
+}
+
+template <class T>
+void batch_queue_enqueue(fdtd_batch* b, int nsteps) {
+  const int n = (int)b->sims.size();
+  const auto* tab = static_cast<const BatchModel<T>*>(b->d_qtab);
+  for (int k = 0; k < nsteps; ++k) {
+    const BatchModel<T>* bm = tab + (size_t)(k & 1) * n;
+    launch_batch_queue<T>(bm, b->d_qm, b->d_tiles, b->ntiles, b->d_counter, b->qblocks, k, b->stream);
+    launch_batch_phasors<T>(bm, b->d_qstart_ph, n, b->qblocks_ph, k, b->d_counter, b->stream);
+  }
+  launch_batch_advance<T>(tab, n, nsteps, b->stream);
+}
+
+template <class T>
+int batch_run_queue(fdtd_batch* b, int nsteps) {
+  bool stale = !b->qtable_ok;
+  for (size_t m = 0; m < b->sims.size(); ++m) stale = stale || b->qsig[m] != b->sims[m]->cur;
+  if (stale) {
+    int rc = batch_build_queue<T>(b);
+    if (rc) return rc;
+  }
+  for (fdtd_sim* s : b->sims) {
+    CK(cudaEventRecord(b->ev, s->stream));
+    CK(cudaStreamWaitEvent(b->stream, b->ev, 0));
+  }
+  int left = nsteps;
+  // an even chunk leaves every member on its starting set, so each replay
+  // starts at parity 0 again
+  const int chunk = b->graph_chunk & ~1;
+  if (chunk > 0 && left >= chunk) {
+    if (!b->qgexec || b->qgexec_chunk != chunk) {
+      if (b->qgexec) { cudaGraphExecDestroy(b->qgexec); b->qgexec = nullptr; }
+      cudaGraph_t g = nullptr;
+      CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+      batch_queue_enqueue<T>(b, chunk);
+      cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+      if (e != cudaSuccess) return fail(FDTD_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+      e = cudaGraphInstantiate(&b->qgexec, g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) {
+        b->qgexec = nullptr;
+        return fail(FDTD_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+      }
+      b->qgexec_chunk = chunk;
+    }
+    while (left >= chunk) {
+      CK(cudaGraphLaunch(b->qgexec, b->stream));
+      left -= chunk;
+    }
+  }
+  if (left > 0) batch_queue_enqueue<T>(b, left);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(b->ev, b->stream));
+  for (fdtd_sim* s : b->sims) {
+    CK(cudaStreamWaitEvent(s->stream, b->ev, 0));
+    s->t += nsteps;
+    if (nsteps & 1) s->cur = 1 - s->cur;
+  }
+  return FDTD_OK;
+}
+
+// FDTD_BATCH_STREAMS: every member advances by its own step path (its
 // kernel choice, its graph chunks) on its own stream, forked from the batch
 // stream after the batch's earlier work and joined back into it, so that the
 // members' small launches run side by side on the device. Each member's
@@ -1228,6 +1431,12 @@ int fdtd_batch_destroy(fdtd_batch* b) {
   if (b->d_models) cudaFree(b->d_models);
   if (b->d_start) cudaFree(b->d_start);
   if (b->d_start_ph) cudaFree(b->d_start_ph);
+  if (b->qgexec) cudaGraphExecDestroy(b->qgexec);
+  if (b->d_qtab) cudaFree(b->d_qtab);
+  if (b->d_qm) cudaFree(b->d_qm);
+  if (b->d_tiles) cudaFree(b->d_tiles);
+  if (b->d_counter) cudaFree(b->d_counter);
+  if (b->d_qstart_ph) cudaFree(b->d_qstart_ph);
   if (b->ev) cudaEventDestroy(b->ev);
   for (cudaEvent_t ev : b->mev)
     if (ev) cudaEventDestroy(ev);
@@ -1241,7 +1450,13 @@ int fdtd_batch_set_option(fdtd_batch* b, int option, int value) {
   if (!b) return fail(FDTD_ERR_INVALID, "null batch handle");
   if (option == FDTD_OPT_BATCH_STREAMS) {
     if (value != 0 && value != 1) return fail(FDTD_ERR_INVALID, "batch streams must be 0 or 1");
-    b->streams = value == 1;
+    b->mode = value == 1 ? FDTD_BATCH_STREAMS : FDTD_BATCH_SPLIT;
+    return FDTD_OK;
+  }
+  if (option == FDTD_OPT_BATCH_MODE) {
+    if (value != FDTD_BATCH_SPLIT && value != FDTD_BATCH_STREAMS && value != FDTD_BATCH_QUEUE)
+      return fail(FDTD_ERR_INVALID, "unknown batch mode %d", value);
+    b->mode = value;
     return FDTD_OK;
   }
   if (option != FDTD_OPT_GRAPH_CHUNK) return fail(FDTD_ERR_INVALID, "unknown batch option %d", option);
@@ -1266,9 +1481,11 @@ int fdtd_batch_run(fdtd_batch* b, int nsteps) {
   if (nsteps == 0) return FDTD_OK;
   cudaError_t e = cudaSetDevice(b->device);
   if (e != cudaSuccess) return fail(FDTD_ERR_CUDA, "cudaSetDevice: %s", cudaGetErrorString(e));
-  if (b->streams)
+  if (b->mode == FDTD_BATCH_STREAMS)
     return b->dtype == FDTD_F32 ? batch_run_streams<float>(b, nsteps)
                                 : batch_run_streams<double>(b, nsteps);
+  if (b->mode == FDTD_BATCH_QUEUE)
+    return b->dtype == FDTD_F32 ? batch_run_queue<float>(b, nsteps) : batch_run_queue<double>(b, nsteps);
   return b->dtype == FDTD_F32 ? batch_run<float>(b, nsteps) : batch_run<double>(b, nsteps);
 }
 

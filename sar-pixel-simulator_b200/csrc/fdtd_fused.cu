@@ -39,15 +39,13 @@
 #include <cstring>
 
 #include "fdtd_launch.h"
-#include "fdtd_vec.cuh"
+#include "fdtd_tiles.cuh"
 
 namespace fdtd {
 
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
-constexpr int kLanes = 32;
-constexpr int kRowCells = kLanes * kVec;   // x cells of one tile row
 // z planes per block of the shell march (a box of up to 1.5 times this
 // height is one chunk)
 constexpr int kMarchZChunk = 48;
@@ -58,94 +56,11 @@ constexpr int interior_min_blocks() { return sizeof(T) == 4 && TY <= 8 ? 2 : 1; 
 template <class T, int TY>
 __global__ void __launch_bounds__(kLanes * (TY + 1), interior_min_blocks<T, TY>())
 k_fused_interior(const __grid_constant__ State<T> s, InteriorBox ib) {
-  using M = R<T>;
-  // E(z) of every thread row (read by the row below as its +y neighbour)
-  // and H^{n+1/2}(z) (read by the row above as its -y neighbour).
-  __shared__ __align__(32) T sEx[TY + 1][kRowCells];
-  __shared__ __align__(32) T sEz[TY + 1][kRowCells];
-  __shared__ __align__(32) T sHx[TY + 1][kRowCells];
-  __shared__ __align__(32) T sHz[TY + 1][kRowCells];
-
-  const int lane = threadIdx.x, r = threadIdx.y;
-  const int x0 = ib.xa + blockIdx.x * kRowCells + lane * kVec;
-  const int y = ib.ya + blockIdx.y * TY + r - 1;   // row 0 is the row below the tile
-  int c = blockIdx.z, k = 0;
-  if (c >= ib.chunks0) { c -= ib.chunks0; k = 1; }
-  const int z0 = ib.z0[k] + c * ib.zchunk;
-  const int z1 = min(ib.z1[k], z0 + ib.zchunk);
-  const int zs = z0 - 1;                           // plane below the chunk (interior)
-  // Rows from ya - 1 >= 0 up; rows past the grid and lanes past the pitch
-  // only feed the shared-memory exchange and the shuffles (as zeros).
-  const bool vin = x0 < s.pitch && y < s.ny;
-  const bool own = vin && r >= 1 && y < ib.yb && x0 < ib.xb;
-  const long long P = s.plane, W = s.pitch;
-  long long i = (long long)zs * P + (vin ? (long long)y * W + x0 : 0);
-  const int so = lane * kVec;
-
-  EVec<T> e;
-  HVec<T> h;
-  T ezz[kVec];   // Ez(z+1)
-  if (vin) { ld4(e.ex, s.iex + i); ld4(e.ey, s.iey + i); ld4(e.ez, s.iez + i); }
-  else { zero4(e.ex); zero4(e.ey); zero4(e.ez); }
-  zero4(h.hxz); zero4(h.hyz);
-
-  for (int z = zs; z < z1; ++z, i += P) {
-    const bool work = own && z >= z0;   // this thread updates and stores plane z
-    // ---- loads of plane z (z + 1 < nz: the interior ends npml planes below the top)
-    if (vin) {
-      ld4(e.exz, s.iex + i + P); ld4(e.eyz, s.iey + i + P); ld4(ezz, s.iez + i + P);
-      ld4(h.hx, s.ihx + i); ld4(h.hy, s.ihy + i); ld4(h.hz, s.ihz + i);
-    } else {
-      zero4(e.exz); zero4(e.eyz); zero4(ezz); zero4(h.hx); zero4(h.hy); zero4(h.hz);
-    }
-    T ca[kVec], cb[kVec];
-    if (work) { ld4(ca, s.ca + i); ld4(cb, s.cb + i); }
-    else { zero4(ca); zero4(cb); }
-    if (r == TY) {   // +y neighbour of the top row lies in the next tile
-      if (vin && y + 1 < s.ny) { ld4(e.exy, s.iex + i + W); ld4(e.ezy, s.iez + i + W); }
-      else { zero4(e.exy); zero4(e.ezy); }
-    }
-    T eyr = T(0), ezr = T(0);   // +x neighbour of lane 31 lies in the next tile
-    if (lane == kLanes - 1 && vin && x0 + kVec < s.pitch) { eyr = s.iey[i + kVec]; ezr = s.iez[i + kVec]; }
-    // lane 0: the source values that H^{n+1/2} at (z, y, x0 - 1) needs
-    // (x0 - 1 >= xa - 1 >= 0; z + 1 and y + 1 lie inside the grid)
-    T gx = T(0), gy = T(0), gz = T(0), gxz = T(0), gxy = T(0), ghy = T(0), ghz = T(0);
-    if (work && lane == 0) {
-      const long long j = i - 1;
-      gx = s.iex[j]; gy = s.iey[j]; gz = s.iez[j];
-      ghy = s.ihy[j]; ghz = s.ihz[j];
-      gxz = s.iex[j + P]; gxy = s.iex[j + W];
-    }
-    // ---- H^{n+1/2}(z) -----------------------------------------------------
-    st4(&sEx[r][so], e.ex);
-    st4(&sEz[r][so], e.ez);
-    __syncthreads();
-    if (r < TY) { ld4(e.exy, &sEx[r + 1][so]); ld4(e.ezy, &sEz[r + 1][so]); }
-    e.eyn = __shfl_down_sync(kFull, e.ey[0], 1);
-    e.ezn = __shfl_down_sync(kFull, e.ez[0], 1);
-    if (lane == kLanes - 1) { e.eyn = eyr; e.ezn = ezr; }
-    h_vec_interior(s, e, h.hx, h.hy, h.hz);
-    st4(&sHx[r][so], h.hx);
-    st4(&sHz[r][so], h.hz);
-    __syncthreads();
-    // ---- E^{n+1}(z) ---------------------------------------------------------
-    h.hyp = __shfl_up_sync(kFull, h.hy[kVec - 1], 1);
-    h.hzp = __shfl_up_sync(kFull, h.hz[kVec - 1], 1);
-    if (work) {
-      ld4(h.hxy, &sHx[r - 1][so]);
-      ld4(h.hzy, &sHz[r - 1][so]);
-      if (lane == 0) {   // Taflove 3.30 for hy, hz at x0 - 1 (an interior cell)
-        h.hyp = M::sub(ghy, M::mul(s.db, M::sub(M::sub(gxz, gx), M::sub(e.ez[0], gz))));
-        h.hzp = M::sub(ghz, M::mul(s.db, M::sub(M::sub(e.ey[0], gy), M::sub(gxy, gx))));
-      }
-      e_vec_interior(h, ca, cb, e.ex, e.ey, e.ez);
-      st4(s.ohx + i, h.hx); st4(s.ohy + i, h.hy); st4(s.ohz + i, h.hz);
-      st4(s.oex + i, e.ex); st4(s.oey + i, e.ey); st4(s.oez + i, e.ez);
-    }
-    // ---- next plane: E(z+1) becomes E(z), H^{n+1/2}(z) becomes H(z-1) -----
-    copy4(e.ex, e.exz); copy4(e.ey, e.eyz); copy4(e.ez, ezz);
-    copy4(h.hxz, h.hx); copy4(h.hyz, h.hy);
-  }
+  __shared__ __align__(32) T sEx[(TY + 1) * kRowCells];
+  __shared__ __align__(32) T sEz[(TY + 1) * kRowCells];
+  __shared__ __align__(32) T sHx[(TY + 1) * kRowCells];
+  __shared__ __align__(32) T sHz[(TY + 1) * kRowCells];
+  interior_tile<T, TY>(s, ib, threadIdx.x, threadIdx.y, blockIdx.x, blockIdx.y, blockIdx.z, sEx, sEz, sHx, sHz);
 }
 
 // The z slabs of the same x-y box: z in [0, npml) and [nz - npml, nz), one

@@ -24,6 +24,37 @@ void launch_batch_step(const BatchModel<T>* bm, const int* start, int n, int blo
                        const int* start_ph, int blocks_ph, int toff, cudaStream_t st);
 template <class T>
 void launch_batch_advance(const BatchModel<T>* bm, int n, int steps, cudaStream_t st);
+// The phasor pass of every model (one launch); with reset, block 0 first
+// zeroes *reset (the tile counter of the tile-queue step).
+template <class T>
+void launch_batch_phasors(const BatchModel<T>* bm, const int* start_ph, int n, int blocks_ph, int toff,
+                          int* reset, cudaStream_t st);
+
+// Batched tile-queue step (fdtd_batch.cu): per member its fused plan, as
+// tiles of the interior march (tile height 4) and of the shell march.
+struct QueueMember {
+  int has_interior;
+  InteriorBox ib;
+  MarchBoxes mb;
+};
+// One tile: member, kind (0 interior, 1 shell march), the shell box (kind
+// 1), the tile's x and y position in its box and its z chunk.
+struct QueueTile {
+  int member, kind, box, bx, by, c;
+};
+// Dynamic shared memory a block of the tile-queue kernel needs, and the
+// resident blocks per SM it reaches (0 on error).
+template <class T>
+size_t batch_queue_smem();
+template <class T>
+int batch_queue_blocks_per_sm();
+// One fused step of every member: `blocks` persistent blocks walk the tiles
+// (`ntiles` of them, longest first) through the counter, which must be zero
+// at the launch; bm holds each member's State of this step (source ->
+// destination set) and step counter.
+template <class T>
+void launch_batch_queue(const BatchModel<T>* bm, const QueueMember* qm, const QueueTile* tiles, int ntiles,
+                        int* counter, int blocks, int toff, cudaStream_t st);
 
 // Packed rows of nx elements into rows of `pitch` elements.
 template <class T>

@@ -263,8 +263,11 @@ __global__ void __launch_bounds__(128, split_min_blocks<T>()) k_batch_split(cons
 template <class T>
 __global__ void __launch_bounds__(256) k_batch_phasors(const BatchModel<T>* __restrict__ bm,
                                                        const int* __restrict__ start, int n,
-                                                       int toff) {
+                                                       int toff, int* __restrict__ reset) {
   const int bid = blockIdx.x;
+  // the tile counter of the step's tile-queue kernel, which has finished
+  // (stream order), starts the next step at zero
+  if (reset && bid == 0 && threadIdx.x == 0) *reset = 0;
   const int mi = find_model(start, n, bid);
   const BatchModel<T>& b = bm[mi];
   const int local = bid - start[mi];
@@ -358,7 +361,13 @@ void launch_batch_step(const BatchModel<T>* bm, const int* start, int n, int blo
                        const int* start_ph, int blocks_ph, int toff, cudaStream_t st) {
   k_batch_split<T, true><<<blocks, 128, 0, st>>>(bm, start, n, toff);
   k_batch_split<T, false><<<blocks, 128, 0, st>>>(bm, start, n, toff);
-  k_batch_phasors<T><<<blocks_ph, 256, 0, st>>>(bm, start_ph, n, toff);
+  k_batch_phasors<T><<<blocks_ph, 256, 0, st>>>(bm, start_ph, n, toff, nullptr);
+}
+
+template <class T>
+void launch_batch_phasors(const BatchModel<T>* bm, const int* start_ph, int n, int blocks_ph, int toff,
+                          int* reset, cudaStream_t st) {
+  k_batch_phasors<T><<<blocks_ph, 256, 0, st>>>(bm, start_ph, n, toff, reset);
 }
 
 template <class T>
@@ -442,6 +451,10 @@ template void launch_batch_step<float>(const BatchModel<float>*, const int*, int
                                        int, int, cudaStream_t);
 template void launch_batch_step<double>(const BatchModel<double>*, const int*, int, int,
                                         const int*, int, int, cudaStream_t);
+template void launch_batch_phasors<float>(const BatchModel<float>*, const int*, int, int, int, int*,
+                                          cudaStream_t);
+template void launch_batch_phasors<double>(const BatchModel<double>*, const int*, int, int, int, int*,
+                                           cudaStream_t);
 template void launch_batch_advance<float>(const BatchModel<float>*, int, int, cudaStream_t);
 template void launch_batch_advance<double>(const BatchModel<double>*, int, int, cudaStream_t);
 template void launch_phasors<float>(const State<float>&, const int*, int, cudaStream_t);

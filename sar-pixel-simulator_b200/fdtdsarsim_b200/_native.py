@@ -41,6 +41,10 @@ OPT_BATCH_STREAMS = 10
 OPT_SHELL = 11
 SHELL_MARCH = 0
 SHELL_SPLIT = 1
+OPT_BATCH_MODE = 12
+BATCH_SPLIT = 0
+BATCH_STREAMS = 1
+BATCH_QUEUE = 2
 
 TIME_STEP = 0
 TIME_PHASOR = 1
@@ -500,10 +504,12 @@ class Batch:
     """Several NativeSim members advanced together (fdtd_batch_*): by
     default one launch per pass for all members each step, chunks of steps
     replayed from a captured CUDA graph; with ``streams=True`` every member
-    runs its own step path on its own stream, side by side. Members keep
-    their own state and readback calls."""
+    runs its own step path on its own stream, side by side; with
+    ``mode=BATCH_QUEUE`` one persistent launch per step walks a tile queue
+    over every member's fused step. Members keep their own state and
+    readback calls."""
 
-    def __init__(self, sims, graph_chunk=None, streams=False):
+    def __init__(self, sims, graph_chunk=None, streams=False, mode=None):
         self.sims = list(sims)   # keeps the members alive while the batch exists
         arr = (_P * len(self.sims))(*[s.h for s in self.sims])
         self.h = _P()
@@ -512,6 +518,12 @@ class Batch:
             self.set_graph_chunk(graph_chunk)
         if streams:
             self.set_streams(True)
+        if mode is not None:
+            self.set_mode(mode)
+
+    def set_mode(self, mode):
+        """BATCH_SPLIT, BATCH_STREAMS or BATCH_QUEUE (FDTD_OPT_BATCH_MODE)."""
+        check(lib.fdtd_batch_set_option(self.h, OPT_BATCH_MODE, int(mode)))
 
     def set_graph_chunk(self, steps):
         check(lib.fdtd_batch_set_option(self.h, OPT_GRAPH_CHUNK, int(steps)))

@@ -136,3 +136,57 @@ def test_batch_rejects_bad_members():
     batch.close()
     a.close()
     assert a.h is None
+
+
+# members for the tile queue: uneven grids, two wide enough for an interior
+# box (x 32..), one with its injection plane in the upper CPML
+QUEUE_MODELS = MODELS + [(261, 45, 30, 14, 30, 16), (173, 53, 40, 28, 30, 20)]
+
+
+@pytest.mark.parametrize('chunk,calls', [(0, (30,)), (7, (30,)), (4, (3, 10, 17)), (64, (1, 29))])
+def test_queue_mode_matches_oracle_for_every_member(chunk, calls):
+    """FDTD_BATCH_QUEUE: one persistent launch per step walks the tiles of
+    every member's fused step (interior and shell z-march tiles, longest
+    first). Odd calls flip every member's current field set, even graph
+    chunks keep it; every member ends with the oracle's bits."""
+    members = _members(QUEUE_MODELS, seed=580)
+    batch = _native.Batch([s for _, s in members], graph_chunk=chunk, mode=_native.BATCH_QUEUE)
+    for n in calls:
+        batch.run(n)
+    batch.synchronize()
+    for orc, sim in members:
+        assert sim.step_index() == 30
+        _assert_member(orc, sim)
+    batch.close()
+    for _, sim in members:
+        sim.close()
+
+
+def test_queue_mode_interleaves_with_other_modes_and_own_steps():
+    """The tile queue after a member's own steps, between split-pass and
+    member-stream calls, in float32 and float64 members."""
+    for dtype, models in (('float32', QUEUE_MODELS), ('float64', MODELS[:2] + QUEUE_MODELS[-1:])):
+        members = _members(models, seed=600, dtype=dtype)
+        sims = [s for _, s in members]
+        for s in sims:
+            s.set_option(_native.OPT_KERNEL, _native.FDTD_KERNEL_FUSED)
+            s.run(1)
+        batch = _native.Batch(sims, graph_chunk=6, mode=_native.BATCH_QUEUE)
+        batch.run(9)
+        batch.set_mode(_native.BATCH_SPLIT)
+        batch.run(5)
+        batch.set_mode(_native.BATCH_QUEUE)
+        batch.run(8)
+        batch.set_mode(_native.BATCH_STREAMS)
+        batch.run(3)
+        batch.set_mode(_native.BATCH_QUEUE)
+        batch.run(4)
+        batch.synchronize()
+        for orc, sim in members:
+            assert sim.step_index() == 30
+            _assert_member(orc, sim)
+        with pytest.raises(_native.FdtdError):
+            batch.set_mode(3)
+        batch.close()
+        for s in sims:
+            s.close()
