@@ -1100,6 +1100,8 @@ namespace {
 
 template <class T>
 int batch_build_table(fdtd_batch* b) {
+  // the batch's earlier steps may still read the table: they finish first
+  CK(cudaStreamSynchronize(b->stream));
   const int n = (int)b->sims.size();
   std::vector<BatchModel<T>> tab(n);
   std::vector<int> start(n + 1), start_ph(n + 1);
@@ -1206,6 +1208,9 @@ constexpr double kMarchTileCost = 3.0;   // a shell-march cell costs about 3 int
 
 template <class T>
 int batch_build_queue(fdtd_batch* b) {
+  // the batch's earlier steps may still read the tables: they finish first
+  // (the blocking copies below do not wait for a non-blocking stream)
+  CK(cudaStreamSynchronize(b->stream));
   const int n = (int)b->sims.size();
   std::vector<BatchModel<T>> tab(2 * (size_t)n);
   std::vector<QueueMember> qm(n);
