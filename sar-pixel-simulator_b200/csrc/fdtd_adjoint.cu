@@ -90,8 +90,8 @@ __device__ __forceinline__ long long kz(const State<T>& s, int q, int y, int x) 
   return ((long long)q * s.ny + y) * s.pitch + x;
 }
 template <class T>
-__device__ __forceinline__ long long kx(const State<T>& s, int z, int y, int q) {
-  return ((long long)z * s.ny + y) * s.npml + q;
+__device__ __forceinline__ long long kx(const State<T>& s, int z, int y, int side, int q) {
+  return xpsi_index(s, z, y, side, side ? q + (s.nx - s.npml) : q);
 }
 template <class T>
 __device__ __forceinline__ long long ky(const State<T>& s, int z, int q, int x) {
@@ -329,7 +329,7 @@ __device__ __forceinline__ void h_own_vec(const State<T>& s, const Adj<T>& a, in
     for (int j = 0; j < kVec; ++j) {
       const int x = x0 + j;
       if (x >= nx - 1 || !h_face(x, nx, m, side, q)) continue;
-      const long long k = kx(s, z, y, q);
+      const long long k = kx(s, z, y, side, q);
       const T b = s.prof[side ? BH_U : BH_D][q];
       T* p3 = a.lps.x[side][3];
       T* p2 = a.lps.x[side][2];
@@ -469,7 +469,7 @@ __device__ __forceinline__ void e_to_h_vec(const State<T>& s, const Adj<T>& a, i
         xt1[p] = T(0);
         int side, q;
         if (z < nz - 1 && y < ny - 1 && xx < nx - 1 && e_face(xx, nx, m, side, q)) {
-          const long long k = kx(s, z, y, q);
+          const long long k = kx(s, z, y, side, q);
           const T c = s.prof[side ? CE_U : CE_D][q] * s.rdx;
           xt0[p] = c * (a.lps.x[side][0][k] - s.dx * fyv);
           xt1[p] = c * (a.lps.x[side][1][k] + s.dx * fzv);
@@ -578,7 +578,7 @@ __device__ __forceinline__ void e_own_vec(const State<T>& s, const Adj<T>& a, in
         for (int j = 0; j < kVec; ++j) {
           const int x = x0 + j;
           if (x >= nx - 1 || !e_face(x, nx, m, side, q)) continue;
-          const long long k = kx(s, z, y, q);
+          const long long k = kx(s, z, y, side, q);
           const T b = s.prof[side ? BE_U : BE_D][q];
           T* p1 = a.lps.x[side][1];
           T* p0 = a.lps.x[side][0];
@@ -713,7 +713,7 @@ __device__ __forceinline__ void h_to_e_vec(const State<T>& s, const Adj<T>& a, i
         xt3[p] = T(0);
         int side, q;
         if (xx >= 0 && z < nz - 1 && y < ny - 1 && xx < nx - 1 && h_face(xx, nx, m, side, q)) {
-          const long long k = kx(s, z, y, q);
+          const long long k = kx(s, z, y, side, q);
           const T c = s.prof[side ? CH_U : CH_D][q] * s.rdx;
           xt2[p] = c * (a.lps.x[side][2][k] + s.dtm0 * lyv);
           xt3[p] = c * (a.lps.x[side][3][k] - s.dtm0 * lzv);

@@ -207,6 +207,8 @@ State<T> make_state(const fdtd_sim* s, int src, int dst) {
   st.nx = g.nx; st.ny = g.ny; st.nz = g.nz; st.npml = g.npml; st.tfsf_z = g.tfsf_z;
   st.nt_inc = g.nt_inc;
   st.pitch = s->pitch;
+  st.xw = xpsi_width(g.npml);
+  st.xo1 = xpsi_origin_high(g.nx, g.npml);
   st.plane = s->plane;
   st.db = (T)g.db; st.dtm0 = (T)g.dtm0; st.dte0dx = (T)g.dte0dx;
   st.dx = (T)g.cell_size;
@@ -498,10 +500,10 @@ int fdtd_create(const fdtd_geometry* geom, int device, fdtd_sim** out) {
   A(fb, &s->ca);
   A(fb, &s->cb);
   // psi layout within one set: z faces (npml, ny, pitch), x faces
-  // (nz, ny, npml), y faces (nz, npml, pitch); 4 components per face side
+  // (nz, ny, xw), y faces (nz, npml, pitch); 4 components per face side
   long long off = 0;
   const long long zsz = (long long)g.npml * g.ny * s->pitch;
-  const long long xsz = (long long)g.nz * g.ny * g.npml;
+  const long long xsz = (long long)g.nz * g.ny * xpsi_width(g.npml);
   const long long ysz = (long long)g.nz * g.npml * s->pitch;
   auto align32 = [](long long v) { return (v + 31) / 32 * 32; };
   for (int side = 0; side < 2; ++side)

@@ -88,7 +88,7 @@ __device__ __forceinline__ void h_cell(const State<T>& s, const ENbr<T>& e,
       if (side >= 0) {
         const T b = s.prof[side ? BH_U : BH_D][q];
         const T c = s.prof[side ? CH_U : CH_D][q];
-        const long long k = ((long long)z * ny + y) * m + q;
+        const long long k = xpsi_index(s, z, y, side, x);
         const T pzx = M::add(M::mul(b, s.ps.x[side][3][k]), div_dx(s, M::mul(c, dey_x)));
         const T pyx = M::add(M::mul(b, s.ps.x[side][2][k]), div_dx(s, M::mul(c, dez_x)));
         if (wpsi) { s.pd.x[side][3][k] = pzx; s.pd.x[side][2][k] = pyx; }
@@ -165,7 +165,7 @@ __device__ __forceinline__ void e_cell(const State<T>& s, const HNbr<T>& h,
       if (side >= 0) {
         const T b = s.prof[side ? BE_U : BE_D][q];
         const T c = s.prof[side ? CE_U : CE_D][q];
-        const long long k = ((long long)z * ny + y) * m + q;
+        const long long k = xpsi_index(s, z, y, side, x);
         const T pzx = M::add(M::mul(b, s.ps.x[side][1][k]), div_dx(s, M::mul(c, dhy_x)));
         const T pyx = M::add(M::mul(b, s.ps.x[side][0][k]), div_dx(s, M::mul(c, dhz_x)));
         if (wpsi) { s.pd.x[side][1][k] = pzx; s.pd.x[side][0][k] = pyx; }

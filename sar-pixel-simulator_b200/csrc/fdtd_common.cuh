@@ -38,8 +38,13 @@ enum { BE_D = 0, BH_D, CE_D, CH_D, BE_U, BH_U, CE_U, CH_U };
 
 // psi component slots per face.
 //   z faces (down/up):    0 Exz, 1 Eyz, 2 Hxz, 3 Hyz   shape (npml, ny, pitch)
-//   x faces (left/right): 0 Eyx, 1 Ezx, 2 Hyx, 3 Hzx   shape (nz, ny, npml)
+//   x faces (left/right): 0 Eyx, 1 Ezx, 2 Hyx, 3 Hzx   shape (nz, ny, xw)
 //   y faces (front/back): 0 Exy, 1 Ezy, 2 Hxy, 3 Hzy   shape (nz, npml, pitch)
+// An x-face row holds the cells x = xo + p, p < xw, with xo = 0 for the low
+// face and xo = (nx - npml) rounded down to a multiple of 4 for the high
+// face, xw = npml + 3 rounded up to a multiple of 4: every 4-cell vector
+// that touches an x face is one aligned vector of its row (slots of cells
+// outside the face are never read).
 // Side 0 is the low face (down/left/front), side 1 the high face.
 template <class T>
 struct Psi {
@@ -55,6 +60,7 @@ template <class T>
 struct State {
   int nx, ny, nz, npml, tfsf_z, nt_inc;
   int pitch;
+  int xw, xo1;       // x-face psi rows: width, first x of the high face's row
   long long plane;   // ny * pitch
   T db, dtm0, dte0dx, dx;
   T rdx;   // 1 / dx correctly rounded (host IEEE division)
@@ -183,6 +189,16 @@ __device__ __forceinline__ T div_const(T u, T d, T r) {
 
 template <class T>
 __device__ __forceinline__ T div_dx(const State<T>& s, T u) { return div_const(u, s.dx, s.rdx); }
+
+// Index of cell x of plane z, row y in an x-face psi array of side `side`.
+template <class T>
+__device__ __forceinline__ long long xpsi_index(const State<T>& s, int z, int y, int side, int x) {
+  return ((long long)z * s.ny + y) * s.xw + (x - (side ? s.xo1 : 0));
+}
+
+// Row width and high-face origin of the x-face psi arrays (host and device).
+__host__ __device__ constexpr int xpsi_width(int npml) { return (npml + 3 + 3) / 4 * 4; }
+__host__ __device__ constexpr int xpsi_origin_high(int nx, int npml) { return (nx - npml) / 4 * 4; }
 
 __global__ void k_advance(int* t, int n);
 

@@ -239,23 +239,28 @@ __device__ __forceinline__ void h_vec(const State<T>& s, const EVec<T>& e, int z
     }
     if (wpsi) { st4(s.pd.z[side][3] + k, p3); st4(s.pd.z[side][2] + k, p2); }
   }
-  // x faces (cpml_h_left/right, :285-324), per cell
-  if (zyb && (x0 < m - 1 || x0 + kVec - 1 >= nx - m)) {
+  // x faces (cpml_h_left/right, :285-324): the vector's psi is one aligned
+  // vector of the face's row (xpsi_index); cells outside the face keep
+  // their slot. A vector with no cell below nx - 1 has nothing to update.
+  if (zyb && x0 <= nx - 2 && (x0 < m - 1 || x0 + kVec - 1 >= nx - m)) {
+    const int side = x0 < m - 1 ? 0 : 1;   // no vector reaches both faces (nx >= 2 npml + 3)
+    const long long k = xpsi_index(s, z, y, side, x0);
+    T p3[kVec], p2[kVec];
+    ld4(p3, s.ps.x[side][3] + k);
+    ld4(p2, s.ps.x[side][2] + k);
 #pragma unroll
     for (int j = 0; j < kVec; ++j) {
       const int x = x0 + j;
-      if (!inb[j] || !(x < m - 1 || x >= nx - m)) continue;
-      const int side = x < m - 1 ? 0 : 1;
+      if (!inb[j] || !(side ? x >= nx - m : x < m - 1)) continue;
       const int q = side ? x - (nx - m) : x;
       const T b = s.prof[side ? BH_U : BH_D][q];
       const T c = s.prof[side ? CH_U : CH_D][q];
-      const long long k = ((long long)z * ny + y) * m + q;
-      const T pzx = M::add(M::mul(b, s.ps.x[side][3][k]), div_dx(s, M::mul(c, dey_x[j])));
-      const T pyx = M::add(M::mul(b, s.ps.x[side][2][k]), div_dx(s, M::mul(c, dez_x[j])));
-      if (wpsi) { s.pd.x[side][3][k] = pzx; s.pd.x[side][2][k] = pyx; }
-      hz[j] = M::sub(hz[j], M::mul(s.dtm0, pzx));
-      hy[j] = M::add(hy[j], M::mul(s.dtm0, pyx));
+      p3[j] = M::add(M::mul(b, p3[j]), div_dx(s, M::mul(c, dey_x[j])));   // psi_Hzx
+      p2[j] = M::add(M::mul(b, p2[j]), div_dx(s, M::mul(c, dez_x[j])));   // psi_Hyx
+      hz[j] = M::sub(hz[j], M::mul(s.dtm0, p3[j]));
+      hy[j] = M::add(hy[j], M::mul(s.dtm0, p2[j]));
     }
+    if (wpsi) { st4(s.pd.x[side][3] + k, p3); st4(s.pd.x[side][2] + k, p2); }
   }
   // y faces (cpml_h_front/back, :327-366)
   if (zyb && (y < m - 1 || y >= ny - m)) {
@@ -343,23 +348,27 @@ __device__ __forceinline__ void e_vec(const State<T>& s, const HVec<T>& h, const
     }
     if (wpsi) { st4(s.pd.z[side][1] + k, p1); st4(s.pd.z[side][0] + k, p0); }
   }
-  // x faces (cpml_e_left/right, :108-148), per cell
-  if (zyb && (x0 < m || x0 + kVec - 1 >= nx - m)) {
+  // x faces (cpml_e_left/right, :108-148): one aligned psi vector per
+  // face component, as for H
+  if (zyb && x0 <= nx - 2 && (x0 < m || x0 + kVec - 1 >= nx - m)) {
+    const int side = x0 < m ? 0 : 1;
+    const long long k = xpsi_index(s, z, y, side, x0);
+    T p1[kVec], p0[kVec];
+    ld4(p1, s.ps.x[side][1] + k);
+    ld4(p0, s.ps.x[side][0] + k);
 #pragma unroll
     for (int j = 0; j < kVec; ++j) {
       const int x = x0 + j;
-      if (!inb[j] || !((x >= 1 && x < m) || x >= nx - m)) continue;
-      const int side = (x >= 1 && x < m) ? 0 : 1;
+      if (!inb[j] || !(side ? x >= nx - m : (x >= 1 && x < m))) continue;
       const int q = side ? x - (nx - m) : x;
       const T b = s.prof[side ? BE_U : BE_D][q];
       const T c = s.prof[side ? CE_U : CE_D][q];
-      const long long k = ((long long)z * ny + y) * m + q;
-      const T pzx = M::add(M::mul(b, s.ps.x[side][1][k]), div_dx(s, M::mul(c, dhy_x[j])));
-      const T pyx = M::add(M::mul(b, s.ps.x[side][0][k]), div_dx(s, M::mul(c, dhz_x[j])));
-      if (wpsi) { s.pd.x[side][1][k] = pzx; s.pd.x[side][0][k] = pyx; }
-      ez[j] = M::add(ez[j], M::mul(cbdx[j], pzx));
-      ey[j] = M::sub(ey[j], M::mul(cbdx[j], pyx));
+      p1[j] = M::add(M::mul(b, p1[j]), div_dx(s, M::mul(c, dhy_x[j])));   // psi_Ezx
+      p0[j] = M::add(M::mul(b, p0[j]), div_dx(s, M::mul(c, dhz_x[j])));   // psi_Eyx
+      ez[j] = M::add(ez[j], M::mul(cbdx[j], p1[j]));
+      ey[j] = M::sub(ey[j], M::mul(cbdx[j], p0[j]));
     }
+    if (wpsi) { st4(s.pd.x[side][1] + k, p1); st4(s.pd.x[side][0] + k, p0); }
   }
   // y faces (cpml_e_front/back, :151-191)
   if (zyb && ((y >= 1 && y < m) || y >= ny - m)) {
