@@ -35,6 +35,8 @@ extern "C" {
 #define FDTD_ERR_STATE     3  /* call out of order (e.g. run before set_materials) */
 #define FDTD_ERR_NONFINITE 4  /* a NaN/Inf was detected in the fields */
 #define FDTD_ERR_NOMEM     5  /* device allocation failed */
+#define FDTD_ERR_BOUNDS    6  /* bounds-checked build only: a kernel access left
+                                 its allocation or array (it was skipped) */
 
 /* element types */
 #define FDTD_F32 0
@@ -291,6 +293,14 @@ int fdtd_batch_set_option(fdtd_batch *b, int option, int value);
 int fdtd_batch_run(fdtd_batch *b, int nsteps);
 int fdtd_batch_synchronize(fdtd_batch *b);
 int fdtd_batch_get_stream(fdtd_batch *b, void **stream);
+
+/* Diagnostic (no counterpart in the reference): 1 in the bounds-checked
+ * build of this library (libfdtd_b200_check.so: every global access of the
+ * step kernels is checked against the library's live allocations and every
+ * shared index against its array; a failed check skips the access and
+ * fdtd_synchronize / fdtd_batch_synchronize return FDTD_ERR_BOUNDS), 0 in
+ * the normal build. */
+int fdtd_bounds_check_enabled(void);
 
 /* Diagnostic (no counterpart in the reference): the CPML terms divide by
  * the cell size with a correctly rounded reciprocal and one FMA correction

@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include "fdtd_b200.h"
+#include "fdtd_check.cuh"
 #include "fdtd_launch.h"
 
 using namespace fdtd;
@@ -185,14 +186,30 @@ int alloc(fdtd_sim* s, size_t bytes, void** out) {
     return fail(FDTD_ERR_NOMEM, "cudaMalloc(%zu bytes) failed: %s", bytes, cudaGetErrorString(e));
   }
   s->bufs.push_back({p, bytes});
+  check_register(p, bytes);   // the bounds-checked build's allocation table
   *out = p;
   return FDTD_OK;
+}
+
+// A violation the bounds-checked build recorded since the last look, as
+// FDTD_ERR_BOUNDS (FDTD_OK in the normal build).
+int take_bounds_violation() {
+  unsigned long long n = 0, what = 0;
+  long long bytes = 0, line = 0;
+  if (check_take(&n, &what, &bytes, &line)) return fail(FDTD_ERR_CUDA, "bounds check word unreadable");
+  if (!n) return FDTD_OK;
+  if (bytes < 0)
+    return fail(FDTD_ERR_BOUNDS, "bounds check: %llu bad accesses; the first: shared index %lld (line %lld)", n,
+                (long long)what, line);
+  return fail(FDTD_ERR_BOUNDS, "bounds check: %llu bad accesses; the first: %lld bytes at address 0x%llx (line %lld)",
+              n, bytes, what, line);
 }
 
 void release(fdtd_sim* s, void* p) {
   if (!p) return;
   for (size_t i = 0; i < s->bufs.size(); ++i)
     if (s->bufs[i].p == p) {
+      check_unregister(p);
       cudaFree(p);
       s->bufs.erase(s->bufs.begin() + i);
       return;
@@ -586,7 +603,10 @@ int fdtd_destroy(fdtd_sim* s) {
                 s->batch_refs);
   cudaSetDevice(s->device);
   if (s->own) cudaStreamSynchronize(s->own);
-  for (auto& b : s->bufs) cudaFree(b.p);
+  for (auto& b : s->bufs) {
+    check_unregister(b.p);
+    cudaFree(b.p);
+  }
   if (s->side) cudaStreamSynchronize(s->side);
   if (s->copy) cudaStreamSynchronize(s->copy);
   for (int k = 0; k < 2; ++k) {
@@ -914,6 +934,7 @@ int fdtd_synchronize(fdtd_sim* s) {
   if (rc) return rc;
   CK(cudaStreamSynchronize(s->stream));
   CK(cudaGetLastError());
+  if ((rc = take_bounds_violation())) return rc;
   if (s->check_every > 0) {
     int f[2] = {0, 0};
     CK(cudaMemcpy(f, s->flags, sizeof(f), cudaMemcpyDeviceToHost));
@@ -1501,8 +1522,10 @@ int fdtd_batch_synchronize(fdtd_batch* b) {
   CK(cudaSetDevice(b->device));
   CK(cudaStreamSynchronize(b->stream));
   CK(cudaGetLastError());
-  return FDTD_OK;
+  return take_bounds_violation();
 }
+
+int fdtd_bounds_check_enabled(void) { return check_enabled() ? 1 : 0; }
 
 int fdtd_batch_get_stream(fdtd_batch* b, void** stream) {
   if (!b || !stream) return fail(FDTD_ERR_INVALID, "null argument");

@@ -125,14 +125,14 @@ k_fused_slab(const __grid_constant__ State<T> s, InteriorBox ib) {
       else { zero4(e.exy); zero4(e.ezy); }
     }
     T eyr = T(0), ezr = T(0);
-    if (lane == kLanes - 1 && vin && x0 + kVec < s.pitch) { eyr = s.iey[i + kVec]; ezr = s.iez[i + kVec]; }
+    if (lane == kLanes - 1 && vin && x0 + kVec < s.pitch) { eyr = ldc(s.iey + (i + kVec)); ezr = ldc(s.iez + (i + kVec)); }
     T gx = T(0), gy = T(0), gz = T(0), gxz = T(0), gxy = T(0), ghy = T(0), ghz = T(0), gpy = T(0);
     if (work && lane == 0) {
       const long long j = i - 1;
-      gx = s.iex[j]; gy = s.iey[j]; gz = s.iez[j];
-      ghy = s.ihy[j]; ghz = s.ihz[j];
-      gxz = top ? T(0) : s.iex[j + P];
-      gxy = s.iex[j + W];
+      gx = ldc(s.iex + (j)); gy = ldc(s.iey + (j)); gz = ldc(s.iez + (j));
+      ghy = ldc(s.ihy + (j)); ghz = ldc(s.ihz + (j));
+      gxz = top ? T(0) : ldc(s.iex + (j + P));
+      gxy = ldc(s.iex + (j + W));
       if (hf) gpy = s.ps.z[hside][3][((long long)hq * s.ny + y) * W + x0 - 1];
     }
     // ---- H^{n+1/2}(z) -----------------------------------------------------

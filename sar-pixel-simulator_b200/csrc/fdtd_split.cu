@@ -52,8 +52,8 @@ __device__ __forceinline__ void h_split_vec(const State<T>& s, int t, int z, int
   e.ezn = __shfl_down_sync(0xffffffffu, e.ez[0], 1, width);
   if (lane == width - 1) {
     const bool ok = vin && x0 + kVec < s.nx;
-    e.eyn = ok ? s.iey[i + kVec] : T(0);
-    e.ezn = ok ? s.iez[i + kVec] : T(0);
+    e.eyn = ok ? ldc(s.iey + (i + kVec)) : T(0);
+    e.ezn = ok ? ldc(s.iez + (i + kVec)) : T(0);
   }
   if (!(act && vin)) return;
   if (interior(s, z, y, x0, t)) h_vec_interior(s, e, hx, hy, hz);
@@ -88,8 +88,8 @@ __device__ __forceinline__ void e_split_vec(const State<T>& s, int t, int z, int
   h.hzp = __shfl_up_sync(0xffffffffu, h.hz[kVec - 1], 1, width);
   if (lane == 0) {
     const bool ok = vin && x0 >= 1;
-    h.hyp = ok ? s.ihy[i - 1] : T(0);
-    h.hzp = ok ? s.ihz[i - 1] : T(0);
+    h.hyp = ok ? ldc(s.ihy + (i - 1)) : T(0);
+    h.hzp = ok ? ldc(s.ihz + (i - 1)) : T(0);
   }
   if (!(act && vin)) return;
   if (interior(s, z, y, x0, t)) e_vec_interior(h, ca, cb, ex, ey, ez);
@@ -140,17 +140,18 @@ __device__ __forceinline__ void ph_acc(const State<T>& s, int plane, long long k
   T* p = s.ph + s.ph_off[plane] + 2 * k;
   if (!s.kahan) {
     // float64 sum of the stored value and the float64 term, rounded to T
-    p[0] = M::from_double(__dadd_rn((double)p[0], __dmul_rn(m, c)));
-    p[1] = M::from_double(__dadd_rn((double)p[1], __dmul_rn(m, sn)));
+    stc(p, M::from_double(__dadd_rn((double)ldc(p), __dmul_rn(m, c))));
+    stc(p + 1, M::from_double(__dadd_rn((double)ldc(p + 1), __dmul_rn(m, sn))));
   } else {
     T* pc = s.phc + s.ph_off[plane] + 2 * k;
 #pragma unroll
     for (int j = 0; j < 2; ++j) {
       const T term = M::from_double(__dmul_rn(m, j ? sn : c));
-      const T yv = M::sub(term, pc[j]);
-      const T tv = M::add(p[j], yv);
-      pc[j] = M::sub(M::sub(tv, p[j]), yv);
-      p[j] = tv;
+      const T yv = M::sub(term, ldc(pc + j));
+      const T pj = ldc(p + j);
+      const T tv = M::add(pj, yv);
+      stc(pc + j, M::sub(M::sub(tv, pj), yv));
+      stc(p + j, tv);
     }
   }
 }
@@ -187,26 +188,26 @@ __device__ __forceinline__ void phasor_cell(const State<T>& s, int g, int idx, i
     const int pz = g == 0 ? m + 1 : s.nz - m - 1;
     const long long i = pz * P + (long long)(m + a) * W + (m + b);
     const int base = g * 4;  // ex, ey, hx, hy
-    ph_acc(s, base + 0, k, mean2(ex[i], ex[i - 1]), cE, sE);
-    ph_acc(s, base + 1, k, mean2(ey[i], ey[i - W]), cE, sE);
-    ph_acc(s, base + 2, k, mean4(hx[i], hx[i - W], hx[i - P], hx[i - P - W]), cH, sH);
-    ph_acc(s, base + 3, k, mean4(hy[i], hy[i - 1], hy[i - P], hy[i - P - 1]), cH, sH);
+    ph_acc(s, base + 0, k, mean2(ldc(ex + i), ldc(ex + i - 1)), cE, sE);
+    ph_acc(s, base + 1, k, mean2(ldc(ey + i), ldc(ey + i - W)), cE, sE);
+    ph_acc(s, base + 2, k, mean4(ldc(hx + i), ldc(hx + i - W), ldc(hx + i - P), ldc(hx + i - P - W)), cH, sH);
+    ph_acc(s, base + 3, k, mean4(ldc(hy + i), ldc(hy + i - 1), ldc(hy + i - P), ldc(hy + i - P - 1)), cH, sH);
   } else if (g < 4) {
     const int px = g == 2 ? m + 1 : s.nx - m - 1;
     const long long i = (long long)(m + a) * P + (long long)(m + b) * W + px;
     const int base = 8 + (g - 2) * 4;  // ey, ez, hy, hz
-    ph_acc(s, base + 0, k, mean2(ey[i], ey[i - W]), cE, sE);
-    ph_acc(s, base + 1, k, mean2(ez[i], ez[i - P]), cE, sE);
-    ph_acc(s, base + 2, k, mean4(hy[i], hy[i - 1], hy[i - P], hy[i - P - 1]), cH, sH);
-    ph_acc(s, base + 3, k, mean4(hz[i], hz[i - 1], hz[i - W], hz[i - W - 1]), cH, sH);
+    ph_acc(s, base + 0, k, mean2(ldc(ey + i), ldc(ey + i - W)), cE, sE);
+    ph_acc(s, base + 1, k, mean2(ldc(ez + i), ldc(ez + i - P)), cE, sE);
+    ph_acc(s, base + 2, k, mean4(ldc(hy + i), ldc(hy + i - 1), ldc(hy + i - P), ldc(hy + i - P - 1)), cH, sH);
+    ph_acc(s, base + 3, k, mean4(ldc(hz + i), ldc(hz + i - 1), ldc(hz + i - W), ldc(hz + i - W - 1)), cH, sH);
   } else {
     const int py = g == 4 ? m + 1 : s.ny - m - 1;
     const long long i = (long long)(m + a) * P + (long long)py * W + (m + b);
     const int base = 16 + (g - 4) * 4;  // ex, ez, hx, hz
-    ph_acc(s, base + 0, k, mean2(ex[i], ex[i - 1]), cE, sE);
-    ph_acc(s, base + 1, k, mean2(ez[i], ez[i - P]), cE, sE);
-    ph_acc(s, base + 2, k, mean4(hx[i], hx[i - W], hx[i - P], hx[i - P - W]), cH, sH);
-    ph_acc(s, base + 3, k, mean4(hz[i], hz[i - W], hz[i - 1], hz[i - W - 1]), cH, sH);
+    ph_acc(s, base + 0, k, mean2(ldc(ex + i), ldc(ex + i - 1)), cE, sE);
+    ph_acc(s, base + 1, k, mean2(ldc(ez + i), ldc(ez + i - P)), cE, sE);
+    ph_acc(s, base + 2, k, mean4(ldc(hx + i), ldc(hx + i - W), ldc(hx + i - P), ldc(hx + i - P - W)), cH, sH);
+    ph_acc(s, base + 3, k, mean4(ldc(hz + i), ldc(hz + i - W), ldc(hz + i - 1), ldc(hz + i - W - 1)), cH, sH);
   }
 }
 

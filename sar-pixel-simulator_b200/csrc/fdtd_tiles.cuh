@@ -40,6 +40,10 @@ __device__ __forceinline__ void interior_tile(const State<T>& s, const InteriorB
   const long long P = s.plane, W = s.pitch;
   long long i = (long long)zs * P + (vin ? (long long)y * W + x0 : 0);
   const int so = lane * kVec;
+  // shared indices of this thread (checked build: a bad one skips the
+  // thread's shared accesses; the constant true otherwise)
+  const bool sm_ok = FDTD_CHECK_SMEM(r * kRowCells + so + kVec - 1, (TY + 1) * kRowCells) &&
+                     FDTD_CHECK_SMEM(r * kRowCells + so, (TY + 1) * kRowCells);
 
   EVec<T> e;
   HVec<T> h;
@@ -65,34 +69,35 @@ __device__ __forceinline__ void interior_tile(const State<T>& s, const InteriorB
       else { zero4(e.exy); zero4(e.ezy); }
     }
     T eyr = T(0), ezr = T(0);   // +x neighbour of lane 31 lies in the next tile
-    if (lane == kLanes - 1 && vin && x0 + kVec < s.pitch) { eyr = s.iey[i + kVec]; ezr = s.iez[i + kVec]; }
+    if (lane == kLanes - 1 && vin && x0 + kVec < s.pitch) { eyr = ldc(s.iey + (i + kVec)); ezr = ldc(s.iez + (i + kVec)); }
     // lane 0: the source values that H^{n+1/2} at (z, y, x0 - 1) needs
     // (x0 - 1 >= xa - 1 >= 0; z + 1 and y + 1 lie inside the grid)
     T gx = T(0), gy = T(0), gz = T(0), gxz = T(0), gxy = T(0), ghy = T(0), ghz = T(0);
     if (work && lane == 0) {
       const long long j = i - 1;
-      gx = s.iex[j]; gy = s.iey[j]; gz = s.iez[j];
-      ghy = s.ihy[j]; ghz = s.ihz[j];
-      gxz = s.iex[j + P]; gxy = s.iex[j + W];
+      gx = ldc(s.iex + (j)); gy = ldc(s.iey + (j)); gz = ldc(s.iez + (j));
+      ghy = ldc(s.ihy + (j)); ghz = ldc(s.ihz + (j));
+      gxz = ldc(s.iex + (j + P)); gxy = ldc(s.iex + (j + W));
     }
     // ---- H^{n+1/2}(z) -----------------------------------------------------
-    st4(&sEx[r * kRowCells + so], e.ex);
-    st4(&sEz[r * kRowCells + so], e.ez);
+    if (sm_ok) { st4(&sEx[r * kRowCells + so], e.ex); st4(&sEz[r * kRowCells + so], e.ez); }
     __syncthreads();
-    if (r < TY) { ld4(e.exy, &sEx[(r + 1) * kRowCells + so]); ld4(e.ezy, &sEz[(r + 1) * kRowCells + so]); }
+    if (r < TY) {
+      if (sm_ok) { ld4(e.exy, &sEx[(r + 1) * kRowCells + so]); ld4(e.ezy, &sEz[(r + 1) * kRowCells + so]); }
+      else { zero4(e.exy); zero4(e.ezy); }
+    }
     e.eyn = __shfl_down_sync(kFullMask, e.ey[0], 1);
     e.ezn = __shfl_down_sync(kFullMask, e.ez[0], 1);
     if (lane == kLanes - 1) { e.eyn = eyr; e.ezn = ezr; }
     h_vec_interior(s, e, h.hx, h.hy, h.hz);
-    st4(&sHx[r * kRowCells + so], h.hx);
-    st4(&sHz[r * kRowCells + so], h.hz);
+    if (sm_ok) { st4(&sHx[r * kRowCells + so], h.hx); st4(&sHz[r * kRowCells + so], h.hz); }
     __syncthreads();
     // ---- E^{n+1}(z) ---------------------------------------------------------
     h.hyp = __shfl_up_sync(kFullMask, h.hy[kVec - 1], 1);
     h.hzp = __shfl_up_sync(kFullMask, h.hz[kVec - 1], 1);
     if (work) {
-      ld4(h.hxy, &sHx[(r - 1) * kRowCells + so]);
-      ld4(h.hzy, &sHz[(r - 1) * kRowCells + so]);
+      if (sm_ok) { ld4(h.hxy, &sHx[(r - 1) * kRowCells + so]); ld4(h.hzy, &sHz[(r - 1) * kRowCells + so]); }
+      else { zero4(h.hxy); zero4(h.hzy); }
       if (lane == 0) {   // Taflove 3.30 for hy, hz at x0 - 1 (an interior cell)
         h.hyp = M::sub(ghy, M::mul(s.db, M::sub(M::sub(gxz, gx), M::sub(e.ez[0], gz))));
         h.hzp = M::sub(ghz, M::mul(s.db, M::sub(M::sub(e.ey[0], gy), M::sub(gxy, gx))));
@@ -130,6 +135,7 @@ struct MarchSmem {
 // zeros (its source is any valid address).
 template <class T>
 __device__ __forceinline__ void cp_vec(T* dst, const T* src, bool valid) {
+  if (valid && !FDTD_CHECK_PTR(src, (int)sizeof(T) * kVec)) valid = false;   // checked build
   const unsigned sa = (unsigned)__cvta_generic_to_shared(dst);
   const int n = valid ? 16 : 0;
 #pragma unroll
@@ -140,6 +146,7 @@ __device__ __forceinline__ void cp_vec(T* dst, const T* src, bool valid) {
 }
 template <class T>
 __device__ __forceinline__ void cp_elem(T* dst, const T* src, bool valid) {
+  if (valid && !FDTD_CHECK_PTR(src, (int)sizeof(T))) valid = false;   // checked build
   const unsigned sa = (unsigned)__cvta_generic_to_shared(dst);
   const int n = valid ? (int)sizeof(T) : 0;
   asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(sa), "l"(src), "n"((int)sizeof(T)),
@@ -188,6 +195,13 @@ __device__ __forceinline__ void march_tile(const State<T>& s, const MarchBox& b,
   const int su = so + width * kVec;   // the next row's slot
   const int sd = so - width * kVec;   // the previous row's slot
   const bool top_row = r == rows - 1, last_lane = lane == width - 1;
+  // shared indices of this thread (checked build: a bad one skips the
+  // thread's shared accesses; the constant true otherwise)
+  const bool sm_ok = FDTD_CHECK_SMEM(so + kVec - 1, SM::kEx) &&
+                     (top_row || FDTD_CHECK_SMEM(su + kVec - 1, SM::kEx)) && (r == 0 || FDTD_CHECK_SMEM(sd, SM::kEx)) &&
+                     FDTD_CHECK_SMEM((SM::kSlots - 1) * SM::kEx + so + kVec - 1, SM::kMain) &&
+                     (!top_row || FDTD_CHECK_SMEM(SM::kMain + (32 + lane) * kVec + kVec - 1, SM::kStage)) &&
+                     (!last_lane || FDTD_CHECK_SMEM(SM::kMain + SM::kTop + 2 * r + 1, SM::kStage));
 
   auto slot = [&](int st, int k) { return stage0 + st * SM::kStage + k * SM::kEx + so; };
   auto top = [&](int st, int k) { return stage0 + st * SM::kStage + SM::kMain + (k * 32 + lane) * kVec; };
@@ -195,6 +209,7 @@ __device__ __forceinline__ void march_tile(const State<T>& s, const MarchBox& b,
 
   // Stage st <- what plane zz's update reads from global memory.
   auto issue = [&](int zz, int st) {
+    if (!sm_ok) return;
     const long long i = (long long)zz * P + base;
     const bool a = vin && zz + 1 < nz;
     cp_vec(slot(st, 0), a ? s.iex + i + P : s.iex, a);
@@ -252,18 +267,25 @@ __device__ __forceinline__ void march_tile(const State<T>& s, const MarchBox& b,
     cp_commit();
     cp_wait_prev();
     const bool work = own && z >= z0;   // this thread updates and stores plane z
-    ld4(e.exz, slot(st, 0)); ld4(e.eyz, slot(st, 1)); ld4(ezz, slot(st, 2));
-    ld4(h.hx, slot(st, 3)); ld4(h.hy, slot(st, 4)); ld4(h.hz, slot(st, 5));
     T ca[kVec], cb[kVec];
-    ld4(ca, slot(st, 6)); ld4(cb, slot(st, 7));
-    if (top_row) { ld4(e.exy, top(st, 0)); ld4(e.ezy, top(st, 1)); }
     T eyr = T(0), ezr = T(0);
-    if (last_lane) { eyr = right(st)[0]; ezr = right(st)[1]; }
+    if (sm_ok) {
+      ld4(e.exz, slot(st, 0)); ld4(e.eyz, slot(st, 1)); ld4(ezz, slot(st, 2));
+      ld4(h.hx, slot(st, 3)); ld4(h.hy, slot(st, 4)); ld4(h.hz, slot(st, 5));
+      ld4(ca, slot(st, 6)); ld4(cb, slot(st, 7));
+      if (top_row) { ld4(e.exy, top(st, 0)); ld4(e.ezy, top(st, 1)); }
+      if (last_lane) { eyr = right(st)[0]; ezr = right(st)[1]; }
+    } else {
+      zero4(e.exz); zero4(e.eyz); zero4(ezz); zero4(h.hx); zero4(h.hy); zero4(h.hz);
+      zero4(ca); zero4(cb); zero4(e.exy); zero4(e.ezy);
+    }
     // ---- H^{n+1/2}(z) -----------------------------------------------------
-    st4(&sEx[so], e.ex);
-    st4(&sEz[so], e.ez);
+    if (sm_ok) { st4(&sEx[so], e.ex); st4(&sEz[so], e.ez); }
     __syncthreads();
-    if (!top_row) { ld4(e.exy, &sEx[su]); ld4(e.ezy, &sEz[su]); }
+    if (!top_row) {
+      if (sm_ok) { ld4(e.exy, &sEx[su]); ld4(e.ezy, &sEz[su]); }
+      else { zero4(e.exy); zero4(e.ezy); }
+    }
     e.eyn = __shfl_down_sync(kFullMask, e.ey[0], 1, width);
     e.ezn = __shfl_down_sync(kFullMask, e.ez[0], 1, width);
     if (last_lane) { e.eyn = eyr; e.ezn = ezr; }
@@ -274,7 +296,7 @@ __device__ __forceinline__ void march_tile(const State<T>& s, const MarchBox& b,
     if (vin) {
       if (plain_h) h_vec_interior(s, e, h.hx, h.hy, h.hz);
       else if (zface_h) {
-        if constexpr (kStagePsi) {
+        if (kStagePsi && sm_ok) {
           h_vec_zface(s, e, z, y, x0, work, slot(st, 8), slot(st, 9), h.hx, h.hy, h.hz);
         } else {
           const int sd_ = z < m - 1 ? 0 : 1;
@@ -284,8 +306,7 @@ __device__ __forceinline__ void march_tile(const State<T>& s, const MarchBox& b,
       }
       else h_vec(s, e, z, y, x0, t, work, h.hx, h.hy, h.hz);
     }
-    st4(&sHx[so], h.hx);
-    st4(&sHz[so], h.hz);
+    if (sm_ok) { st4(&sHx[so], h.hx); st4(&sHz[so], h.hz); }
     __syncthreads();
     // ---- E^{n+1}(z) ---------------------------------------------------------
     h.hyp = __shfl_up_sync(kFullMask, h.hy[kVec - 1], 1, width);
@@ -295,11 +316,11 @@ __device__ __forceinline__ void march_tile(const State<T>& s, const MarchBox& b,
       h.hzp = T(0);
     }
     if (work) {
-      ld4(h.hxy, &sHx[sd]);
-      ld4(h.hzy, &sHz[sd]);
+      if (sm_ok) { ld4(h.hxy, &sHx[sd]); ld4(h.hzy, &sHz[sd]); }
+      else { zero4(h.hxy); zero4(h.hzy); }
       if (plain_h) e_vec_interior(h, ca, cb, e.ex, e.ey, e.ez);
       else if (zface_h) {
-        if constexpr (kStagePsi) {
+        if (kStagePsi && sm_ok) {
           e_vec_zface(s, h, ca, cb, z, y, x0, slot(st, 10), slot(st, 11), e.ex, e.ey, e.ez);
         } else {
           const int sd_ = z < m ? 0 : 1;

@@ -18,6 +18,7 @@
 #pragma once
 
 #include "fdtd_cell.cuh"
+#include "fdtd_check.cuh"
 
 namespace fdtd {
 
@@ -25,6 +26,11 @@ constexpr int kVec = 4;
 
 template <class T>
 __device__ __forceinline__ void ld4(T (&d)[kVec], const T* p) {
+  if (!FDTD_CHECK_PTR(p, (int)sizeof(T) * kVec)) {   // bounds-checked build only
+#pragma unroll
+    for (int j = 0; j < kVec; ++j) d[j] = T(0);
+    return;
+  }
   if constexpr (sizeof(T) == 4) {
     const float4 v = *reinterpret_cast<const float4*>(p);
     d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
@@ -37,6 +43,7 @@ __device__ __forceinline__ void ld4(T (&d)[kVec], const T* p) {
 
 template <class T>
 __device__ __forceinline__ void st4(T* p, const T (&d)[kVec]) {
+  if (!FDTD_CHECK_PTR(p, (int)sizeof(T) * kVec)) return;   // bounds-checked build only
   if constexpr (sizeof(T) == 4) {
     *reinterpret_cast<float4*>(p) = make_float4(d[0], d[1], d[2], d[3]);
   } else {

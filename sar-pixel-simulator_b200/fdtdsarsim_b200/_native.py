@@ -9,7 +9,11 @@ import os
 
 import numpy as np
 
-LIB_NAME = 'libfdtd_b200.so'
+# FDTDSARSIM_B200_LIBRARY=check selects the bounds-checked build
+# (libfdtd_b200_check.so): every global access of the step kernels checked
+# against the live allocations, violations reported as FDTD_ERR_BOUNDS
+LIB_NAME = ('libfdtd_b200_check.so' if os.environ.get('FDTDSARSIM_B200_LIBRARY', '') == 'check'
+            else 'libfdtd_b200.so')
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), LIB_NAME)
 
 FDTD_OK = 0
@@ -18,6 +22,7 @@ FDTD_ERR_CUDA = 2
 FDTD_ERR_STATE = 3
 FDTD_ERR_NONFINITE = 4
 FDTD_ERR_NOMEM = 5
+FDTD_ERR_BOUNDS = 6
 
 FDTD_F32 = 0
 FDTD_F64 = 1
@@ -90,6 +95,7 @@ _D = ctypes.c_double
 SIGNATURES = {
     'fdtd_last_error': [ctypes.c_char_p, _I],
     'fdtd_version': [],
+    'fdtd_bounds_check_enabled': [],
     'fdtd_device_count': [ctypes.POINTER(_I)],
     'fdtd_device_name': [_I, ctypes.c_char_p, _I],
     'fdtd_create': [ctypes.POINTER(Geometry), _I, ctypes.POINTER(_P)],
@@ -143,8 +149,8 @@ SIGNATURES = {
 def _load():
     if not os.path.exists(LIB_PATH):
         raise ImportError(
-            f'{LIB_PATH} is missing: build it with '
-            f'`python sar-pixel-simulator_b200/build.py` (there is no CPU fallback)')
+            f'{LIB_PATH} is missing: build it with `python sar-pixel-simulator_b200/build.py'
+            f'{" --bounds-check" if LIB_NAME.endswith("_check.so") else ""}` (there is no CPU fallback)')
     lib = ctypes.CDLL(LIB_PATH)
     for name, argtypes in SIGNATURES.items():
         fn = getattr(lib, name)
@@ -484,6 +490,11 @@ def check_cell_division(dtype, cell_size, device=0):
     check(lib.fdtd_check_cell_division(dtype_code(dtype), float(cell_size), int(device),
                                        ctypes.byref(tested), ctypes.byref(bad)))
     return tested.value, bad.value
+
+
+def bounds_check_enabled():
+    """True when the loaded library is the bounds-checked build."""
+    return bool(lib.fdtd_bounds_check_enabled())
 
 
 def fused_plan_boxes(nx, ny, nz, npml, tfsf_z, tile_y=4, zchunk=0, slab=False, march=False):

@@ -95,6 +95,7 @@ def test_every_entry_point_rejects_null_handles():
     returns FDTD_ERR_INVALID with a message (the destroy calls accept NULL
     and return FDTD_OK), before any device is touched."""
     no_handle = {'fdtd_last_error', 'fdtd_version', 'fdtd_device_count', 'fdtd_fused_plan_boxes',
+                 'fdtd_bounds_check_enabled',
                  'fdtd_check_cell_division'}
     for name, argtypes in _native.SIGNATURES.items():
         if name in no_handle:
