@@ -335,12 +335,17 @@ int fdtd_fused_plan_boxes(int nx, int ny, int nz, int npml, int tfsf_z, int tile
  * (1200000 for complex64), ntheta <= 4096, nphi <= 64 and
  * ntheta * nphi <= 8192; larger requests return FDTD_ERR_INVALID with a
  * message naming the limit. The first call on a device looks up the
- * array's device address with that device current (make that first call
- * before any stream capture). All calls share the array: calls from one
- * process are serialized by a lock, and work that overlaps a call on the
- * same device through other means races with it. Nothing in the array has
- * to start at zero: each call writes every byte it reads back. Calls are
- * synchronous. */
+ * array's device address with that device current and keeps it for the
+ * process: after a cudaDeviceReset (or anything else that destroys the
+ * device's primary context) the library must be loaded again before this
+ * entry point is used. Every call is synchronous: it copies through
+ * cudaMemcpy and launches on the legacy default stream, so it waits for the
+ * caller's blocking streams, and it cannot be called while a stream is
+ * being captured. All calls share the array: calls from one process are
+ * serialized by a lock, and work that overlaps a call on the same device
+ * through other means races with it. Nothing in the array has to start at
+ * zero: each call writes every byte it reads back. The calling thread's
+ * current device is the same after the call as before. */
 int fdtd_near2far_noalloc(const void *ex_u, const void *ey_u,
                           const void *hx_u, const void *hy_u, int in_dtype,
                           int nx_ph, int ny_ph, int nz_ph, double dx, double r,

@@ -471,6 +471,7 @@ int fdtd_device_name(int device, char* name, int len) {
 }
 
 int fdtd_create(const fdtd_geometry* geom, int device, fdtd_sim** out) {
+  DeviceGuard device_guard;   // the caller's current device is restored on return
   if (!geom || !out) return fail(FDTD_ERR_INVALID, "null argument");
   *out = nullptr;
   const fdtd_geometry& g = *geom;
@@ -597,6 +598,7 @@ int fdtd_create(const fdtd_geometry* geom, int device, fdtd_sim** out) {
 }
 
 int fdtd_destroy(fdtd_sim* s) {
+  DeviceGuard device_guard;   // the caller's current device is restored on return
   if (!s) return FDTD_OK;
   if (s->batch_refs > 0)
     return fail(FDTD_ERR_STATE, "simulation is a member of %d batch(es): destroy them first",
@@ -694,6 +696,7 @@ int fdtd_get_option(fdtd_sim* s, int option, int* value) {
 }
 
 int fdtd_set_absorbers(fdtd_sim* s, const void* profiles) {
+  DeviceGuard device_guard;   // the caller's current device is restored on return
   int rc = check_sim(s);
   if (rc) return rc;
   if (!profiles) return fail(FDTD_ERR_INVALID, "null profiles");
@@ -729,6 +732,7 @@ static int upload_volume(fdtd_sim* s, void* dst, const void* src) {
 }
 
 int fdtd_set_materials(fdtd_sim* s, const void* ca, const void* cb) {
+  DeviceGuard device_guard;   // the caller's current device is restored on return
   int rc = check_sim(s);
   if (rc) return rc;
   if (!ca || !cb) return fail(FDTD_ERR_INVALID, "null Ca/Cb");
@@ -739,6 +743,7 @@ int fdtd_set_materials(fdtd_sim* s, const void* ca, const void* cb) {
 }
 
 int fdtd_set_materials_eps_sigma(fdtd_sim* s, const void* eps_r, const void* sigma, int nz_mat) {
+  DeviceGuard device_guard;   // the caller's current device is restored on return
   int rc = check_sim(s);
   if (rc) return rc;
   if (!eps_r || !sigma) return fail(FDTD_ERR_INVALID, "null eps/sigma");
@@ -772,6 +777,7 @@ int fdtd_set_materials_eps_sigma(fdtd_sim* s, const void* eps_r, const void* sig
 
 int fdtd_set_incident(fdtd_sim* s, const void* ex, const void* ey, const void* hx, const void* hy,
                       int nt_inc) {
+  DeviceGuard device_guard;   // the caller's current device is restored on return
   int rc = check_sim(s);
   if (rc) return rc;
   const fdtd_geometry& g = s->g;
@@ -797,6 +803,7 @@ int fdtd_set_incident(fdtd_sim* s, const void* ex, const void* ey, const void* h
 }
 
 int fdtd_reset(fdtd_sim* s) {
+  DeviceGuard device_guard;   // the caller's current device is restored on return
   int rc = check_sim(s);
   if (rc) return rc;
   const size_t fb = (size_t)s->vol * s->esz;
@@ -815,6 +822,7 @@ int fdtd_reset(fdtd_sim* s) {
 }
 
 int fdtd_run(fdtd_sim* s, int nsteps) {
+  DeviceGuard device_guard;   // the caller's current device is restored on return
   int rc = check_sim(s);
   if (rc) return rc;
   if (nsteps < 0) return fail(FDTD_ERR_INVALID, "negative step count");
@@ -830,6 +838,7 @@ int fdtd_run(fdtd_sim* s, int nsteps) {
 
 int fdtd_run_streamed(fdtd_sim* s, int nsteps, const void* ex, const void* ey, const void* hx,
                       const void* hy) {
+  DeviceGuard device_guard;   // the caller's current device is restored on return
   int rc = check_sim(s);
   if (rc) return rc;
   if (nsteps < 0) return fail(FDTD_ERR_INVALID, "negative step count");
@@ -930,6 +939,7 @@ int fdtd_run_streamed(fdtd_sim* s, int nsteps, const void* ex, const void* ey, c
 }
 
 int fdtd_synchronize(fdtd_sim* s) {
+  DeviceGuard device_guard;   // the caller's current device is restored on return
   int rc = check_sim(s);
   if (rc) return rc;
   CK(cudaStreamSynchronize(s->stream));
@@ -956,6 +966,7 @@ int fdtd_get_stream(fdtd_sim* s, void** stream) {
 }
 
 int fdtd_set_stream(fdtd_sim* s, void* stream) {
+  DeviceGuard device_guard;   // the caller's current device is restored on return
   int rc = check_sim(s);
   if (rc) return rc;
   CK(cudaStreamSynchronize(s->stream));
@@ -964,6 +975,7 @@ int fdtd_set_stream(fdtd_sim* s, void* stream) {
 }
 
 int fdtd_get_kernel_time(fdtd_sim* s, int kind, double* total_ms, int* launches) {
+  DeviceGuard device_guard;   // the caller's current device is restored on return
   int rc = check_sim(s);
   if (rc) return rc;
   if (kind != FDTD_TIME_STEP && kind != FDTD_TIME_PHASOR)
@@ -975,6 +987,7 @@ int fdtd_get_kernel_time(fdtd_sim* s, int kind, double* total_ms, int* launches)
 }
 
 int fdtd_clear_kernel_time(fdtd_sim* s) {
+  DeviceGuard device_guard;   // the caller's current device is restored on return
   int rc = check_sim(s);
   if (rc) return rc;
   if ((rc = collect_timing(s))) return rc;
@@ -984,6 +997,7 @@ int fdtd_clear_kernel_time(fdtd_sim* s) {
 }
 
 int fdtd_get_phasor(fdtd_sim* s, int plane, void* out) {
+  DeviceGuard device_guard;   // the caller's current device is restored on return
   int rc = check_sim(s);
   if (rc) return rc;
   if (plane < 0 || plane >= 24) return fail(FDTD_ERR_INVALID, "phasor plane %d outside [0, 24)", plane);
@@ -999,6 +1013,7 @@ int fdtd_get_phasor(fdtd_sim* s, int plane, void* out) {
 }
 
 int fdtd_get_phasors(fdtd_sim* s, void* out) {
+  DeviceGuard device_guard;   // the caller's current device is restored on return
   int rc = check_sim(s);
   if (rc) return rc;
   if (!out) return fail(FDTD_ERR_INVALID, "null output");
@@ -1018,6 +1033,7 @@ int fdtd_get_phasors(fdtd_sim* s, void* out) {
 }
 
 int fdtd_get_field(fdtd_sim* s, int comp, void* out) {
+  DeviceGuard device_guard;   // the caller's current device is restored on return
   int rc = check_sim(s);
   if (rc) return rc;
   if (comp < 0 || comp >= 6) return fail(FDTD_ERR_INVALID, "field component %d outside [0, 6)", comp);
@@ -1030,6 +1046,7 @@ int fdtd_get_field(fdtd_sim* s, int comp, void* out) {
 }
 
 int fdtd_set_field(fdtd_sim* s, int comp, const void* in) {
+  DeviceGuard device_guard;   // the caller's current device is restored on return
   int rc = check_sim(s);
   if (rc) return rc;
   if (comp < 0 || comp >= 6) return fail(FDTD_ERR_INVALID, "field component %d outside [0, 6)", comp);
@@ -1059,6 +1076,7 @@ extern "C" int fdtd_near2far(const void* ex_u, const void* ey_u, const void* hx_
     return fail(FDTD_ERR_CUDA, "no CUDA device available");
   }
   if (device < 0 || device >= ndev) return fail(FDTD_ERR_INVALID, "device %d out of range", device);
+  DeviceGuard device_guard;   // the caller's current device is restored on return
   CK(cudaSetDevice(device));
   // surface currents in complex128, as near2far.py:64-68 converts them:
   // Jx = -Hy, Jy = Hx, Mx = Ey, My = -Ex   (near2far.py:94-96)
@@ -1412,6 +1430,7 @@ int batch_run_streams(fdtd_batch* b, int nsteps) {
 extern "C" {
 
 int fdtd_batch_create(fdtd_sim* const* sims, int n, fdtd_batch** out) {
+  DeviceGuard device_guard;   // the caller's current device is restored on return
   if (!out) return fail(FDTD_ERR_INVALID, "null output handle");
   *out = nullptr;
   if (!sims || n < 1) return fail(FDTD_ERR_INVALID, "a batch needs at least one simulation");
@@ -1450,6 +1469,7 @@ int fdtd_batch_create(fdtd_sim* const* sims, int n, fdtd_batch** out) {
 }
 
 int fdtd_batch_destroy(fdtd_batch* b) {
+  DeviceGuard device_guard;   // the caller's current device is restored on return
   if (!b) return FDTD_OK;
   if (b->members_counted)
     for (fdtd_sim* m : b->sims) --m->batch_refs;
@@ -1494,6 +1514,7 @@ int fdtd_batch_set_option(fdtd_batch* b, int option, int value) {
 }
 
 int fdtd_batch_run(fdtd_batch* b, int nsteps) {
+  DeviceGuard device_guard;   // the caller's current device is restored on return
   if (!b) return fail(FDTD_ERR_INVALID, "null batch handle");
   if (nsteps < 0) return fail(FDTD_ERR_INVALID, "negative step count");
   for (size_t m = 0; m < b->sims.size(); ++m) {
@@ -1518,6 +1539,7 @@ int fdtd_batch_run(fdtd_batch* b, int nsteps) {
 }
 
 int fdtd_batch_synchronize(fdtd_batch* b) {
+  DeviceGuard device_guard;   // the caller's current device is restored on return
   if (!b) return fail(FDTD_ERR_INVALID, "null batch handle");
   CK(cudaSetDevice(b->device));
   CK(cudaStreamSynchronize(b->stream));
@@ -1688,6 +1710,7 @@ int grad_backward(fdtd_sim* s, int nz_out, double* out_ca, double* out_cb) {
 extern "C" {
 
 int fdtd_grad_forward(fdtd_sim* s, int checkpoint_every) {
+  DeviceGuard device_guard;   // the caller's current device is restored on return
   int rc = check_sim(s);
   if (rc) return rc;
   if (checkpoint_every < 1) return fail(FDTD_ERR_INVALID, "checkpoint period must be >= 1");
@@ -1721,6 +1744,7 @@ int fdtd_grad_forward(fdtd_sim* s, int checkpoint_every) {
 
 int fdtd_grad_backward(fdtd_sim* s, const double* dj_dre, const double* dj_dim, int nz_out,
                        double* grad_ca, double* grad_cb) {
+  DeviceGuard device_guard;   // the caller's current device is restored on return
   int rc = check_sim(s);
   if (rc) return rc;
   if (!dj_dre || !dj_dim) return fail(FDTD_ERR_INVALID, "null phasor gradient");
@@ -1940,6 +1964,7 @@ int fdtd_fused_plan_boxes(int nx, int ny, int nz, int npml, int tfsf_z, int tile
 }
 
 int fdtd_incident_set_option(fdtd_incident* b, int option, int value) {
+  DeviceGuard device_guard;   // the caller's current device is restored on return
   int rc = check_inc(b);
   if (rc) return rc;
   if (option != FDTD_OPT_KERNEL && option != FDTD_OPT_TILE_Y && option != FDTD_OPT_ZCHUNK &&
@@ -1949,6 +1974,7 @@ int fdtd_incident_set_option(fdtd_incident* b, int option, int value) {
 }
 
 int fdtd_incident_set_absorbers(fdtd_incident* b, const void* profiles) {
+  DeviceGuard device_guard;   // the caller's current device is restored on return
   int rc = check_inc(b);
   if (rc) return rc;
   return fdtd_set_absorbers(b->sim, profiles);
@@ -1957,6 +1983,7 @@ int fdtd_incident_set_absorbers(fdtd_incident* b, const void* profiles) {
 int fdtd_incident_make_excitation(fdtd_incident* b, const double* k_vals, const double* pulse_fft,
                                   int nt_fft, double theta_deg, double phi_deg, int pol,
                                   double gauss_radius, double* peak) {
+  DeviceGuard device_guard;   // the caller's current device is restored on return
   int rc = check_inc(b);
   if (rc) return rc;
   if (!k_vals || !pulse_fft) return fail(FDTD_ERR_INVALID, "null pulse spectrum");
@@ -1995,6 +2022,7 @@ int fdtd_incident_make_excitation(fdtd_incident* b, const double* k_vals, const 
 }
 
 int fdtd_incident_set_excitation(fdtd_incident* b, const void* ex_imag, const void* ey_imag) {
+  DeviceGuard device_guard;   // the caller's current device is restored on return
   int rc = check_inc(b);
   if (rc) return rc;
   if ((!ex_imag || !ey_imag) && b->nt_pulse > 0) return fail(FDTD_ERR_INVALID, "null excitation");
@@ -2010,6 +2038,7 @@ int fdtd_incident_set_excitation(fdtd_incident* b, const void* ex_imag, const vo
 }
 
 int fdtd_incident_get_excitation(fdtd_incident* b, void* ex_imag, void* ey_imag) {
+  DeviceGuard device_guard;   // the caller's current device is restored on return
   int rc = check_inc(b);
   if (rc) return rc;
   if (!b->have_exc) return fail(FDTD_ERR_STATE, "no excitation (fdtd_incident_make_excitation)");
@@ -2025,6 +2054,7 @@ int fdtd_incident_get_excitation(fdtd_incident* b, void* ex_imag, void* ey_imag)
 }
 
 int fdtd_incident_run(fdtd_incident* b) {
+  DeviceGuard device_guard;   // the caller's current device is restored on return
   int rc = check_inc(b);
   if (rc) return rc;
   if (!b->sim->have_abs) return fail(FDTD_ERR_STATE, "absorbers not set (fdtd_incident_set_absorbers)");
@@ -2033,6 +2063,7 @@ int fdtd_incident_run(fdtd_incident* b) {
 }
 
 int fdtd_incident_get_planes(fdtd_incident* b, void* ex, void* ey, void* hx, void* hy) {
+  DeviceGuard device_guard;   // the caller's current device is restored on return
   int rc = check_inc(b);
   if (rc) return rc;
   if (!b->ran) return fail(FDTD_ERR_STATE, "incident run not done (fdtd_incident_run)");
@@ -2048,6 +2079,7 @@ int fdtd_incident_get_planes(fdtd_incident* b, void* ex, void* ey, void* hx, voi
 }
 
 int fdtd_incident_get_phasors(fdtd_incident* b, void* ex_ph, void* ey_ph, void* hx_ph, void* hy_ph) {
+  DeviceGuard device_guard;   // the caller's current device is restored on return
   int rc = check_inc(b);
   if (rc) return rc;
   if (!b->ran) return fail(FDTD_ERR_STATE, "incident run not done (fdtd_incident_run)");
@@ -2062,6 +2094,7 @@ int fdtd_incident_get_phasors(fdtd_incident* b, void* ex_ph, void* ey_ph, void* 
 }
 
 int fdtd_set_incident_from(fdtd_sim* s, const fdtd_incident* b) {
+  DeviceGuard device_guard;   // the caller's current device is restored on return
   int rc = check_sim(s);
   if (rc) return rc;
   if (!b || !b->sim) return fail(FDTD_ERR_INVALID, "null incident handle");

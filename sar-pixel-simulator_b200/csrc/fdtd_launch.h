@@ -8,6 +8,24 @@
 
 namespace fdtd {
 
+// Restores the calling thread's current device when it leaves scope: every
+// entry point that makes its simulation's device current leaves the
+// caller's device as it found it.
+struct DeviceGuard {
+  int prev = -1;
+  DeviceGuard() {
+    if (cudaGetDevice(&prev) != cudaSuccess) {
+      prev = -1;
+      cudaGetLastError();
+    }
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+  DeviceGuard(const DeviceGuard&) = delete;
+  DeviceGuard& operator=(const DeviceGuard&) = delete;
+};
+
 template <class T>
 void launch_split_step(const State<T>& s, const int* tdev, int toff, cudaStream_t st);
 

@@ -72,6 +72,7 @@ extern "C" int fdtd_check_cell_division(int dtype, double cell_size, int device,
   if (!tested || !mismatches) return report_error(FDTD_ERR_INVALID, "null argument");
   if (dtype != FDTD_F32 && dtype != FDTD_F64) return report_error(FDTD_ERR_INVALID, "bad dtype");
   if (!(cell_size > 0)) return report_error(FDTD_ERR_INVALID, "cell size must be positive");
+  DeviceGuard device_guard;   // the caller's current device is restored on return
   cudaError_t e = cudaSetDevice(device);
   if (e != cudaSuccess) return report_error(FDTD_ERR_CUDA, cudaGetErrorString(e));
   unsigned long long* bad = nullptr;

@@ -268,6 +268,7 @@ extern "C" int fdtd_near2far_noalloc(const void* ex_u, const void* ey_u, const v
   }
   if (device < 0 || device >= ndev || device >= 64) return n2f_fail(FDTD_ERR_INVALID, "device out of range");
   std::lock_guard<std::mutex> lock(g_n2f_mutex);
+  DeviceGuard device_guard;   // the caller's current device is restored on return
   cudaError_t e = cudaSetDevice(device);
   if (e != cudaSuccess) return n2f_fail(FDTD_ERR_CUDA, cudaGetErrorString(e));
   // set-up, once per device, with that device current: the address of the

@@ -166,6 +166,7 @@ def generate_incident_beam(params: ParameterCollection, write: bool = True, devi
 # Readers in this process wait for the write (wait_written); the threads are
 # not daemons, so the interpreter also waits for them before it exits.
 _WRITES = {}
+_WRITES_LOCK = threading.Lock()
 
 
 def store_incident_beam(params: ParameterCollection, planes, phasors, background: bool = False):
@@ -194,20 +195,27 @@ def store_incident_beam(params: ParameterCollection, planes, phasors, background
 
     t = threading.Thread(target=run, name='incident-file-write')
     t.errors = errors
-    _WRITES[fname] = t
-    t.start()
+    with _WRITES_LOCK:   # a waiter never finds an entry whose thread has not started
+        _WRITES[fname] = t
+        t.start()
 
 
 def wait_written(fname=None):
     """Wait for the background write of incident file ``fname`` (of every
-    such write when None) and raise the first error one of them met."""
-    keys = [os.path.abspath(fname)] if fname is not None else list(_WRITES)
+    such write when None) and raise the first error one of them met. Every
+    waiter that finds a write in progress blocks until it ends and sees its
+    error; the entry is removed only after the write has ended."""
+    with _WRITES_LOCK:
+        keys = [os.path.abspath(fname)] if fname is not None else list(_WRITES)
+        found = [(key, _WRITES.get(key)) for key in keys]
     first = None
-    for key in keys:
-        t = _WRITES.pop(key, None)
+    for key, t in found:
         if t is None:
             continue
         t.join()
+        with _WRITES_LOCK:
+            if _WRITES.get(key) is t:
+                del _WRITES[key]
         if t.errors and first is None:
             first = t.errors[0]
     if first is not None:

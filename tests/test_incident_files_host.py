@@ -114,3 +114,40 @@ def test_run_experiment_returns_with_the_incident_file_on_disk(tmp_path, slow_wr
     experiment.run_experiment(pc, [MaterialModel(np.ones(shape, np.float32),
                                                  np.zeros(shape, np.float32), g.cell_size, 'm')])
     assert os.path.exists(inc_filename(pc)) and not incident._WRITES
+
+
+def test_concurrent_waiters_all_block_and_all_see_the_error(tmp_path, monkeypatch):
+    """Two threads wait for the same background write: both return only once
+    it has ended, and both get its error."""
+    import threading
+    pc = params(tmp_path)
+    planes, phasors = beam(pc)
+    started = threading.Event()
+
+    def slow_fail(*a, **k):
+        started.set()
+        time.sleep(0.4)
+        raise OSError('disk full')
+
+    monkeypatch.setattr(incidentbeam, 'write_incident_file', slow_fail)
+    incident.store_incident_beam(pc, planes, phasors, background=True)
+    assert started.wait(5)
+    fname = inc_filename(pc)
+    seen = {}
+
+    def waiter(k):
+        t0 = time.perf_counter()
+        try:
+            incident.wait_written(fname)
+            seen[k] = ('ok', time.perf_counter() - t0)
+        except OSError as e:
+            seen[k] = (str(e), time.perf_counter() - t0)
+
+    ts = [threading.Thread(target=waiter, args=(k,)) for k in range(2)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join(10)
+    assert [seen[k][0] for k in range(2)] == ['disk full', 'disk full'], seen
+    assert all(seen[k][1] > 0.2 for k in range(2)), seen     # both waited for the write
+    assert not incident._WRITES
