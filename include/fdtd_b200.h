@@ -294,6 +294,24 @@ int fdtd_batch_run(fdtd_batch *b, int nsteps);
 int fdtd_batch_synchronize(fdtd_batch *b);
 int fdtd_batch_get_stream(fdtd_batch *b, void **stream);
 
+/* Poynting power through the simulation's internal phasor planes, in
+ * float64, from its current phasors on the device. Replaces the near-field
+ * half of process_results (processresults.py:128-257), which evaluates it
+ * on the host from the result file. inc_phasors: the incident beam's
+ * ex, ey, hx, hy phasors, four consecutive (ny_ph, nx_ph) complex planes of
+ * the simulation's element type (host). weights: the Simpson weights that
+ * scipy.integrate.simpson applies along each axis, ny_ph values (rows of z
+ * planes, columns of x planes), nx_ph values (columns of z and y planes),
+ * then size_z_material values (side-plane rows below the material top) and
+ * nz_ph - 1 - size_z_material values (the rows above, the last phasor row
+ * excluded as the reference excludes it). out: 11 powers: incident, left
+ * bottom, left top, right bottom, right top, front bottom, front top, back
+ * bottom, back top, down, up. The flux of each cell, Re(E x conj(H)) . n / 2,
+ * is formed in float64 (the reference forms it in complex64 and integrates
+ * in float64), so the powers agree to rounding. Synchronous. */
+int fdtd_near_field_power(fdtd_sim *sim, const void *inc_phasors, int size_z_material,
+                          const double *weights, double *out);
+
 /* Diagnostic (no counterpart in the reference): 1 in the bounds-checked
  * build of this library (libfdtd_b200_check.so: every global access of the
  * step kernels is checked against the library's live allocations and every

@@ -95,6 +95,11 @@ struct fdtd_sim {
   // slot, re-pitched into the incident buffers on the copy stream
   void* dstage = nullptr;
   size_t dstage_bytes = 0;
+  // fdtd_near_field_power: incident phasors, Simpson weights, partial sums
+  // (made on first use)
+  void* nf_inc = nullptr;
+  double* nf_w = nullptr;
+  double* nf_part = nullptr;
   // packed (nz, ny, nx) device copy of a host volume, re-pitched on the
   // device by upload_volume (created on first use)
   void* packed = nullptr;
@@ -1548,6 +1553,38 @@ int fdtd_batch_synchronize(fdtd_batch* b) {
 }
 
 int fdtd_bounds_check_enabled(void) { return check_enabled() ? 1 : 0; }
+
+int fdtd_near_field_power(fdtd_sim* s, const void* inc_phasors, int size_z_material, const double* weights,
+                          double* out) {
+  DeviceGuard device_guard;   // the caller's current device is restored on return
+  int rc = check_sim(s);
+  if (rc) return rc;
+  if (!inc_phasors || !weights || !out) return fail(FDTD_ERR_INVALID, "null argument");
+  const int szm = size_z_material;
+  if (szm < 1 || szm > s->nz_ph - 2)
+    return fail(FDTD_ERR_INVALID, "size_z_material %d outside [1, nz_phasor - 2 = %d]", szm, s->nz_ph - 2);
+  const int kBlocks = 296;
+  const size_t plane = (size_t)s->ny_ph * s->nx_ph;
+  const size_t nw = (size_t)s->ny_ph + s->nx_ph + (size_t)(s->nz_ph - 1);
+  if (!s->nf_inc && (rc = alloc(s, 4 * plane * 2 * s->esz, &s->nf_inc))) return rc;
+  if (!s->nf_w && (rc = alloc(s, sizeof(double) * (size_t)(s->ny_ph + s->nx_ph + s->nz_ph), (void**)&s->nf_w)))
+    return rc;
+  if (!s->nf_part && (rc = alloc(s, sizeof(double) * 11 * kBlocks, (void**)&s->nf_part))) return rc;
+  CK(cudaMemcpyAsync(s->nf_inc, inc_phasors, 4 * plane * 2 * s->esz, cudaMemcpyHostToDevice, s->stream));
+  CK(cudaMemcpyAsync(s->nf_w, weights, sizeof(double) * nw, cudaMemcpyHostToDevice, s->stream));
+  const int e = s->g.dtype == FDTD_F32
+                    ? near_field_power_run<float>((const float*)s->ph, s->ph_off, (const float*)s->nf_inc, s->nx_ph,
+                                                  s->ny_ph, s->nz_ph, szm, s->nf_w, s->nf_part, kBlocks, out,
+                                                  s->stream)
+                    : near_field_power_run<double>((const double*)s->ph, s->ph_off, (const double*)s->nf_inc,
+                                                   s->nx_ph, s->ny_ph, s->nz_ph, szm, s->nf_w, s->nf_part, kBlocks,
+                                                   out, s->stream);
+  if (e) {
+    cudaError_t ce = cudaGetLastError();
+    return fail(FDTD_ERR_CUDA, "near-field power: %s", cudaGetErrorString(ce));
+  }
+  return take_bounds_violation();
+}
 
 int fdtd_batch_get_stream(fdtd_batch* b, void** stream) {
   if (!b || !stream) return fail(FDTD_ERR_INVALID, "null argument");

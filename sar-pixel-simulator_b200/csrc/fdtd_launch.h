@@ -198,6 +198,17 @@ struct FieldPtrs {
 template <class T>
 void launch_check_finite(const FieldPtrs<T>& f, long long vol, int step, int* flags, cudaStream_t st);
 
+// Near-field power (fdtd_nearfield.cu): the 11 face powers (incident, left,
+// right, front, back bottom/top, down, up) of a simulation's phasor planes
+// (ph, plane offsets off) and the incident phasors inc (4 consecutive
+// (ny_ph, nx_ph) complex planes, device), with the Simpson weights w_dev
+// (ny_ph, nx_ph, szm, nz_ph - 1 - szm values, device) and `blocks` x 11
+// float64 partial sums in `partial`. Returns 0 or 1 (CUDA error).
+template <class T>
+int near_field_power_run(const T* ph, const long long* off, const T* inc, int nx_ph, int ny_ph, int nz_ph,
+                         int szm, const double* w_dev, double* partial, int blocks, double* out,
+                         cudaStream_t st);
+
 // Records an error message for fdtd_last_error(); returns code.
 int report_error(int code, const char* msg);
 

@@ -96,6 +96,7 @@ SIGNATURES = {
     'fdtd_last_error': [ctypes.c_char_p, _I],
     'fdtd_version': [],
     'fdtd_bounds_check_enabled': [],
+    'fdtd_near_field_power': [_P, _P, _I, _P, _P],
     'fdtd_device_count': [ctypes.POINTER(_I)],
     'fdtd_device_name': [_I, ctypes.c_char_p, _I],
     'fdtd_create': [ctypes.POINTER(Geometry), _I, ctypes.POINTER(_P)],
@@ -370,6 +371,20 @@ class NativeSim:
 
     def get_fields(self):
         return {c: self.get_field(c) for c in FIELD_NAMES}
+
+    def near_field_power(self, inc_phasors, size_z_material, weights):
+        """The 11 face powers of fdtd_near_field_power (incident, left /
+        right / front / back bottom and top, down, up) from the current
+        phasors; inc_phasors: ex, ey, hx, hy incident phasor planes (ny_ph,
+        nx_ph); weights: the concatenated Simpson weights."""
+        cd = np.complex64 if self.dtype == np.float32 else np.complex128
+        inc = np.ascontiguousarray(np.stack([np.asarray(inc_phasors[k]) for k in
+                                             ('ex_inc_phasor', 'ey_inc_phasor', 'hx_inc_phasor',
+                                              'hy_inc_phasor')]), dtype=cd)
+        w = np.ascontiguousarray(weights, dtype=np.float64)
+        out = np.zeros(11, np.float64)
+        check(lib.fdtd_near_field_power(self.h, ptr(inc), int(size_z_material), ptr(w), ptr(out)))
+        return out
 
     def set_incident_from(self, inc):
         """The first nt_inc planes recorded by a NativeIncident run, device

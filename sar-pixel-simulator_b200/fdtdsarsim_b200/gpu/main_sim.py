@@ -57,6 +57,13 @@ def _device_of(params):
 class MainSimGpu:
     """Runs one material model per ``run`` call on one B200."""
 
+    # With True, save_results also writes the near-field power computed on
+    # the device from the resident phasors (fdtd_near_field_power; float64
+    # flux, equal to the reference's host evaluation to rounding), and
+    # process_results keeps it; with False (the default) process_results
+    # evaluates it on the host from the file, bit for bit as the reference.
+    device_postprocess = False
+
     def __init__(self, params: ParameterCollection, mpi=False, kernel=None, tile=None):
         self.params = params
         self.mpi = mpi
@@ -230,6 +237,16 @@ class MainSimGpu:
             if material_meta is not None:
                 for k, v in material_meta.items():
                     mg.attrs[k] = v
+            if self.device_postprocess:
+                from ..processresults import near_field_power_device
+                g = self.params.geom_params
+                inc = {k: pg[k][()] for k in ('ex_inc_phasor', 'ey_inc_phasor', 'hx_inc_phasor',
+                                              'hy_inc_phasor')}
+                nf = out.create_group('near_field_power')
+                for k, v in near_field_power_device(self.native, inc, g.cell_size,
+                                                    g.size_z_material).items():
+                    nf.attrs[k] = v
+                nf.attrs['powers_computed'] = True
 
     def close(self):
         self.native.close()

@@ -76,6 +76,35 @@ def near_field_power(phasors: Mapping, dx: float, size_z_material: int):
     return power
 
 
+def simpson_weights(n, dx):
+    """The weights scipy.integrate.simpson applies to n samples spaced dx:
+    the integral of each unit vector (so even n gets scipy's own end
+    correction)."""
+    return scipy.integrate.simpson(np.eye(n), dx=dx, axis=1)
+
+
+_NF_KEYS = ('incident', 'left_bottom', 'left_top', 'right_bottom', 'right_top', 'front_bottom',
+            'front_top', 'back_bottom', 'back_top', 'down', 'up')
+
+
+def near_field_power_device(native, inc_phasors: Mapping, dx: float, size_z_material: int):
+    """near_field_power from a simulation's phasors on the device
+    (fdtd_near_field_power: the flux formed in float64, summed with the
+    Simpson weights scipy applies); same keys as near_field_power. native:
+    the simulation's NativeSim, after its run."""
+    nx, ny, nz = native.nx_ph, native.ny_ph, native.nz_ph
+    szm = int(size_z_material)
+    w = np.concatenate([simpson_weights(ny, dx), simpson_weights(nx, dx), simpson_weights(szm, dx),
+                        simpson_weights(nz - 1 - szm, dx)])
+    vals = native.near_field_power(inc_phasors, szm, w)
+    power = dict(zip(_NF_KEYS, (float(v) for v in vals)))
+    power['top_total'] = power['up'] + power['left_top'] + power['right_top'] \
+        + power['front_top'] + power['back_top']
+    power['bottom_total'] = power['down'] + power['left_bottom'] + power['right_bottom'] \
+        + power['front_bottom'] + power['back_bottom']
+    return power
+
+
 def scattering_coefficient(out_pwr_far, incident_power, nx_phasor, ny_phasor, dx):
     """Far-field power normalised by the incident power through the
     illuminated area, times 4 pi r^2 (processresults.py:103-119)."""
