@@ -294,6 +294,29 @@ int fdtd_batch_run(fdtd_batch *b, int nsteps);
 int fdtd_batch_synchronize(fdtd_batch *b);
 int fdtd_batch_get_stream(fdtd_batch *b, void **stream);
 
+/* A material block made on the device instead of uploaded (replaces the
+ * host fill of the reference's generators: materials/materials.py:112-164
+ * rough_dielectric, materials/soilmodels.py:16-195 one- and two-layer
+ * soils, materials/bubbles.py:21-199 bubbles). fdtd_fill_layers stages the
+ * block's eps_r and sigma, (nz_mat, ny, nx), from `nlayers` interface height
+ * maps in cells ((ny, nx) doubles each, lowest first, host): a cell takes
+ * eps_r[k], sigma[k] of the first interface k with z <= height_k(y, x),
+ * else eps_r[nlayers], sigma[nlayers] (the medium above: vacuum is 1, 0);
+ * values rounded to the element type. fdtd_paint_spheres paints n spheres
+ * (zc, yc, xc, rc, ri as doubles each: centre and radius in cells, integer
+ * half-width ri <= 64) into the staged block: every cell
+ * (rint(zc + dz), rint(yc + dy), rint(xc + dx)), |dz|, |dy|, |dx| <= ri,
+ * dz^2 + dy^2 + dx^2 < rc^2, takes eps_r, sigma. fdtd_set_materials_staged
+ * makes Ca/Cb from the staged block, as fdtd_set_materials_eps_sigma does
+ * from an uploaded one; fdtd_get_staged_materials copies the block back
+ * (nz_mat must be the staged block's height).
+ * A later fdtd_set_materials discards the staged block. Synchronous. */
+int fdtd_fill_layers(fdtd_sim *sim, int nz_mat, int nlayers, const double *heights, const double *eps_r,
+                     const double *sigma);
+int fdtd_paint_spheres(fdtd_sim *sim, int n, const double *spheres, double eps_r, double sigma);
+int fdtd_set_materials_staged(fdtd_sim *sim);
+int fdtd_get_staged_materials(fdtd_sim *sim, int nz_mat, void *eps_r, void *sigma);
+
 /* Poynting power through the simulation's internal phasor planes, in
  * float64, from its current phasors on the device. Replaces the near-field
  * half of process_results (processresults.py:128-257), which evaluates it

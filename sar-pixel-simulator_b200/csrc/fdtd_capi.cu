@@ -100,6 +100,11 @@ struct fdtd_sim {
   void* nf_inc = nullptr;
   double* nf_w = nullptr;
   double* nf_part = nullptr;
+  // material block staged in packed (eps_r) and packed2 (sigma): its height
+  // (-1: none), and scratch for height maps / spheres (grown as needed)
+  int mat_nz = -1;
+  void* mat_scratch = nullptr;
+  size_t mat_scratch_bytes = 0;
   // packed (nz, ny, nx) device copy of a host volume, re-pitched on the
   // device by upload_volume (created on first use)
   void* packed = nullptr;
@@ -220,6 +225,54 @@ void release(fdtd_sim* s, void* p) {
       return;
     }
 }
+
+// The handle's two packed volume buffers (made on first use, kept): they
+// stage a material block's eps_r (packed) and sigma (packed2).
+int stage_buffers(fdtd_sim* s) {
+  const size_t vol_bytes = (size_t)s->g.nx * s->g.ny * s->g.nz * s->esz;
+  int rc;
+  if (!s->packed && (rc = alloc(s, vol_bytes, &s->packed))) return rc;
+  if (!s->packed2 && (rc = alloc(s, vol_bytes, &s->packed2))) return rc;
+  return FDTD_OK;
+}
+
+// Device scratch of at least `bytes` for height maps or sphere lists.
+int mat_scratch(fdtd_sim* s, size_t bytes, void** out) {
+  if (s->mat_scratch_bytes < bytes) {
+    release(s, s->mat_scratch);
+    s->mat_scratch = nullptr;
+    s->mat_scratch_bytes = 0;
+    int rc = alloc(s, bytes, &s->mat_scratch);
+    if (rc) return rc;
+    s->mat_scratch_bytes = bytes;
+  }
+  *out = s->mat_scratch;
+  return FDTD_OK;
+}
+
+// Ca, Cb from the staged eps_r (packed) and sigma (packed2) of the block's
+// mat_nz planes, vacuum above (materials/materials.py:23-68).
+int materials_from_stage(fdtd_sim* s) {
+  const fdtd_geometry& g = s->g;
+  const int nz_mat = s->mat_nz;
+  const void* de = s->packed;
+  const void* ds = s->packed2;
+  // eps0 as hard-coded in materials/materials.py:45, rounded to the dtype
+  const double eps0 = 8.8541878128e-12;
+  if (g.dtype == FDTD_F32)
+    launch_eps_sigma<float>(g.nx, g.ny, g.nz, nz_mat, s->pitch, (const float*)de, (const float*)ds,
+                            (float)eps0, (float)g.timestep, (float)g.cell_size, (float*)s->ca,
+                            (float*)s->cb, s->stream);
+  else
+    launch_eps_sigma<double>(g.nx, g.ny, g.nz, nz_mat, s->pitch, (const double*)de,
+                             (const double*)ds, eps0, g.timestep, g.cell_size, (double*)s->ca,
+                             (double*)s->cb, s->stream);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(s->stream));
+  s->have_mat = true;
+  return FDTD_OK;
+}
+
 
 template <class T>
 State<T> make_state(const fdtd_sim* s, int src, int dst) {
@@ -721,6 +774,7 @@ static int upload_volume(fdtd_sim* s, void* dst, const void* src) {
   const size_t w = (size_t)s->g.nx * s->esz;
   const long long rows = (long long)s->g.ny * s->g.nz;
   if (!s->packed && alloc(s, w * rows, &s->packed) != FDTD_OK) s->packed = nullptr;
+  s->mat_nz = -1;   // the staging buffer now holds a coefficient volume
   if (s->packed) {
     CK(cudaMemcpyAsync(s->packed, src, w * rows, cudaMemcpyHostToDevice, s->stream));
     if (s->g.dtype == FDTD_F32)
@@ -755,28 +809,96 @@ int fdtd_set_materials_eps_sigma(fdtd_sim* s, const void* eps_r, const void* sig
   const fdtd_geometry& g = s->g;
   if (nz_mat < 0 || nz_mat > g.nz) return fail(FDTD_ERR_INVALID, "nz_mat %d outside [0, %d]", nz_mat, g.nz);
   const size_t n = (size_t)nz_mat * g.ny * g.nx;
-  // the two packed volume buffers of the handle (made on first use, kept)
-  // stage eps_r and sigma; no allocation per call
-  const size_t vol_bytes = (size_t)g.nx * g.ny * g.nz * s->esz;
-  if (!s->packed && (rc = alloc(s, vol_bytes, &s->packed))) return rc;
-  if (!s->packed2 && (rc = alloc(s, vol_bytes, &s->packed2))) return rc;
+  if ((rc = stage_buffers(s))) return rc;
   void* de = s->packed;
   void* ds = s->packed2;
   CK(cudaMemcpyAsync(de, eps_r, n * s->esz, cudaMemcpyHostToDevice, s->stream));
   CK(cudaMemcpyAsync(ds, sigma, n * s->esz, cudaMemcpyHostToDevice, s->stream));
-  // eps0 as hard-coded in materials/materials.py:45, rounded to the dtype
-  const double eps0 = 8.8541878128e-12;
+  s->mat_nz = nz_mat;
+  return materials_from_stage(s);
+}
+
+int fdtd_fill_layers(fdtd_sim* s, int nz_mat, int nlayers, const double* heights, const double* eps_r,
+                     const double* sigma) {
+  DeviceGuard device_guard;   // the caller's current device is restored on return
+  int rc = check_sim(s);
+  if (rc) return rc;
+  const fdtd_geometry& g = s->g;
+  if (nz_mat < 0 || nz_mat > g.nz) return fail(FDTD_ERR_INVALID, "nz_mat %d outside [0, %d]", nz_mat, g.nz);
+  if (nlayers < 0 || nlayers > 64) return fail(FDTD_ERR_INVALID, "%d layers (0 to 64)", nlayers);
+  if ((nlayers > 0 && !heights) || !eps_r || !sigma) return fail(FDTD_ERR_INVALID, "null argument");
+  if ((rc = stage_buffers(s))) return rc;
+  const size_t plane = (size_t)g.ny * g.nx;
+  const size_t hbytes = sizeof(double) * (plane * nlayers + 2 * (nlayers + 1));
+  double* d = nullptr;
+  if ((rc = mat_scratch(s, hbytes, (void**)&d))) return rc;
+  double* dh = d;
+  double* dev = d + plane * nlayers;
+  double* dsv = dev + nlayers + 1;
+  if (nlayers) CK(cudaMemcpyAsync(dh, heights, sizeof(double) * plane * nlayers, cudaMemcpyHostToDevice, s->stream));
+  CK(cudaMemcpyAsync(dev, eps_r, sizeof(double) * (nlayers + 1), cudaMemcpyHostToDevice, s->stream));
+  CK(cudaMemcpyAsync(dsv, sigma, sizeof(double) * (nlayers + 1), cudaMemcpyHostToDevice, s->stream));
+  if (nz_mat > 0) {
+    if (g.dtype == FDTD_F32)
+      launch_fill_layers<float>((float*)s->packed, (float*)s->packed2, g.nx, g.ny, nz_mat, nlayers, dh, dev, dsv,
+                                s->stream);
+    else
+      launch_fill_layers<double>((double*)s->packed, (double*)s->packed2, g.nx, g.ny, nz_mat, nlayers, dh, dev,
+                                 dsv, s->stream);
+    CK(cudaGetLastError());
+  }
+  CK(cudaStreamSynchronize(s->stream));   // the scratch is reused by the next call
+  s->mat_nz = nz_mat;
+  return take_bounds_violation();
+}
+
+int fdtd_paint_spheres(fdtd_sim* s, int n, const double* spheres, double eps_r, double sigma) {
+  DeviceGuard device_guard;   // the caller's current device is restored on return
+  int rc = check_sim(s);
+  if (rc) return rc;
+  if (s->mat_nz < 0) return fail(FDTD_ERR_STATE, "no staged material block (fdtd_fill_layers)");
+  if (n < 0 || (n > 0 && !spheres)) return fail(FDTD_ERR_INVALID, "bad sphere list");
+  if (n == 0) return FDTD_OK;
+  const fdtd_geometry& g = s->g;
+  for (int k = 0; k < n; ++k) {
+    const double ri = spheres[5 * k + 4];
+    if (!(ri >= 0 && ri <= 64 && ri == (double)(int)ri))
+      return fail(FDTD_ERR_INVALID, "sphere %d: integer radius %g outside [0, 64]", k, ri);
+  }
+  double* d = nullptr;
+  if ((rc = mat_scratch(s, sizeof(double) * 5 * (size_t)n, (void**)&d))) return rc;
+  CK(cudaMemcpyAsync(d, spheres, sizeof(double) * 5 * (size_t)n, cudaMemcpyHostToDevice, s->stream));
   if (g.dtype == FDTD_F32)
-    launch_eps_sigma<float>(g.nx, g.ny, g.nz, nz_mat, s->pitch, (const float*)de, (const float*)ds,
-                            (float)eps0, (float)g.timestep, (float)g.cell_size, (float*)s->ca,
-                            (float*)s->cb, s->stream);
+    launch_paint_spheres<float>((float*)s->packed, (float*)s->packed2, g.nx, g.ny, s->mat_nz, d, n, eps_r, sigma,
+                                s->stream);
   else
-    launch_eps_sigma<double>(g.nx, g.ny, g.nz, nz_mat, s->pitch, (const double*)de,
-                             (const double*)ds, eps0, g.timestep, g.cell_size, (double*)s->ca,
-                             (double*)s->cb, s->stream);
+    launch_paint_spheres<double>((double*)s->packed, (double*)s->packed2, g.nx, g.ny, s->mat_nz, d, n, eps_r,
+                                 sigma, s->stream);
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(s->stream));
-  s->have_mat = true;
+  return take_bounds_violation();
+}
+
+int fdtd_set_materials_staged(fdtd_sim* s) {
+  DeviceGuard device_guard;   // the caller's current device is restored on return
+  int rc = check_sim(s);
+  if (rc) return rc;
+  if (s->mat_nz < 0) return fail(FDTD_ERR_STATE, "no staged material block (fdtd_fill_layers)");
+  return materials_from_stage(s);
+}
+
+int fdtd_get_staged_materials(fdtd_sim* s, int nz_mat, void* eps_r, void* sigma) {
+  DeviceGuard device_guard;   // the caller's current device is restored on return
+  int rc = check_sim(s);
+  if (rc) return rc;
+  if (!eps_r || !sigma) return fail(FDTD_ERR_INVALID, "null argument");
+  if (s->mat_nz < 0) return fail(FDTD_ERR_STATE, "no staged material block");
+  if (nz_mat != s->mat_nz)
+    return fail(FDTD_ERR_INVALID, "staged block has %d planes, not %d", s->mat_nz, nz_mat);
+  const size_t n = (size_t)s->mat_nz * s->g.ny * s->g.nx * s->esz;
+  CK(cudaMemcpyAsync(eps_r, s->packed, n, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaMemcpyAsync(sigma, s->packed2, n, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
   return FDTD_OK;
 }
 

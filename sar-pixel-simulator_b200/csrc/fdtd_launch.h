@@ -209,6 +209,17 @@ int near_field_power_run(const T* ph, const long long* off, const T* inc, int nx
                          int szm, const double* w_dev, double* partial, int blocks, double* out,
                          cudaStream_t st);
 
+// Material blocks made on the device (fdtd_materials.cu): layers from
+// height maps h (nlayers x (ny, nx) cells, device) with values ev, sv
+// (nlayers + 1, device), and spheres sp (n x (zc, yc, xc, rc, ri), device),
+// into eps / sig volumes (nz_mat, ny, nx).
+template <class T>
+void launch_fill_layers(T* eps, T* sig, int nx, int ny, int nz_mat, int nlayers, const double* h, const double* ev,
+                        const double* sv, cudaStream_t st);
+template <class T>
+void launch_paint_spheres(T* eps, T* sig, int nx, int ny, int nz_mat, const double* sp, int n, double e_val,
+                          double s_val, cudaStream_t st);
+
 // Records an error message for fdtd_last_error(); returns code.
 int report_error(int code, const char* msg);
 

@@ -97,6 +97,10 @@ SIGNATURES = {
     'fdtd_version': [],
     'fdtd_bounds_check_enabled': [],
     'fdtd_near_field_power': [_P, _P, _I, _P, _P],
+    'fdtd_fill_layers': [_P, _I, _I, _P, _P, _P],
+    'fdtd_paint_spheres': [_P, _I, _P, _D, _D],
+    'fdtd_set_materials_staged': [_P],
+    'fdtd_get_staged_materials': [_P, _I, _P, _P],
     'fdtd_device_count': [ctypes.POINTER(_I)],
     'fdtd_device_name': [_I, ctypes.c_char_p, _I],
     'fdtd_create': [ctypes.POINTER(Geometry), _I, ctypes.POINTER(_P)],
@@ -371,6 +375,33 @@ class NativeSim:
 
     def get_fields(self):
         return {c: self.get_field(c) for c in FIELD_NAMES}
+
+    def fill_layers(self, nz_mat, heights, eps_r, sigma):
+        """Stage a material block made on the device from interface height
+        maps (fdtd_fill_layers); heights: (nlayers, ny, nx) cells."""
+        g = self.geom
+        h = np.ascontiguousarray(np.asarray(heights, dtype=np.float64).reshape(-1, g.ny, g.nx))
+        e = np.ascontiguousarray(eps_r, dtype=np.float64)
+        s = np.ascontiguousarray(sigma, dtype=np.float64)
+        if e.shape != (h.shape[0] + 1,) or s.shape != e.shape:
+            raise ValueError('eps_r and sigma need one value per layer and one above')
+        check(lib.fdtd_fill_layers(self.h, int(nz_mat), int(h.shape[0]), ptr(h), ptr(e), ptr(s)))
+
+    def paint_spheres(self, spheres, eps_r, sigma):
+        """Paint (n, 5) spheres (zc, yc, xc, rc, ri in cells) into the
+        staged block (fdtd_paint_spheres)."""
+        sp = np.ascontiguousarray(np.asarray(spheres, dtype=np.float64).reshape(-1, 5))
+        check(lib.fdtd_paint_spheres(self.h, int(sp.shape[0]), ptr(sp), float(eps_r), float(sigma)))
+
+    def set_materials_staged(self):
+        check(lib.fdtd_set_materials_staged(self.h))
+
+    def get_staged_materials(self, nz_mat):
+        g = self.geom
+        e = np.empty((nz_mat, g.ny, g.nx), self.dtype)
+        s = np.empty_like(e)
+        check(lib.fdtd_get_staged_materials(self.h, int(nz_mat), ptr(e), ptr(s)))
+        return e, s
 
     def near_field_power(self, inc_phasors, size_z_material, weights):
         """The 11 face powers of fdtd_near_field_power (incident, left /

@@ -101,7 +101,7 @@ def run_experiment(params: ParameterCollection, materials: Iterable[MaterialMode
         # the first model sets the geometry before any other model is made
         first = next(it, None)
         if first is not None:
-            nz_mat, ny, nx = first.conductivity.shape
+            nz_mat, ny, nx = _shape(first)
             dx = first.cell_size
             set_geom_params(params, nx * dx, ny * dx, nz_mat * dx,
                             params.geom_params.simulation_duration, dx, 'metre')
@@ -116,7 +116,19 @@ def run_experiment(params: ParameterCollection, materials: Iterable[MaterialMode
     wait_written()       # every incident file of this experiment is on disk
 
 
+def _shape(material):
+    from .materials.device import LayeredMaterial
+    if isinstance(material, LayeredMaterial):
+        return material.shape
+    return material.conductivity.shape
+
+
 def _simulate(sim, material: MaterialModel):
+    from .materials.device import LayeredMaterial
+    if isinstance(material, LayeredMaterial):
+        # the block made on the device from its recipe
+        sim.run_layered(material)
+        return
     # Ca/Cb on the device: the values compute_material_arrays gives
     sim.run_eps_sigma(material.relative_permittivity, material.conductivity,
                       material.name, material.metadata)

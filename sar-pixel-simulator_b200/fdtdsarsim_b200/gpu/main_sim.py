@@ -164,6 +164,29 @@ class MainSimGpu:
         self.native.run(self.params.geom_params.size_t)
         self.native.synchronize()
 
+    def simulate_layered(self, recipe):
+        """As simulate, with the material block made on the device from a
+        LayeredMaterial recipe (fdtd_fill_layers, fdtd_paint_spheres) and
+        Ca/Cb computed from it."""
+        self.native.reset()
+        recipe.stage(self.native)
+        self.native.set_materials_staged()
+        self._ensure_incident()
+        self.native.run(self.params.geom_params.size_t)
+        self.native.synchronize()
+
+    def run_layered(self, recipe):
+        """run() for a material model given as a LayeredMaterial recipe
+        (materials/device.py): the device fills the block, so it is never
+        made on the host nor uploaded; the result file is the one
+        run_eps_sigma writes for recipe.to_model()."""
+        g = self.params.geom_params
+        want = (g.size_z_material, g.size_y, g.size_x)
+        if tuple(recipe.shape) != want:
+            raise ValueError(f'material block is {tuple(recipe.shape)}, expected {want}')
+        self.Ca = self.Cb = None
+        self._run_and_save(lambda: self.simulate_layered(recipe), recipe.name, recipe.metadata)
+
     def run(self, Ca: np.ndarray, Cb: np.ndarray, material_name: str, material_meta: dict):
         """Simulate one material model and save its phasors
         (gpu/main_sim.py:74-115)."""

@@ -53,12 +53,25 @@ def _paint(eps, cond, surf, rng, target, vol, r_min, r_max, fixed_radius, cell, 
 
 
 def _fill(mat_model, surf_height_cells, bubble_frac, r_min, r_max, fixed, eps_b, cond_b, seed):
+    from .device import LayeredMaterial, bubble_spheres
+    if isinstance(mat_model, LayeredMaterial):
+        # a recipe made on the device: the same draws as a sphere list
+        vol = mat_model.material_volume() if not mat_model.spheres else \
+            int(material_volume(*_arrays(mat_model.to_model())))
+        sp = bubble_spheres(mat_model.shape, vol, surf_height_cells, bubble_frac, r_min, r_max, fixed,
+                            mat_model.cell_size, seed)
+        mat_model.spheres.append((sp, eps_b, cond_b))
+        return
     rng = np.random.default_rng(seed=seed)
     vol = int(material_volume(mat_model.relative_permittivity, mat_model.conductivity))
     target = int(round(vol * (1.0 - bubble_frac)))
     _paint(mat_model.relative_permittivity, mat_model.conductivity,
            np.asarray(surf_height_cells, dtype=np.float64), rng, target, vol, float(r_min),
            float(r_max), fixed, float(mat_model.cell_size), eps_b, cond_b)
+
+
+def _arrays(model):
+    return model.relative_permittivity, model.conductivity
 
 
 def add_bubbles(mat_model: MaterialModel, surf_height_cells: np.ndarray, bubble_frac: float,

@@ -59,12 +59,14 @@ def flat_surface(params: ParameterCollection, epsilon_r: float, conductivity: fl
 
 def rough_dielectric(params: ParameterCollection, epsilon_r: float, conductivity: float,
                      height_rms: float, mean_depth: float, corr_len: float, count: int,
-                     seed=None):
+                     seed=None, device=False):
     """``count`` models of one dielectric under a Gaussian-correlated rough
     surface of mean depth ``mean_depth`` [m] (materials/materials.py:
     112-164): a cell is dielectric when its z index is at most the surface
     height in cells. The reference draws unseeded surfaces; ``seed`` (this
-    package's addition) makes surface i use seed + i."""
+    package's addition) makes surface i use seed + i. With ``device`` (this
+    package's addition) the models are LayeredMaterial recipes that the
+    device fills."""
     from .roughsurface import gaussian_correlated_surface
     g = params.geom_params
     nx, ny, nz, dx = g.size_x, g.size_y, g.size_z_material, g.cell_size
@@ -81,6 +83,11 @@ def rough_dielectric(params: ParameterCollection, epsilon_r: float, conductivity
                                         seed=None if seed is None else seed + i)
         h /= dx
         h += mean_cells
+        if device:
+            from .device import LayeredMaterial
+            yield LayeredMaterial((nz, ny, nx), dx, h[None], [epsilon_r, 1.0], [conductivity, 0.0],
+                                  f'rough_surf_{i}', dict(meta), dtype)
+            continue
         below = z <= h[np.newaxis]
         yield MaterialModel(np.where(below, epsilon_r, 1.0).astype(dtype),
                             np.where(below, conductivity, 0.0).astype(dtype), dx,

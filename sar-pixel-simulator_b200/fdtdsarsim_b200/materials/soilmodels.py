@@ -42,11 +42,13 @@ def _z(nz):
 
 def one_layer_gaussian(params: ParameterCollection, moistures: Sequence[float], sand_frac: float,
                        clay_frac: float, height_rms: float, corr_len: float, mean_depth: float,
-                       count: int, seed: int, grooved: bool = False, rabus_compat: bool = False):
+                       count: int, seed: int, grooved: bool = False, rabus_compat: bool = False,
+                       device: bool = False):
     """One soil layer under a rough surface of mean depth ``mean_depth`` [m]
     (materials/soilmodels.py:16-90): ``count`` surfaces (seeds seed + i),
     each with every moisture in ``moistures``; ``grooved`` repeats the
-    surface's first row along y."""
+    surface's first row along y. ``device`` (this package's addition)
+    yields LayeredMaterial recipes that the device fills."""
     nx, ny, nz, dx, dtype, freq = _geometry(params, mean_depth)
     mean_cells = mean_depth / dx
     model = HallikainenSoilModel()
@@ -64,6 +66,11 @@ def one_layer_gaussian(params: ParameterCollection, moistures: Sequence[float], 
             meta = {'moisture': mv, 'sand_frac': sand_frac, 'clay_frac': clay_frac,
                     'epsilon_r': eps_r, 'conductivity': sigma, 'height_rms': height_rms,
                     'mean_depth': mean_depth, 'mean_depth_cells': mean_cells, 'corr_len': corr_len}
+            if device:
+                from .device import LayeredMaterial
+                yield LayeredMaterial((nz, ny, nx), dx, h[None].astype(np.float64), [eps_r, 1.0],
+                                      [sigma, 0.0], f'mv_{mv:.2f}_num_{i}', meta, dtype)
+                continue
             eps = np.where(below, eps_r, 1.0).astype(dtype)
             sig = np.where(below, sigma, 0.0).astype(dtype)
             yield MaterialModel(eps, sig, dx, f'mv_{mv:.2f}_num_{i}', meta)
@@ -91,9 +98,10 @@ def two_layer_gaussian(params: ParameterCollection, top_moisture: float,
                        bottom_moistures: Sequence[float], sand_frac: float, clay_frac: float,
                        height_rms: float, corr_len: float, inter_layer_corr: float,
                        mean_total_depth: float, top_layer_height: float, count: int, seed: int,
-                       grooved: bool = False, rabus_compat: bool = False):
+                       grooved: bool = False, rabus_compat: bool = False, device: bool = False):
     """Two soil layers of different moisture under two correlated rough
-    surfaces (materials/soilmodels.py:93-195)."""
+    surfaces (materials/soilmodels.py:93-195); ``device`` (this package's
+    addition) yields LayeredMaterial recipes that the device fills."""
     nx, ny, nz, dx, dtype, freq = _geometry(params, mean_total_depth)
     _check_layers(mean_total_depth, top_layer_height, dx)
     model = HallikainenSoilModel()
@@ -113,6 +121,11 @@ def two_layer_gaussian(params: ParameterCollection, top_moisture: float,
                     'total_depth_cells': mean_total_depth / dx,
                     'top_layer_height': top_layer_height, 'top_layer_cells': top_layer_height / dx,
                     'inter_layer_corr': inter_layer_corr, 'corr_len': corr_len}
+            if device:
+                from .device import LayeredMaterial
+                yield LayeredMaterial((nz, ny, nx), dx, h.astype(np.float64), [eps_bot, eps_top, 1.0],
+                                      [sig_bot, sig_top, 0.0], f'mv_{mv:.2f}_num_{i}', meta, dtype)
+                continue
             eps = np.where(bottom, eps_bot, np.where(top, eps_top, 1.0)).astype(dtype)
             sig = np.where(bottom, sig_bot, np.where(top, sig_top, 0.0)).astype(dtype)
             yield MaterialModel(eps, sig, dx, f'mv_{mv:.2f}_num_{i}', meta)
