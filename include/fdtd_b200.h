@@ -359,9 +359,7 @@ int fdtd_check_cell_division(int dtype, double cell_size, int device, int64_t *t
  * (FDTD_SHELL_MARCH, the default step). Rows of 7 ints (kind, x0, x1, y0,
  * y1, z0, z1), kind 0 the interior z-march, 1 the CPML z slabs, 2 a shell
  * box swept by the split passes, 3 a shell box of the general march; every
- * cell lies in exactly one box of kinds 0-3. Kind 4 (modes 0 and 1): the
- * near layer, shell vectors whose E update reads H a march writes, updated
- * after the marches (the rest of the shell E pass runs beside them). */
+ * cell lies in exactly one box. */
 int fdtd_fused_plan_boxes(int nx, int ny, int nz, int npml, int tfsf_z, int tile_y, int zchunk,
                           int mode, int *out, int cap, int *count);
 

@@ -383,18 +383,14 @@ int enqueue_steps(fdtd_sim* s, int n, bool phasors = true) {
         CK(cudaEventRecord(s->join, s->side));
         CK(cudaStreamWaitEvent(s->stream, s->join, 0));
       } else {
-        // side stream: the shell H pass, then the E pass of every shell
-        // cell that reads shell H only (far), beside the interior march;
-        // after both, the E pass of the near layer
-        State<T> se = st;
-        se.ihx = (const T*)s->fld[nxt][3]; se.ihy = (const T*)s->fld[nxt][4]; se.ihz = (const T*)s->fld[nxt][5];
         launch_shell_pass<T>(st, s->tdev, k, s->plan.shell, true, s->side);
-        launch_shell_pass<T>(se, s->tdev, k, s->plan.shell, false, s->side, &s->plan.near);
         launch_fused_interior<T>(st, s->plan, s->tile_y, s->stream);
         launch_fused_slab<T>(st, s->plan, s->tile_y, s->stream);
         CK(cudaEventRecord(s->join, s->side));
         CK(cudaStreamWaitEvent(s->stream, s->join, 0));
-        launch_shell_pass<T>(se, s->tdev, k, s->plan.near_boxes, false, s->stream);
+        State<T> se = st;
+        se.ihx = (const T*)s->fld[nxt][3]; se.ihy = (const T*)s->fld[nxt][4]; se.ihz = (const T*)s->fld[nxt][5];
+        launch_shell_pass<T>(se, s->tdev, k, s->plan.shell, false, s->stream);
       }
       s->cur = nxt;
       mark(s, e1);
@@ -2121,10 +2117,6 @@ int fdtd_fused_plan_boxes(int nx, int ny, int nz, int npml, int tfsf_z, int tile
   for (int k = 0; k < p.mshell.n; ++k) {
     const MarchBox& b = p.mshell.b[k];
     put(3, b.x0, b.x1, b.y0, b.y1, b.z0, b.z1);
-  }
-  for (int k = 0; k < p.near.n; ++k) {
-    const int* b = p.near.b[k];
-    put(4, b[0], b[1], b[2], b[3], b[4], b[5]);
   }
   *count = n;
   return n <= cap ? FDTD_OK : fail(FDTD_ERR_INVALID, "%d boxes, room for %d", n, cap);

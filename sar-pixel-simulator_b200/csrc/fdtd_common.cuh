@@ -129,15 +129,6 @@ struct ShellBoxes {
   ShellBox b[kMaxShellBoxes];
 };
 
-// Boxes [x0, x1) x [y0, y1) x [z0, z1) (x0, x1 multiples of 4) whose
-// vectors a shell pass leaves alone: the fused step's near layer, the shell
-// cells whose E update reads H that the interior or slab march writes.
-constexpr int kMaxSkipBoxes = 12;
-struct SkipBoxes {
-  int n;
-  int b[kMaxSkipBoxes][6];
-};
-
 // A box of the fused step's shell marched in z by the general kernel
 // (fdtd_march.cu): [x0, x1) x [y0, y1) x [z0, z1), x0 a multiple of 4. A
 // block is kMarchThreads threads: `width` lanes of 4 x cells by

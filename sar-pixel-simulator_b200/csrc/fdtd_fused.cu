@@ -349,46 +349,7 @@ FusedPlan make_fused_plan(int nx, int ny, int nz, int npml, int tfsf_z, int tile
     add(0, ib.xa, ib.ya, ib.yb, cz0[k], cz1[k]);
     add(ib.xb, nx, ib.ya, ib.yb, cz0[k], cz1[k]);
   }
-  if (march) {
-    finish_march_boxes(p.mshell);
-    return p;
-  }
-  // the near layer of the split-pass shell: the shell cells just past a
-  // march box's high x, y and z faces, whose E update reads H the march
-  // writes (E at (z, y, x) reads H at x - 1, y - 1, z - 1); every other
-  // shell cell reads shell H only, so its E update can follow the shell H
-  // pass at once, beside the marches
-  int mb[4][6], nm = 0;
-  for (int k = 0; k < nzr; ++k) {
-    const int b[6] = {ib.xa, ib.xb, ib.ya, ib.yb, ib.z0[k], ib.z1[k]};
-    memcpy(mb[nm++], b, sizeof(b));
-  }
-  for (int k = 0; k < sb.nz_ranges; ++k) {
-    const int b[6] = {sb.xa, sb.xb, sb.ya, sb.yb, sb.z0[k], sb.z1[k]};
-    memcpy(mb[nm++], b, sizeof(b));
-  }
-  auto marched_plane = [&](int z) {
-    for (int k = 0; k < nm; ++k)
-      if (z >= mb[k][4] && z < mb[k][5]) return true;
-    return false;
-  };
-  auto add_near = [&](int x0, int x1, int y0, int y1, int z0, int z1) {
-    if (x0 >= x1 || y0 >= y1 || z0 >= z1) return;
-    if (p.near.n >= kMaxSkipBoxes) {
-      ++p.shell.dropped;
-      return;
-    }
-    int* b = p.near.b[p.near.n++];
-    b[0] = x0; b[1] = x1; b[2] = y0; b[3] = y1; b[4] = z0; b[5] = z1;
-    add_shell_box(p.near_boxes, x0, x1, y0, y1, z0, z1);
-  };
-  for (int k = 0; k < nm; ++k) {
-    const int* b = mb[k];
-    add_near(b[1], b[1] + kVec, b[2], b[3], b[4], b[5]);                 // x = xb
-    if (b[3] < ny) add_near(b[0], b[1], b[3], b[3] + 1, b[4], b[5]);     // y = yb
-    if (b[5] < nz && !marched_plane(b[5])) add_near(b[0], b[1], b[2], b[3], b[5], b[5] + 1);   // z = z1
-  }
-  if (p.near_boxes.dropped) ++p.shell.dropped;
+  if (march) finish_march_boxes(p.mshell);
   return p;
 }
 

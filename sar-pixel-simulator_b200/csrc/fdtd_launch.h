@@ -90,11 +90,6 @@ struct FusedPlan {
   int has_slab;
   InteriorBox slab;   // the z slabs [0, npml), [nz - npml, nz) of the same x-y box
   ShellBoxes shell;   // the shell swept by the split passes (shell mode 1)
-  // the shell's near layer (cells whose E update reads H that the interior
-  // or slab march writes): left out of the E pass that runs beside the
-  // marches (far), swept by a short E pass after them (near)
-  SkipBoxes near;
-  ShellBoxes near_boxes;
   int march;          // shell mode 0: the shell is marched by k_march
   MarchBoxes mshell;  // the shell's boxes for k_march (shell mode 0)
 };
@@ -134,11 +129,10 @@ bool launch_fused_slab(const State<T>& s, const FusedPlan& p, int tile_y, cudaSt
 void add_shell_box(ShellBoxes& bl, int x0, int x1, int y0, int y1, int z0, int z1);
 
 // Split H pass (h_pass) or E pass over the shell boxes, from the State's
-// source pointers to its destination pointers; vectors inside `skip` (if
-// given) are left alone.
+// source pointers to its destination pointers.
 template <class T>
 void launch_shell_pass(const State<T>& s, const int* tdev, int toff, const ShellBoxes& bl,
-                       bool h_pass, cudaStream_t st, const SkipBoxes* skip = nullptr);
+                       bool h_pass, cudaStream_t st);
 
 // One transposed step (fdtd_adjoint.cu): s holds E^n in its source E
 // pointers, H^{n+1/2} in its source H pointers and the CPML auxiliaries

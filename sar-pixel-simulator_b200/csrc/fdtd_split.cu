@@ -111,9 +111,9 @@ __device__ __forceinline__ const ShellBox& find_box(const ShellBoxes& bl, int bi
 template <class T>
 constexpr int split_min_blocks() { return sizeof(T) == 4 ? 8 : 1; }
 
-template <class T, bool kH, bool kSkip>
+template <class T, bool kH>
 __global__ void __launch_bounds__(128, split_min_blocks<T>()) k_shell(State<T> s, const int* __restrict__ tp, int toff,
-                                               ShellBoxes bl, SkipBoxes skip) {
+                                               ShellBoxes bl) {
   const int bid = blockIdx.x;
   const ShellBox& b = find_box(bl, bid);
   int local = bid - b.first;
@@ -125,12 +125,7 @@ __global__ void __launch_bounds__(128, split_min_blocks<T>()) k_shell(State<T> s
   const int x0 = b.x0 + (bx * b.width + lane) * kVec;
   const int y = b.y0 + by * (128 / b.width) + row;
   const int z = b.z0 + bz;
-  bool act = x0 < b.x1 && y < b.y1;
-  if (kSkip)
-    for (int k = 0; k < skip.n; ++k)
-      if (x0 >= skip.b[k][0] && x0 < skip.b[k][1] && y >= skip.b[k][2] && y < skip.b[k][3] && z >= skip.b[k][4] &&
-          z < skip.b[k][5])
-        act = false;
+  const bool act = x0 < b.x1 && y < b.y1;
   if (kH) h_split_vec(s, *tp + toff, z, y, x0, lane, b.width, act);
   else e_split_vec(s, *tp + toff, z, y, x0, lane, b.width, act);
 }
@@ -383,17 +378,10 @@ void launch_batch_advance(const BatchModel<T>* bm, int n, int steps, cudaStream_
 
 template <class T>
 void launch_shell_pass(const State<T>& s, const int* tdev, int toff, const ShellBoxes& bl,
-                       bool h_pass, cudaStream_t st, const SkipBoxes* skip) {
+                       bool h_pass, cudaStream_t st) {
   if (bl.n == 0 || bl.total_blocks == 0) return;
-  SkipBoxes none;
-  none.n = 0;
-  if (skip && skip->n > 0) {
-    if (h_pass) k_shell<T, true, true><<<bl.total_blocks, 128, 0, st>>>(s, tdev, toff, bl, *skip);
-    else k_shell<T, false, true><<<bl.total_blocks, 128, 0, st>>>(s, tdev, toff, bl, *skip);
-    return;
-  }
-  if (h_pass) k_shell<T, true, false><<<bl.total_blocks, 128, 0, st>>>(s, tdev, toff, bl, none);
-  else k_shell<T, false, false><<<bl.total_blocks, 128, 0, st>>>(s, tdev, toff, bl, none);
+  if (h_pass) k_shell<T, true><<<bl.total_blocks, 128, 0, st>>>(s, tdev, toff, bl);
+  else k_shell<T, false><<<bl.total_blocks, 128, 0, st>>>(s, tdev, toff, bl);
 }
 
 void launch_advance(int* tdev, int n, cudaStream_t st) {
@@ -457,9 +445,9 @@ void launch_eps_sigma(int nx, int ny, int nz, int nz_mat, int pitch, const T* ep
 template void launch_split_step<float>(const State<float>&, const int*, int, cudaStream_t);
 template void launch_split_step<double>(const State<double>&, const int*, int, cudaStream_t);
 template void launch_shell_pass<float>(const State<float>&, const int*, int, const ShellBoxes&,
-                                       bool, cudaStream_t, const SkipBoxes*);
+                                       bool, cudaStream_t);
 template void launch_shell_pass<double>(const State<double>&, const int*, int, const ShellBoxes&,
-                                        bool, cudaStream_t, const SkipBoxes*);
+                                        bool, cudaStream_t);
 template void launch_batch_step<float>(const BatchModel<float>*, const int*, int, int, const int*,
                                        int, int, cudaStream_t);
 template void launch_batch_step<double>(const BatchModel<double>*, const int*, int, int,

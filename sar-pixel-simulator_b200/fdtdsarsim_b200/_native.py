@@ -547,9 +547,8 @@ def fused_plan_boxes(nx, ny, nz, npml, tfsf_z, tile_y=4, zchunk=0, slab=False, m
     """(kind, x0, x1, y0, y1, z0, z1) rows of the fused step's boxes
     (fdtd_fused_plan_boxes; host computation, no device needed): kind 0
     interior march, 1 CPML z slab march, 2 split-pass shell box, 3 general
-    march shell box, 4 near-layer box of the split-pass shell (inside kind
-    2 boxes). ``march`` gives the plan with the shell marched; otherwise the
-    split-pass shell, with ``slab`` the z slabs marched."""
+    march shell box. ``march`` gives the default step's plan (shell marched);
+    otherwise the split-pass shell, with ``slab`` the z slabs marched."""
     out = np.zeros((64, 7), np.int32)
     n = ctypes.c_int(0)
     mode = 2 if march else int(bool(slab))

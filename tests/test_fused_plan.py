@@ -27,32 +27,9 @@ def test_boxes_partition_the_grid(grid, tile_y, mode):
     # the march plan sends the whole shell to the general march, the others
     # to the split passes
     shell_kind = 3 if mode == 'march' else 2
-    assert set(boxes[:, 0]) <= {0, 1, shell_kind, 4}
+    assert set(boxes[:, 0]) <= {0, 1, shell_kind}
     if mode != 'slab':
         assert 1 not in boxes[:, 0]
-    near = boxes[boxes[:, 0] == 4]
-    boxes = boxes[boxes[:, 0] != 4]
-    if mode == 'march':
-        assert len(near) == 0
-    else:
-        # the near layer: every shell cell whose -x, -y or -z neighbour a
-        # march updates lies in a near box; near boxes hold shell cells only
-        # (whole vectors: x bounds on vector edges)
-        marched = np.zeros((nz, ny, nx), bool)
-        shell = np.zeros((nz, ny, nx), bool)
-        for kind, x0, x1, y0, y1, z0, z1 in boxes:
-            (marched if kind in (0, 1) else shell)[z0:z1, y0:y1, x0:x1] = True
-        need = np.zeros_like(shell)
-        need[:, :, 1:] |= marched[:, :, :-1]
-        need[:, 1:, :] |= marched[:, :-1, :]
-        need[1:, :, :] |= marched[:-1, :, :]
-        need &= shell
-        got = np.zeros_like(shell)
-        for _, x0, x1, y0, y1, z0, z1 in near:
-            assert x0 % 4 == 0 and x1 % 4 == 0
-            got[z0:z1, y0:y1, x0:min(x1, nx)] = True
-        assert not (need & ~got).any()
-        assert not (got & ~shell).any()
     count = np.zeros((nz, ny, nx), np.int32)
     for kind, x0, x1, y0, y1, z0, z1 in boxes:
         assert x0 % 4 == 0
