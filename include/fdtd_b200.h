@@ -260,7 +260,8 @@ int fdtd_near2far(const void *ex_u, const void *ey_u, const void *hx_u,
  * the order above). The backward sweep recomputes each segment of steps
  * from its checkpoint and runs the transposed step backwards through it.
  * Outputs: dJ/dCa and dJ/dCb of the first nz_out planes, (nz_out, ny, nx)
- * float64. The simulation keeps the forward solve's fields and phasors.
+ * float64. The simulation keeps the forward solve's fields and its four
+ * upper-plane phasors (the forward accumulates no other phasor plane).
  * Device memory: (size_t / checkpoint_every + 2 checkpoint_every) states of
  * 6 fields and the CPML auxiliaries, plus the adjoint state. */
 int fdtd_grad_forward(fdtd_sim *s, int checkpoint_every);

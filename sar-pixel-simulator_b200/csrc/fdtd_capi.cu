@@ -342,8 +342,10 @@ int collect_timing(fdtd_sim* s) {
   return FDTD_OK;
 }
 
+// ph_g0, ph_ng: the phasor plane groups each step accumulates (all six by
+// default; none with ph_ng = 0; the gradient's forward only the upper plane)
 template <class T>
-int enqueue_steps(fdtd_sim* s, int n, bool phasors = true) {
+int enqueue_steps(fdtd_sim* s, int n, int ph_g0 = 0, int ph_ng = 6) {
   for (int k = 0; k < n; ++k) {
     if (s->timing && s->ev_used + 3 > 3 * 4096) {
       int rc = collect_timing(s);
@@ -395,12 +397,12 @@ int enqueue_steps(fdtd_sim* s, int n, bool phasors = true) {
       s->cur = nxt;
       mark(s, e1);
       State<T> sp = make_state<T>(s, s->cur, s->cur);
-      if (phasors) launch_phasors<T>(sp, s->tdev, k, s->stream);
+      launch_phasors<T>(sp, s->tdev, k, s->stream, ph_g0, ph_ng);
     } else {
       State<T> st = make_state<T>(s, s->cur, s->cur);
       launch_split_step<T>(st, s->tdev, k, s->stream);
       mark(s, e1);
-      if (phasors) launch_phasors<T>(st, s->tdev, k, s->stream);
+      launch_phasors<T>(st, s->tdev, k, s->stream, ph_g0, ph_ng);
     }
     mark(s, e2);
     const long long done = s->t + k + 1;
@@ -1892,7 +1894,8 @@ int fdtd_grad_forward(fdtd_sim* s, int checkpoint_every) {
   for (int c = 0; c < ncp; ++c) {
     if ((rc = save_state(s, static_cast<unsigned char*>(s->grad_cp) + c * sb))) return rc;
     const int n = std::min(checkpoint_every, nt - c * checkpoint_every);
-    rc = s->g.dtype == FDTD_F32 ? enqueue_steps<float>(s, n) : enqueue_steps<double>(s, n);
+    // the objective reads the upper plane's phasors only (plane group 1)
+    rc = s->g.dtype == FDTD_F32 ? enqueue_steps<float>(s, n, 1, 1) : enqueue_steps<double>(s, n, 1, 1);
     if (rc) return rc;
     s->t += n;
   }
@@ -1999,7 +2002,7 @@ int incident_run(fdtd_incident* b) {
     // destination set, and the next step's source goes onto the destination
     for (int t = 0; t < g.nt; ++t) {
       const int src = s->cur;
-      if ((rc = enqueue_steps<T>(s, 1, false))) return rc;
+      if ((rc = enqueue_steps<T>(s, 1, 0, 0))) return rc;
       r.ex = (const T*)s->fld[src][0]; r.ey = (const T*)s->fld[src][1];
       r.hx = (const T*)s->fld[s->cur][3]; r.hy = (const T*)s->fld[s->cur][4];
       launch_inc_record<T>(r, t, s->stream);

@@ -29,8 +29,10 @@ struct DeviceGuard {
 template <class T>
 void launch_split_step(const State<T>& s, const int* tdev, int toff, cudaStream_t st);
 
+// The phasor pass over plane groups g0 .. g0 + ng - 1 (0 d, 1 u, 2 l, 3 r,
+// 4 f, 5 b).
 template <class T>
-void launch_phasors(const State<T>& s, const int* tdev, int toff, cudaStream_t st);
+void launch_phasors(const State<T>& s, const int* tdev, int toff, cudaStream_t st, int g0 = 0, int ng = 6);
 
 void launch_advance(int* tdev, int n, cudaStream_t st);
 

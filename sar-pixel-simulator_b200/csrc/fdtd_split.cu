@@ -211,10 +211,10 @@ __device__ __forceinline__ void phasor_cell(const State<T>& s, int g, int idx, i
   }
 }
 
-// One thread per phasor cell; blockIdx.y selects the plane group.
+// One thread per phasor cell; g0 + blockIdx.y selects the plane group.
 template <class T>
-__global__ void __launch_bounds__(256) k_phasors(State<T> s, const int* __restrict__ tp, int toff) {
-  phasor_cell(s, (int)blockIdx.y, (int)(blockIdx.x * blockDim.x + threadIdx.x), *tp + toff);
+__global__ void __launch_bounds__(256) k_phasors(State<T> s, const int* __restrict__ tp, int toff, int g0) {
+  phasor_cell(s, g0 + (int)blockIdx.y, (int)(blockIdx.x * blockDim.x + threadIdx.x), *tp + toff);
 }
 
 // ---------------------------------------------------------------------------
@@ -349,12 +349,13 @@ void launch_split_step(const State<T>& s, const int* tdev, int toff, cudaStream_
 }
 
 template <class T>
-void launch_phasors(const State<T>& s, const int* tdev, int toff, cudaStream_t st) {
+void launch_phasors(const State<T>& s, const int* tdev, int toff, cudaStream_t st, int g0, int ng) {
+  if (ng <= 0) return;
   int n = s.ny_ph * s.nx_ph;
   n = max(n, s.nz_ph * s.ny_ph);
   n = max(n, s.nz_ph * s.nx_ph);
-  const dim3 grd((n + 255) / 256, 6, 1);
-  k_phasors<T><<<grd, 256, 0, st>>>(s, tdev, toff);
+  const dim3 grd((n + 255) / 256, ng, 1);
+  k_phasors<T><<<grd, 256, 0, st>>>(s, tdev, toff, g0);
 }
 
 template <class T>
@@ -458,8 +459,8 @@ template void launch_batch_phasors<double>(const BatchModel<double>*, const int*
                                            cudaStream_t);
 template void launch_batch_advance<float>(const BatchModel<float>*, int, int, cudaStream_t);
 template void launch_batch_advance<double>(const BatchModel<double>*, int, int, cudaStream_t);
-template void launch_phasors<float>(const State<float>&, const int*, int, cudaStream_t);
-template void launch_phasors<double>(const State<double>&, const int*, int, cudaStream_t);
+template void launch_phasors<float>(const State<float>&, const int*, int, cudaStream_t, int, int);
+template void launch_phasors<double>(const State<double>&, const int*, int, cudaStream_t, int, int);
 template void launch_eps_sigma<float>(int, int, int, int, int, const float*, const float*, float,
                                       float, float, float*, float*, cudaStream_t);
 template void launch_eps_sigma<double>(int, int, int, int, int, const double*, const double*,
