@@ -355,9 +355,9 @@ int fdtd_check_cell_division(int dtype, double cell_size, int device, int64_t *t
 
 /* Diagnostic (no counterpart in the reference): the boxes of the fused
  * step's decomposition of a grid, host computation only (no device use).
- * mode 0: the shell by the split passes (FDTD_SHELL_SPLIT), 1: the same
- * with the CPML z slabs marched (FDTD_OPT_FUSED_SLAB), 2: the shell marched
- * (FDTD_SHELL_MARCH, the default step). Rows of 7 ints (kind, x0, x1, y0,
+ * mode 0: the shell by the split passes (FDTD_SHELL_SPLIT, the default
+ * step), 1: the same with the CPML z slabs marched (FDTD_OPT_FUSED_SLAB),
+ * 2: the shell marched (FDTD_SHELL_MARCH). Rows of 7 ints (kind, x0, x1, y0,
  * y1, z0, z1), kind 0 the interior z-march, 1 the CPML z slabs, 2 a shell
  * box swept by the split passes, 3 a shell box of the general march; every
  * cell lies in exactly one box. */
