@@ -50,6 +50,8 @@ def parse():
     ap.add_argument('--shell', default=None, choices=['march', 'split'],
                     help='fused kernel: shell marched or swept by the split passes')
     ap.add_argument('--zchunk', type=int, default=0, help='fused kernel z planes per block (0: auto)')
+    ap.add_argument('--slab', type=int, default=None, choices=[0, 1],
+                    help='fused kernel: march the CPML z slabs (1) or sweep them with the shell (0)')
     ap.add_argument('--dtype', default='float32', choices=['float32', 'float64'])
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-cpu-baseline', action='store_true')
@@ -303,6 +305,8 @@ def run_ours(a):
         choice['zchunk'] = a.zchunk
         if a.shell is not None:
             choice['shell'] = _native.SHELL_MARCH if a.shell == 'march' else _native.SHELL_SPLIT
+        if a.slab is not None:
+            choice['slab'] = a.slab
 
     def new_sim():
         sim = _native.NativeSim(geom, local)

@@ -385,9 +385,10 @@ int enqueue_steps(fdtd_sim* s, int n, int ph_g0 = 0, int ph_ng = 6) {
         CK(cudaEventRecord(s->join, s->side));
         CK(cudaStreamWaitEvent(s->stream, s->join, 0));
       } else {
+        // the z slabs' march and the shell H pass beside the interior march
+        launch_fused_slab<T>(st, s->plan, s->tile_y, s->side);
         launch_shell_pass<T>(st, s->tdev, k, s->plan.shell, true, s->side);
         launch_fused_interior<T>(st, s->plan, s->tile_y, s->stream);
-        launch_fused_slab<T>(st, s->plan, s->tile_y, s->stream);
         CK(cudaEventRecord(s->join, s->side));
         CK(cudaStreamWaitEvent(s->stream, s->join, 0));
         State<T> se = st;

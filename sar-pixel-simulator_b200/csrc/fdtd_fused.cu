@@ -71,8 +71,12 @@ k_fused_interior(const __grid_constant__ State<T> s, InteriorBox ib) {
 // the same component as the split kernels apply them; the domain's first and
 // last planes keep the components outside their update ranges
 // (cpu/field_updates.py:18-63, 198-240). No x or y face touches the box.
+// (four blocks per SM in float32 at 4-row tiles: the interior's 95 registers)
 template <class T, int TY>
-__global__ void __launch_bounds__(kLanes * (TY + 1), 1)
+constexpr int slab_min_blocks() { return sizeof(T) == 4 && TY <= 4 ? 4 : 1; }
+
+template <class T, int TY>
+__global__ void __launch_bounds__(kLanes * (TY + 1), slab_min_blocks<T, TY>())
 k_fused_slab(const __grid_constant__ State<T> s, InteriorBox ib) {
   using M = R<T>;
   __shared__ __align__(32) T sEx[TY + 1][kRowCells];
@@ -259,8 +263,11 @@ FusedPlan make_fused_plan(int nx, int ny, int nz, int npml, int tfsf_z, int tile
   if (march) use_slab = false;
   const int m = npml;
   InteriorBox& ib = p.interior;
-  // rows start on a 128-byte line (starting at npml rounded up to 4 cells
-  // instead left 48-byte offsets and measured 5 % slower at 203 x 761 x 761)
+  // rows start on a 128-byte line. Measured at 203 x 761 x 761 against
+  // starting at npml rounded up to 4 cells: 5 % slower with 48-byte row
+  // offsets; no faster with the arrays' origin shifted to align that
+  // column, nor with tiles from column 0 whose lanes left of the box only
+  // feed the shuffle (the narrower x strips of the shell took as long)
   ib.xa = (m + 31) / 32 * 32;
   ib.xb = (nx - m) / kVec * kVec;
   ib.ya = m;

@@ -166,8 +166,57 @@ __device__ __forceinline__ double mean4(T a, T b, T c, T d) {
   return 0.25 * (double)M::add(M::add(M::add(a, b), c), d);
 }
 
+// one complex phasor value (re, im) as a single 8-byte (float) or 16-byte
+// (double) access: planes start at even element offsets of an aligned base
+template <class T>
+__device__ __forceinline__ void ld2(T (&d)[2], const T* p) {
+  if (!FDTD_CHECK_PTR(p, 2 * (int)sizeof(T))) {   // bounds-checked build only
+    d[0] = d[1] = T(0);
+    return;
+  }
+  if constexpr (sizeof(T) == 4) {
+    const float2 v = *reinterpret_cast<const float2*>(p);
+    d[0] = v.x; d[1] = v.y;
+  } else {
+    const double2 v = *reinterpret_cast<const double2*>(p);
+    d[0] = v.x; d[1] = v.y;
+  }
+}
+
+template <class T>
+__device__ __forceinline__ void st2(T* p, T re, T im) {
+  if (!FDTD_CHECK_PTR(p, 2 * (int)sizeof(T))) return;   // bounds-checked build only
+  if constexpr (sizeof(T) == 4) *reinterpret_cast<float2*>(p) = make_float2(re, im);
+  else *reinterpret_cast<double2*>(p) = make_double2(re, im);
+}
+
+// The four components of one phasor cell: base plane `base`, field means
+// m[0..3] (E, E, H, H). Every load (the four stored values) is issued before
+// any store, so the cell costs one memory round trip rather than four.
+template <class T>
+__device__ __forceinline__ void ph_acc4(const State<T>& s, int base, long long k, const double (&m)[4],
+                                        double cE, double sE, double cH, double sH) {
+  using M = R<T>;
+  if (s.kahan) {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) ph_acc(s, base + j, k, m[j], j < 2 ? cE : cH, j < 2 ? sE : sH);
+    return;
+  }
+  T v[4][2];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) ld2(v[j], s.ph + s.ph_off[base + j] + 2 * k);
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const double c = j < 2 ? cE : cH, sn = j < 2 ? sE : sH;
+    // float64 sum of the stored value and the float64 term, rounded to T
+    st2(s.ph + s.ph_off[base + j] + 2 * k, M::from_double(__dadd_rn((double)v[j][0], __dmul_rn(m[j], c))),
+        M::from_double(__dadd_rn((double)v[j][1], __dmul_rn(m[j], sn))));
+  }
+}
+
 // One phasor cell: plane group g = 0 d, 1 u (z planes), 2 l, 3 r (x
-// planes), 4 f, 5 b (y planes); idx runs over the group's plane.
+// planes), 4 f, 5 b (y planes); idx runs over the group's plane. The field
+// loads of all four components come first, then the phasor update.
 template <class T>
 __device__ __forceinline__ void phasor_cell(const State<T>& s, int g, int idx, int t) {
   const int m = s.npml;
@@ -184,31 +233,34 @@ __device__ __forceinline__ void phasor_cell(const State<T>& s, int g, int idx, i
   const T* hx = s.ohx; const T* hy = s.ohy; const T* hz = s.ohz;
   const long long P = s.plane, W = s.pitch;
   const long long k = (long long)a * d1 + b;
+  double mv[4];
+  int base;
   if (g < 2) {
     const int pz = g == 0 ? m + 1 : s.nz - m - 1;
     const long long i = pz * P + (long long)(m + a) * W + (m + b);
-    const int base = g * 4;  // ex, ey, hx, hy
-    ph_acc(s, base + 0, k, mean2(ldc(ex + i), ldc(ex + i - 1)), cE, sE);
-    ph_acc(s, base + 1, k, mean2(ldc(ey + i), ldc(ey + i - W)), cE, sE);
-    ph_acc(s, base + 2, k, mean4(ldc(hx + i), ldc(hx + i - W), ldc(hx + i - P), ldc(hx + i - P - W)), cH, sH);
-    ph_acc(s, base + 3, k, mean4(ldc(hy + i), ldc(hy + i - 1), ldc(hy + i - P), ldc(hy + i - P - 1)), cH, sH);
+    base = g * 4;  // ex, ey, hx, hy
+    mv[0] = mean2(ldc(ex + i), ldc(ex + i - 1));
+    mv[1] = mean2(ldc(ey + i), ldc(ey + i - W));
+    mv[2] = mean4(ldc(hx + i), ldc(hx + i - W), ldc(hx + i - P), ldc(hx + i - P - W));
+    mv[3] = mean4(ldc(hy + i), ldc(hy + i - 1), ldc(hy + i - P), ldc(hy + i - P - 1));
   } else if (g < 4) {
     const int px = g == 2 ? m + 1 : s.nx - m - 1;
     const long long i = (long long)(m + a) * P + (long long)(m + b) * W + px;
-    const int base = 8 + (g - 2) * 4;  // ey, ez, hy, hz
-    ph_acc(s, base + 0, k, mean2(ldc(ey + i), ldc(ey + i - W)), cE, sE);
-    ph_acc(s, base + 1, k, mean2(ldc(ez + i), ldc(ez + i - P)), cE, sE);
-    ph_acc(s, base + 2, k, mean4(ldc(hy + i), ldc(hy + i - 1), ldc(hy + i - P), ldc(hy + i - P - 1)), cH, sH);
-    ph_acc(s, base + 3, k, mean4(ldc(hz + i), ldc(hz + i - 1), ldc(hz + i - W), ldc(hz + i - W - 1)), cH, sH);
+    base = 8 + (g - 2) * 4;  // ey, ez, hy, hz
+    mv[0] = mean2(ldc(ey + i), ldc(ey + i - W));
+    mv[1] = mean2(ldc(ez + i), ldc(ez + i - P));
+    mv[2] = mean4(ldc(hy + i), ldc(hy + i - 1), ldc(hy + i - P), ldc(hy + i - P - 1));
+    mv[3] = mean4(ldc(hz + i), ldc(hz + i - 1), ldc(hz + i - W), ldc(hz + i - W - 1));
   } else {
     const int py = g == 4 ? m + 1 : s.ny - m - 1;
     const long long i = (long long)(m + a) * P + (long long)py * W + (m + b);
-    const int base = 16 + (g - 4) * 4;  // ex, ez, hx, hz
-    ph_acc(s, base + 0, k, mean2(ldc(ex + i), ldc(ex + i - 1)), cE, sE);
-    ph_acc(s, base + 1, k, mean2(ldc(ez + i), ldc(ez + i - P)), cE, sE);
-    ph_acc(s, base + 2, k, mean4(ldc(hx + i), ldc(hx + i - W), ldc(hx + i - P), ldc(hx + i - P - W)), cH, sH);
-    ph_acc(s, base + 3, k, mean4(ldc(hz + i), ldc(hz + i - W), ldc(hz + i - 1), ldc(hz + i - W - 1)), cH, sH);
+    base = 16 + (g - 4) * 4;  // ex, ez, hx, hz
+    mv[0] = mean2(ldc(ex + i), ldc(ex + i - 1));
+    mv[1] = mean2(ldc(ez + i), ldc(ez + i - P));
+    mv[2] = mean4(ldc(hx + i), ldc(hx + i - W), ldc(hx + i - P), ldc(hx + i - P - W));
+    mv[3] = mean4(ldc(hz + i), ldc(hz + i - W), ldc(hz + i - 1), ldc(hz + i - W - 1));
   }
+  ph_acc4(s, base, k, mv, cE, sE, cH, sH);
 }
 
 // One thread per phasor cell; g0 + blockIdx.y selects the plane group.
