@@ -35,6 +35,8 @@ __device__ __forceinline__ void h_split_vec(const State<T>& s, int t, int z, int
   const bool vin = x0 < s.pitch && y < s.ny;          // vector inside the row storage
   const long long P = s.plane, W = s.pitch;
   const long long i = (long long)z * P + (long long)y * W + x0;
+  const bool plain = interior(s, z, y, x0, t);
+  if (act && vin && !plain) h_psi_prefetch(s, z, y, x0);
   EVec<T> e;
   T hx[kVec], hy[kVec], hz[kVec];
   if (vin) {
@@ -56,7 +58,7 @@ __device__ __forceinline__ void h_split_vec(const State<T>& s, int t, int z, int
     e.ezn = ok ? ldc(s.iez + (i + kVec)) : T(0);
   }
   if (!(act && vin)) return;
-  if (interior(s, z, y, x0, t)) h_vec_interior(s, e, hx, hy, hz);
+  if (plain) h_vec_interior(s, e, hx, hy, hz);
   else h_vec(s, e, z, y, x0, t, true, hx, hy, hz);
   st4(s.ohx + i, hx); st4(s.ohy + i, hy); st4(s.ohz + i, hz);
 }
@@ -70,6 +72,8 @@ __device__ __forceinline__ void e_split_vec(const State<T>& s, int t, int z, int
   const bool vin = x0 < s.pitch && y < s.ny;
   const long long P = s.plane, W = s.pitch;
   const long long i = (long long)z * P + (long long)y * W + x0;
+  const bool plain = interior(s, z, y, x0, t);
+  if (act && vin && !plain) e_psi_prefetch(s, z, y, x0);
   HVec<T> h;
   T ex[kVec], ey[kVec], ez[kVec], ca[kVec], cb[kVec];
   if (vin) {
@@ -92,7 +96,7 @@ __device__ __forceinline__ void e_split_vec(const State<T>& s, int t, int z, int
     h.hzp = ok ? ldc(s.ihz + (i - 1)) : T(0);
   }
   if (!(act && vin)) return;
-  if (interior(s, z, y, x0, t)) e_vec_interior(h, ca, cb, ex, ey, ez);
+  if (plain) e_vec_interior(h, ca, cb, ex, ey, ez);
   else e_vec(s, h, ca, cb, z, y, x0, t, true, ex, ey, ez);
   st4(s.oex + i, ex); st4(s.oey + i, ey); st4(s.oez + i, ez);
 }
