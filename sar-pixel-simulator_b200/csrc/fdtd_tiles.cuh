@@ -245,6 +245,13 @@ __device__ __forceinline__ void march_tile(const State<T>& s, const MarchBox& b,
       cp_elem(right(st), v ? s.iey + i + kVec : s.iey, v);
       cp_elem(right(st) + 1, v ? s.iez + i + kVec : s.iez, v);
     }
+    // the CPML auxiliaries the generic update of plane zz reads from global
+    // memory (x and y faces; the z faces too when they are not staged) go
+    // to L2 a plane ahead
+    if (own && zz >= z0) {
+      h_psi_prefetch(s, zz, y, x0, !kStagePsi);
+      e_psi_prefetch(s, zz, y, x0, !kStagePsi);
+    }
   };
 
   EVec<T> e;

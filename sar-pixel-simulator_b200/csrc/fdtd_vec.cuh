@@ -208,10 +208,10 @@ __device__ __forceinline__ void prefetch_l2(const T* p) {
 }
 
 template <class T>
-__device__ __forceinline__ void h_psi_prefetch(const State<T>& s, int z, int y, int x0) {
+__device__ __forceinline__ void h_psi_prefetch(const State<T>& s, int z, int y, int x0, bool zface = true) {
   const int nx = s.nx, ny = s.ny, nz = s.nz, m = s.npml;
   if (!(z < nz - 1 && y < ny - 1)) return;
-  if (z < m - 1 || z >= nz - m) {
+  if (zface && (z < m - 1 || z >= nz - m)) {
     const int side = z < m - 1 ? 0 : 1;
     const long long k = ((long long)(side ? z - (nz - m) : z) * ny + y) * s.pitch + x0;
     prefetch_l2(s.ps.z[side][3] + k);
@@ -232,10 +232,10 @@ __device__ __forceinline__ void h_psi_prefetch(const State<T>& s, int z, int y, 
 }
 
 template <class T>
-__device__ __forceinline__ void e_psi_prefetch(const State<T>& s, int z, int y, int x0) {
+__device__ __forceinline__ void e_psi_prefetch(const State<T>& s, int z, int y, int x0, bool zface = true) {
   const int nx = s.nx, ny = s.ny, nz = s.nz, m = s.npml;
   if (!(z < nz - 1 && y < ny - 1)) return;
-  if ((z >= 1 && z < m) || z >= nz - m) {
+  if (zface && ((z >= 1 && z < m) || z >= nz - m)) {
     const int side = (z >= 1 && z < m) ? 0 : 1;
     const long long k = ((long long)(side ? z - (nz - m) : z) * ny + y) * s.pitch + x0;
     prefetch_l2(s.ps.z[side][1] + k);
