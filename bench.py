@@ -631,9 +631,9 @@ def batch_record(a, n_models, steps, warmup, check_members=(0, 21, 42)):
                    'l2': 'inputs larger than L2 (fields of all models)',
                    'batched': {'streams': 'every model on its own stream, its default kernel, side by side',
                                'split': 'split step of every model per launch, 64-step graph chunks',
-                               'queue': 'one persistent launch per step walking a tile queue over every '
-                                        "model's fused step (interior and shell z-march tiles), then one "
-                                        'phasor launch; 64-step graph chunks'}[mode],
+                               'queue': "every model's fused step: one persistent launch walking a tile "
+                                        'queue over all interior z-march tiles, one launch per split pass '
+                                        'over all shells, one phasor launch; 64-step graph chunks'}[mode],
                    'modes_ms_per_step': {k: round(v / steps, 4) for k, v in times.items()}},
         'sequential': {'value': round(seq_value, 1), 'ms_per_step': round(ms_s / steps, 4),
                        'kernel': 'each model alone, its default kernel, one shared stream'},

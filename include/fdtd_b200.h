@@ -81,10 +81,11 @@ extern "C" {
                                   for all members, in place */
 #define FDTD_BATCH_STREAMS 1   /* every member's own step path on its own
                                   stream, side by side */
-#define FDTD_BATCH_QUEUE   2   /* one persistent launch per step walks a tile
-                                  queue over every member's fused step
-                                  (interior and shell z-march tiles), then
-                                  one phasor launch */
+#define FDTD_BATCH_QUEUE   2   /* every member's fused step: one persistent
+                                  launch walks a tile queue over all
+                                  interior z-march tiles, one launch per
+                                  split pass sweeps all shells, then one
+                                  phasor launch */
 
 /* shell of the fused step (fdtd_set_option(FDTD_OPT_SHELL, ...)) */
 #define FDTD_SHELL_MARCH 0   /* fused z-marches with the CPML faces, edges and

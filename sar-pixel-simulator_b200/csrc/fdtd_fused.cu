@@ -263,11 +263,12 @@ FusedPlan make_fused_plan(int nx, int ny, int nz, int npml, int tfsf_z, int tile
   if (march) use_slab = false;
   const int m = npml;
   InteriorBox& ib = p.interior;
-  // rows start on a 128-byte line. Measured at 203 x 761 x 761 against
-  // starting at npml rounded up to 4 cells: 5 % slower with 48-byte row
-  // offsets; no faster with the arrays' origin shifted to align that
-  // column, nor with tiles from column 0 whose lanes left of the box only
-  // feed the shuffle (the narrower x strips of the shell took as long)
+  // rows start on a 128-byte line. Measured against starting at npml + 1
+  // rounded up to 4 cells: at 203 x 761 x 761 that was 5 % slower with
+  // 48-byte row offsets, and no faster with the arrays' origin shifted to
+  // align that column, nor with tiles from column 0 whose lanes left of the
+  // box only feed the shuffle (the narrower x strips of the shell took as
+  // long); the batched queue's 64-model sweep took 6 % longer with it
   ib.xa = (m + 31) / 32 * 32;
   ib.xb = (nx - m) / kVec * kVec;
   ib.ya = m;

@@ -50,31 +50,40 @@ template <class T>
 void launch_batch_phasors(const BatchModel<T>* bm, const int* start_ph, int n, int blocks_ph, int toff,
                           int* reset, cudaStream_t st);
 
-// Batched tile-queue step (fdtd_batch.cu): per member its fused plan, as
-// tiles of the interior march (tile height 4) and of the shell march.
+// Batched tile-queue step (fdtd_batch.cu): per member the interior box of
+// its fused plan, cut into tiles of the interior march (tile height 4).
 struct QueueMember {
   int has_interior;
   InteriorBox ib;
-  MarchBoxes mb;
 };
-// One tile: member, kind (0 interior, 1 shell march), the shell box (kind
-// 1), the tile's x and y position in its box and its z chunk.
+// One tile: member, the tile's x and y position in the member's interior
+// box and its z chunk.
 struct QueueTile {
-  int member, kind, box, bx, by, c;
+  int member, bx, by, c;
 };
-// Dynamic shared memory a block of the tile-queue kernel needs, and the
-// resident blocks per SM it reaches (0 on error).
-template <class T>
-size_t batch_queue_smem();
+// Resident blocks per SM the tile-queue kernel reaches (0 on error).
 template <class T>
 int batch_queue_blocks_per_sm();
-// One fused step of every member: `blocks` persistent blocks walk the tiles
-// (`ntiles` of them, longest first) through the counter, which must be zero
-// at the launch; bm holds each member's State of this step (source ->
-// destination set) and step counter.
+// The interior tiles of one fused step of every member: `blocks`
+// persistent blocks walk the tiles (`ntiles` of them, longest first)
+// through the counter, which must be zero at the launch; bm holds each
+// member's State of this step (source -> destination set).
 template <class T>
 void launch_batch_queue(const BatchModel<T>* bm, const QueueMember* qm, const QueueTile* tiles, int ntiles,
-                        int* counter, int blocks, int toff, cudaStream_t st);
+                        int* counter, int blocks, cudaStream_t st);
+
+// The shells of every member's fused step as split passes, one launch per
+// pass: a box of member `member`, its first block `b.first` counted over
+// all boxes of the launch (ascending). The H pass reads each member's
+// source set and writes its destination H; the E pass reads the
+// destination H (the State's destination pointers) and source E.
+struct BatchShellBox {
+  int member;
+  ShellBox b;
+};
+template <class T>
+void launch_batch_shell(const BatchModel<T>* bm, const BatchShellBox* boxes, int nboxes, int blocks, bool h_pass,
+                        int toff, cudaStream_t st);
 
 // Packed rows of nx elements into rows of `pitch` elements.
 template <class T>

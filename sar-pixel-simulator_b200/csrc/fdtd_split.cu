@@ -317,6 +317,47 @@ __global__ void __launch_bounds__(128, split_min_blocks<T>()) k_batch_split(cons
   else e_split_vec(s, t, z, y, x0, lane, b.width, true);
 }
 
+// The shell boxes of every member (BatchShellBox): block b belongs to the
+// last box whose first block is <= b. The member's State is staged in
+// shared memory; the E pass reads H from the destination set.
+template <class T, bool kH>
+__global__ void __launch_bounds__(128, split_min_blocks<T>())
+k_batch_shell(const BatchModel<T>* __restrict__ bm, const BatchShellBox* __restrict__ boxes, int nboxes, int toff) {
+  const int bid = blockIdx.x;
+  int lo = 0, hi = nboxes - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (boxes[mid].b.first <= bid) lo = mid;
+    else hi = mid - 1;
+  }
+  const int member = boxes[lo].member;
+  const ShellBox b = boxes[lo].b;
+  static_assert(sizeof(State<T>) % 8 == 0, "State is copied in 8-byte words");
+  __shared__ unsigned long long st_words[sizeof(State<T>) / 8];
+  {
+    const unsigned long long* src = reinterpret_cast<const unsigned long long*>(&bm[member].s);
+    for (int k = threadIdx.x; k < (int)(sizeof(State<T>) / 8); k += blockDim.x) st_words[k] = src[k];
+  }
+  __syncthreads();
+  State<T>& s = *reinterpret_cast<State<T>*>(st_words);
+  if (!kH) {
+    if (threadIdx.x == 0) { s.ihx = s.ohx; s.ihy = s.ohy; s.ihz = s.ohz; }
+    __syncthreads();
+  }
+  int local = bid - b.first;
+  const int bx = local % b.gx;
+  local /= b.gx;
+  const int by = local % b.gy;
+  const int z = b.z0 + local / b.gy;
+  const int lane = threadIdx.x % b.width, row = threadIdx.x / b.width;
+  const int x0 = b.x0 + (bx * b.width + lane) * kVec;
+  const int y = b.y0 + by * (128 / b.width) + row;
+  const bool act = x0 < b.x1 && y < b.y1;
+  const int t = *bm[member].tdev + toff;
+  if (kH) h_split_vec(s, t, z, y, x0, lane, b.width, act);
+  else e_split_vec(s, t, z, y, x0, lane, b.width, act);
+}
+
 template <class T>
 __global__ void __launch_bounds__(256) k_batch_phasors(const BatchModel<T>* __restrict__ bm,
                                                        const int* __restrict__ start, int n,
@@ -429,6 +470,14 @@ void launch_batch_phasors(const BatchModel<T>* bm, const int* start_ph, int n, i
 }
 
 template <class T>
+void launch_batch_shell(const BatchModel<T>* bm, const BatchShellBox* boxes, int nboxes, int blocks, bool h_pass,
+                        int toff, cudaStream_t st) {
+  if (nboxes <= 0 || blocks <= 0) return;
+  if (h_pass) k_batch_shell<T, true><<<blocks, 128, 0, st>>>(bm, boxes, nboxes, toff);
+  else k_batch_shell<T, false><<<blocks, 128, 0, st>>>(bm, boxes, nboxes, toff);
+}
+
+template <class T>
 void launch_batch_advance(const BatchModel<T>* bm, int n, int steps, cudaStream_t st) {
   k_batch_advance<T><<<(n + 127) / 128, 128, 0, st>>>(bm, n, steps);
 }
@@ -513,6 +562,10 @@ template void launch_batch_phasors<float>(const BatchModel<float>*, const int*, 
                                           cudaStream_t);
 template void launch_batch_phasors<double>(const BatchModel<double>*, const int*, int, int, int, int*,
                                            cudaStream_t);
+template void launch_batch_shell<float>(const BatchModel<float>*, const BatchShellBox*, int, int, bool, int,
+                                       cudaStream_t);
+template void launch_batch_shell<double>(const BatchModel<double>*, const BatchShellBox*, int, int, bool, int,
+                                        cudaStream_t);
 template void launch_batch_advance<float>(const BatchModel<float>*, int, int, cudaStream_t);
 template void launch_batch_advance<double>(const BatchModel<double>*, int, int, cudaStream_t);
 template void launch_phasors<float>(const State<float>&, const int*, int, cudaStream_t, int, int);

@@ -562,9 +562,10 @@ class Batch:
     default one launch per pass for all members each step, chunks of steps
     replayed from a captured CUDA graph; with ``streams=True`` every member
     runs its own step path on its own stream, side by side; with
-    ``mode=BATCH_QUEUE`` one persistent launch per step walks a tile queue
-    over every member's fused step. Members keep their own state and
-    readback calls."""
+    ``mode=BATCH_QUEUE`` every member takes its fused step: one persistent
+    launch per step walks a tile queue over all members' interior tiles and
+    one launch per split pass sweeps all their shells. Members keep their
+    own state and readback calls."""
 
     def __init__(self, sims, graph_chunk=None, streams=False, mode=None):
         self.sims = list(sims)   # keeps the members alive while the batch exists

@@ -145,10 +145,11 @@ QUEUE_MODELS = MODELS + [(261, 45, 30, 14, 30, 16), (173, 53, 40, 28, 30, 20)]
 
 @pytest.mark.parametrize('chunk,calls', [(0, (30,)), (7, (30,)), (4, (3, 10, 17)), (64, (1, 29))])
 def test_queue_mode_matches_oracle_for_every_member(chunk, calls):
-    """FDTD_BATCH_QUEUE: one persistent launch per step walks the tiles of
-    every member's fused step (interior and shell z-march tiles, longest
-    first). Odd calls flip every member's current field set, even graph
-    chunks keep it; every member ends with the oracle's bits."""
+    """FDTD_BATCH_QUEUE: every member's fused step, one persistent launch
+    walking the interior z-march tiles of all members (longest first) and
+    the batched split passes over all their shells. Odd calls flip every
+    member's current field set, even graph chunks keep it; every member
+    ends with the oracle's bits."""
     members = _members(QUEUE_MODELS, seed=580)
     batch = _native.Batch([s for _, s in members], graph_chunk=chunk, mode=_native.BATCH_QUEUE)
     for n in calls:
