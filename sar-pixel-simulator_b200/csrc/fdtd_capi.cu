@@ -1299,7 +1299,7 @@ int batch_build_table(fdtd_batch* b) {
     bm.ph_n = std::max(s->ny_ph * s->nx_ph, std::max(s->nz_ph * s->ny_ph, s->nz_ph * s->nx_ph));
     start[m] = (int)blk;
     start_ph[m] = (int)blk_ph;
-    blk += (long long)bm.gx * bm.gy * s->g.nz;
+    blk += (long long)bm.gx * bm.gy * ((s->g.nz + kBatchShellPlanes - 1) / kBatchShellPlanes);
     blk_ph += 6LL * ((bm.ph_n + 255) / 256);
     if (blk > INT32_MAX || blk_ph > INT32_MAX) return fail(FDTD_ERR_INVALID, "batch too large");
   }
@@ -1416,7 +1416,8 @@ int batch_build_queue(fdtd_batch* b) {
       BatchShellBox e;
       e.member = m;
       e.b = plan.shell.b[k];
-      const long long nb = (long long)e.b.gx * e.b.gy * (e.b.z1 - e.b.z0);
+      const long long nb =
+          (long long)e.b.gx * e.b.gy * ((e.b.z1 - e.b.z0 + kBatchShellPlanes - 1) / kBatchShellPlanes);
       if (nb <= 0) continue;
       e.b.first = (int)shell_blocks;
       shell_blocks += nb;

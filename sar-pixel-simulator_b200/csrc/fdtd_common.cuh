@@ -103,7 +103,8 @@ struct Adj {
 
 // One member of a batched sweep: its State (current field set, in place),
 // its step counter, and its tiling: 128-thread blocks of `width` lanes
-// (width * 4 x cells) by 128 / width rows, gx x gy of them per plane; ph_n
+// (width * 4 x cells) by 128 / width rows, gx x gy of them per plane, each
+// block sweeping kBatchShellPlanes planes; ph_n
 // cells in its largest phasor plane.
 template <class T>
 struct BatchModel {

@@ -74,9 +74,11 @@ void launch_batch_queue(const BatchModel<T>* bm, const QueueMember* qm, const Qu
 
 // The shells of every member's fused step as split passes, one launch per
 // pass: a box of member `member`, its first block `b.first` counted over
-// all boxes of the launch (ascending). The H pass reads each member's
-// source set and writes its destination H; the E pass reads the
-// destination H (the State's destination pointers) and source E.
+// all boxes of the launch (ascending); a block sweeps kBatchShellPlanes z
+// planes of one box tile. The H pass reads each member's source set and
+// writes its destination H; the E pass reads the destination H (the
+// State's destination pointers) and source E.
+constexpr int kBatchShellPlanes = 4;   // also the planes of a k_batch_split block
 struct BatchShellBox {
   int member;
   ShellBox b;

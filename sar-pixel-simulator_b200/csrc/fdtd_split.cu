@@ -308,18 +308,22 @@ __global__ void __launch_bounds__(128, split_min_blocks<T>()) k_batch_split(cons
   const int bx = local % b.gx;
   local /= b.gx;
   const int by = local % b.gy;
-  const int z = local / b.gy;
+  const int za = (local / b.gy) * kBatchShellPlanes;   // kBatchShellPlanes planes per block
+  const int zb = min(s.nz, za + kBatchShellPlanes);
   const int lane = threadIdx.x % b.width, row = threadIdx.x / b.width;
   const int x0 = (bx * b.width + lane) * kVec;
   const int y = by * (128 / b.width) + row;
   const int t = *b.tdev + toff;
-  if (kH) h_split_vec(s, t, z, y, x0, lane, b.width, true);
-  else e_split_vec(s, t, z, y, x0, lane, b.width, true);
+  for (int z = za; z < zb; ++z) {   // block-uniform trip count (shuffles inside)
+    if (kH) h_split_vec(s, t, z, y, x0, lane, b.width, true);
+    else e_split_vec(s, t, z, y, x0, lane, b.width, true);
+  }
 }
 
 // The shell boxes of every member (BatchShellBox): block b belongs to the
-// last box whose first block is <= b. The member's State is staged in
-// shared memory; the E pass reads H from the destination set.
+// last box whose first block is <= b and sweeps kBatchShellPlanes planes of
+// one box tile (the staged State serves them all). The member's State is
+// staged in shared memory; the E pass reads H from the destination set.
 template <class T, bool kH>
 __global__ void __launch_bounds__(128, split_min_blocks<T>())
 k_batch_shell(const BatchModel<T>* __restrict__ bm, const BatchShellBox* __restrict__ boxes, int nboxes, int toff) {
@@ -348,14 +352,17 @@ k_batch_shell(const BatchModel<T>* __restrict__ bm, const BatchShellBox* __restr
   const int bx = local % b.gx;
   local /= b.gx;
   const int by = local % b.gy;
-  const int z = b.z0 + local / b.gy;
+  const int za = b.z0 + (local / b.gy) * kBatchShellPlanes;
+  const int zb = min(b.z1, za + kBatchShellPlanes);
   const int lane = threadIdx.x % b.width, row = threadIdx.x / b.width;
   const int x0 = b.x0 + (bx * b.width + lane) * kVec;
   const int y = b.y0 + by * (128 / b.width) + row;
   const bool act = x0 < b.x1 && y < b.y1;
   const int t = *bm[member].tdev + toff;
-  if (kH) h_split_vec(s, t, z, y, x0, lane, b.width, act);
-  else e_split_vec(s, t, z, y, x0, lane, b.width, act);
+  for (int z = za; z < zb; ++z) {   // block-uniform trip count (shuffles inside)
+    if (kH) h_split_vec(s, t, z, y, x0, lane, b.width, act);
+    else e_split_vec(s, t, z, y, x0, lane, b.width, act);
+  }
 }
 
 template <class T>
