@@ -114,10 +114,11 @@ struct BatchModel {
   int ph_n;
 };
 
-// A box of the fused step's shell, swept by the split passes one plane per
-// block row: [x0, x1) x [y0, y1) x [z0, z1), x0 a multiple of 4. A tile is
-// `width` lanes (width * 4 x cells) by 128 / width rows; gx, gy tiles per
-// plane; `first` is the box's first block in the launch.
+// A box of the fused step's shell, swept by the split passes:
+// [x0, x1) x [y0, y1) x [z0, z1), x0 a multiple of 4. A tile is `width`
+// lanes (width * 4 x cells) by 128 / width rows; gx, gy tiles per plane; a
+// block sweeps `planes` planes of one tile (the list's choice); `first` is
+// the box's first block in the launch.
 struct ShellBox {
   int x0, x1, y0, y1, z0, z1;
   int width, gx, gy;
@@ -126,6 +127,7 @@ struct ShellBox {
 constexpr int kMaxShellBoxes = 24;
 struct ShellBoxes {
   int n, total_blocks;
+  int planes;    // z planes per block (0 before launch_shell_pass picks it)
   int dropped;   // boxes that did not fit (a plan with any is rejected)
   ShellBox b[kMaxShellBoxes];
 };

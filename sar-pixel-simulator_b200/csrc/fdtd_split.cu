@@ -102,7 +102,7 @@ __device__ __forceinline__ void e_split_vec(const State<T>& s, int t, int z, int
 }
 
 // The passes over a list of boxes (the whole grid for the split step, the
-// shell of the fused step), one plane of one box tile per 128-thread block. A box tile is `width` lanes
+// shell of the fused step), bl.planes planes of one box tile per 128-thread block. A box tile is `width` lanes
 // (width * kVec x cells) by 128 / width rows.
 __device__ __forceinline__ const ShellBox& find_box(const ShellBoxes& bl, int bid) {
   int k = 0;
@@ -124,14 +124,17 @@ __global__ void __launch_bounds__(128, split_min_blocks<T>()) k_shell(State<T> s
   const int bx = local % b.gx;
   local /= b.gx;
   const int by = local % b.gy;
-  const int bz = local / b.gy;
+  const int za = b.z0 + (local / b.gy) * bl.planes;
+  const int zb = min(b.z1, za + bl.planes);
   const int lane = threadIdx.x % b.width, row = threadIdx.x / b.width;
   const int x0 = b.x0 + (bx * b.width + lane) * kVec;
   const int y = b.y0 + by * (128 / b.width) + row;
-  const int z = b.z0 + bz;
   const bool act = x0 < b.x1 && y < b.y1;
-  if (kH) h_split_vec(s, *tp + toff, z, y, x0, lane, b.width, act);
-  else e_split_vec(s, *tp + toff, z, y, x0, lane, b.width, act);
+  const int t = *tp + toff;
+  for (int z = za; z < zb; ++z) {   // block-uniform trip count (shuffles inside)
+    if (kH) h_split_vec(s, t, z, y, x0, lane, b.width, act);
+    else e_split_vec(s, t, z, y, x0, lane, b.width, act);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -493,8 +496,21 @@ template <class T>
 void launch_shell_pass(const State<T>& s, const int* tdev, int toff, const ShellBoxes& bl,
                        bool h_pass, cudaStream_t st) {
   if (bl.n == 0 || bl.total_blocks == 0) return;
-  if (h_pass) k_shell<T, true><<<bl.total_blocks, 128, 0, st>>>(s, tdev, toff, bl);
-  else k_shell<T, false><<<bl.total_blocks, 128, 0, st>>>(s, tdev, toff, bl);
+  // Several planes per block amortise the block's set-up, but only where
+  // one plane per block gives many waves of blocks: 148 SMs hold about
+  // 1184 of these blocks at once (8 each). add_shell_box numbered the
+  // blocks one plane each; renumber for the choice.
+  constexpr int kResident = 148 * 8;
+  ShellBoxes p = bl;
+  p.planes = bl.total_blocks >= 16 * kResident ? 4 : bl.total_blocks >= 8 * kResident ? 2 : 1;
+  p.total_blocks = 0;
+  for (int k = 0; k < p.n; ++k) {
+    ShellBox& b = p.b[k];
+    b.first = p.total_blocks;
+    p.total_blocks += b.gx * b.gy * ((b.z1 - b.z0 + p.planes - 1) / p.planes);
+  }
+  if (h_pass) k_shell<T, true><<<p.total_blocks, 128, 0, st>>>(s, tdev, toff, p);
+  else k_shell<T, false><<<p.total_blocks, 128, 0, st>>>(s, tdev, toff, p);
 }
 
 void launch_advance(int* tdev, int n, cudaStream_t st) {
