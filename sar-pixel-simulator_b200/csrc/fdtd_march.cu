@@ -68,7 +68,7 @@ k_march(const __grid_constant__ State<T> s, const int* __restrict__ tp, int toff
   local /= b.gx;
   const int by = local % b.gy;
   const int c = local / b.gy;
-  march_tile<T, true>(s, b, bx, by, c, *tp + toff, reinterpret_cast<T*>(march_smem));
+  march_tile<T>(s, b, bx, by, c, *tp + toff, reinterpret_cast<T*>(march_smem));
 }
 
 }  // namespace

@@ -1,6 +1,7 @@
-// fdtd_tiles.cuh -- the bodies of the fused step's two z-marching tiles,
-// shared by the single-simulation kernels (fdtd_fused.cu: k_fused_interior;
-// fdtd_march.cu: k_march) and the batched tile-queue kernel (fdtd_batch.cu).
+// fdtd_tiles.cuh -- the bodies of the fused step's two z-marching tiles:
+// interior_tile, shared by the single-simulation interior kernel
+// (fdtd_fused.cu: k_fused_interior) and the batched tile-queue kernel
+// (fdtd_batch.cu); march_tile, the body of the shell march (fdtd_march.cu).
 //
 // interior_tile: a tile of the interior box, the plain curl updates only
 // (no CPML face, edge or injection touches it or its recomputed halo).
@@ -116,13 +117,13 @@ __device__ __forceinline__ void interior_tile(const State<T>& s, const InteriorB
 // Dynamic shared memory of a march tile, in elements of T: the four
 // exchange arrays, then two stages of the per-thread staging area. A stage
 // holds, per thread, kSlots vectors (E(z+1) x, y, z; H(z) x, y, z; Ca, Cb;
-// with kStagePsi the z-face psi Hyz, Hxz, Eyz, Exz), then the top row's
+// the z-face psi Hyz, Hxz, Eyz, Exz), then the top row's
 // E(y+1) x, z (32 lanes at most) and the last lane's E(x+4) y, z (one pair
 // per row).
-template <class T, bool kStagePsi = true>
+template <class T>
 struct MarchSmem {
   static constexpr int kEx = kMarchThreads * kVec;
-  static constexpr int kSlots = kStagePsi ? 12 : 8;
+  static constexpr int kSlots = 12;
   static constexpr int kMain = kSlots * kMarchThreads * kVec;
   static constexpr int kTop = 2 * 32 * kVec;
   static constexpr int kRight = 2 * (kMarchThreads / 8);
@@ -158,13 +159,13 @@ __device__ __forceinline__ void cp_wait_prev() { asm volatile("cp.async.wait_gro
 
 // One tile of a march box: tile (bx, by) of the box's x-y tiling and z
 // chunk c, by kMarchThreads threads, the step being t. smem: the
-// MarchSmem<T, kStagePsi> area (exchange arrays, then two stages). With
-// kStagePsi the z-face psi is staged with the rest of the plane; without,
-// the z-face path reads it from the source psi.
-template <class T, bool kStagePsi>
+// MarchSmem<T> area (exchange arrays, then two stages). The z-face psi is
+// staged with the rest of the plane (read from the source psi in the
+// bounds-checked build when a shared index fails its check).
+template <class T>
 __device__ __forceinline__ void march_tile(const State<T>& s, const MarchBox& b, int bx, int by, int c, int t,
                                            T* smem) {
-  using SM = MarchSmem<T, kStagePsi>;
+  using SM = MarchSmem<T>;
   // exchange arrays: E(z) of every row (read by the row below as its +y
   // neighbour) and H^{n+1/2}(z) (read by the row above as its -y
   // neighbour), indexed [(row * width + lane) * 4 + j]; then the stages
@@ -228,7 +229,7 @@ __device__ __forceinline__ void march_tile(const State<T>& s, const MarchBox& b,
     const int hsd = zz < m - 1 ? 0 : 1, esd = zz < m ? 0 : 1;
     const long long kh = ((long long)(hsd ? zz - (nz - m) : zz) * ny + y) * W + x0;
     const long long ke = ((long long)(esd ? zz - (nz - m) : zz) * ny + y) * W + x0;
-    if constexpr (kStagePsi) {
+    {
       const T* p0 = s.ps.z[0][0];
       cp_vec(slot(st, 8), hf ? s.ps.z[hsd][3] + kh : p0, hf);
       cp_vec(slot(st, 9), hf ? s.ps.z[hsd][2] + kh : p0, hf);
@@ -246,11 +247,10 @@ __device__ __forceinline__ void march_tile(const State<T>& s, const MarchBox& b,
       cp_elem(right(st) + 1, v ? s.iez + i + kVec : s.iez, v);
     }
     // the CPML auxiliaries the generic update of plane zz reads from global
-    // memory (x and y faces; the z faces too when they are not staged) go
-    // to L2 a plane ahead
+    // memory (x and y faces) go to L2 a plane ahead
     if (own && zz >= z0) {
-      h_psi_prefetch(s, zz, y, x0, !kStagePsi);
-      e_psi_prefetch(s, zz, y, x0, !kStagePsi);
+      h_psi_prefetch(s, zz, y, x0, false);
+      e_psi_prefetch(s, zz, y, x0, false);
     }
   };
 
@@ -303,7 +303,7 @@ __device__ __forceinline__ void march_tile(const State<T>& s, const MarchBox& b,
     if (vin) {
       if (plain_h) h_vec_interior(s, e, h.hx, h.hy, h.hz);
       else if (zface_h) {
-        if (kStagePsi && sm_ok) {
+        if (sm_ok) {
           h_vec_zface(s, e, z, y, x0, work, slot(st, 8), slot(st, 9), h.hx, h.hy, h.hz);
         } else {
           const int sd_ = z < m - 1 ? 0 : 1;
@@ -327,7 +327,7 @@ __device__ __forceinline__ void march_tile(const State<T>& s, const MarchBox& b,
       else { zero4(h.hxy); zero4(h.hzy); }
       if (plain_h) e_vec_interior(h, ca, cb, e.ex, e.ey, e.ez);
       else if (zface_h) {
-        if (kStagePsi && sm_ok) {
+        if (sm_ok) {
           e_vec_zface(s, h, ca, cb, z, y, x0, slot(st, 10), slot(st, 11), e.ex, e.ey, e.ez);
         } else {
           const int sd_ = z < m ? 0 : 1;
