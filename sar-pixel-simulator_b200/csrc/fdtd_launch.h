@@ -138,7 +138,7 @@ template <class T>
 bool launch_fused_slab(const State<T>& s, const FusedPlan& p, int tile_y, cudaStream_t st);
 
 // Appends the box [x0, x1) x [y0, y1) x [z0, z1) to a box list, with the
-// row width (32, 16 or 8 lanes) that pads x the least.
+// row width (32, 16, 8 or 4 lanes) that pads x the least.
 void add_shell_box(ShellBoxes& bl, int x0, int x1, int y0, int y1, int z0, int z1);
 
 // Split H pass (h_pass) or E pass over the shell boxes, from the State's

@@ -435,7 +435,7 @@ void add_shell_box(ShellBoxes& bl, int x0, int x1, int y0, int y1, int z0, int z
   b.x0 = x0; b.x1 = x1; b.y0 = y0; b.y1 = y1; b.z0 = z0; b.z1 = z1;
   // row width with the least x padding (ties: the wider rows)
   long long best = -1;
-  for (int w : {32, 16, 8}) {
+  for (int w : {32, 16, 8, 4}) {
     const long long gx = (x1 - x0 + 4 * w - 1) / (4 * w), gy = (y1 - y0 + 128 / w - 1) / (128 / w);
     const long long padded = gx * 4 * w * gy * (128 / w);
     if (best < 0 || padded < best) { best = padded; b.width = w; }
