@@ -185,11 +185,11 @@ def committed_traffic(kernel_name, workload):
 # ---------------------------------------------------------------------------
 # CPU baseline (the oracle: CPU restatement of the reference's algorithm)
 # ---------------------------------------------------------------------------
-def cpu_baseline(pc, ca, cb, inc, steps):
+def cpu_baseline(pc, ca, cb, inc, steps, warmup=1):
     """The oracle (CPU restatement of the reference's step) on the host: the
     C restatement on every host core when it is built (make -C oracle), else
-    the numpy oracle on one core. `steps` full-grid steps after one untimed
-    step (first touch of every array)."""
+    the numpy oracle on one core. `steps` full-grid steps after `warmup`
+    untimed ones (the first touches every array)."""
     sys.path.insert(0, os.path.join(ROOT, 'oracle'))
     import fdtd_oracle as O
     from fdtdsarsim_b200.absorbers import cpml_profiles
@@ -208,7 +208,8 @@ def cpu_baseline(pc, ca, cb, inc, steps):
         cores = 1
         sim = O.OracleSim(*args)
         what = 'numpy oracle, one thread'
-    sim.step(ca, cb, inc)  # first-touch of every array, untimed
+    for _ in range(max(1, warmup)):
+        sim.step(ca, cb, inc)  # untimed; the first touches every array
     t0 = time.perf_counter()
     for _ in range(steps):
         sim.step(ca, cb, inc)
@@ -217,7 +218,7 @@ def cpu_baseline(pc, ca, cb, inc, steps):
     return {'value': cells * steps / dt / 1e6, 'unit': 'Mcell-updates/s', 'cores': cores,
             'kind': 'port',
             'sample': f'{steps} time steps of the full {g.size_z}x{g.size_y}x{g.size_x} grid '
-                      f'({what}), after one untimed step'}
+                      f'({what}), after {max(1, warmup)} untimed'}
 
 
 # ---------------------------------------------------------------------------
@@ -477,10 +478,11 @@ def run_reference(a):
     g = pc.geom_params
     cells = g.size_x * g.size_y * g.size_z
     steps = max(1, min(a.steps, a.cpu_steps))
-    base = cpu_baseline(pc, ca, cb, inc, steps)
+    warm = max(1, min(a.warmup, 3))   # a bounded sample: at most 3 untimed steps
+    base = cpu_baseline(pc, ca, cb, inc, steps, warm)
     line = {
         'impl': 'reference', 'metric': 'Mcell-updates/s', 'value': round(base['value'], 2),
-        'unit': 'Mcell-updates/s', 'n_gpus': world, 'steps': steps, 'warmup': 1,
+        'unit': 'Mcell-updates/s', 'n_gpus': world, 'steps': steps, 'warmup': warm,
         'ms_per_step': round(cells / (base['value'] * 1e6) * 1e3, 2), 'higher_is_better': True,
         'scaling': 'weak', 'vs_baseline': None,
         'dtype': 'f32' if a.dtype == 'float32' else 'f64',
