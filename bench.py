@@ -50,8 +50,9 @@ def parse():
     ap.add_argument('--shell', default=None, choices=['march', 'split'],
                     help='fused kernel: shell marched or swept by the split passes')
     ap.add_argument('--zchunk', type=int, default=0, help='fused kernel z planes per block (0: auto)')
-    ap.add_argument('--slab', type=int, default=None, choices=[0, 1],
-                    help='fused kernel: march the CPML z slabs (1) or sweep them with the shell (0)')
+    ap.add_argument('--slab', type=int, default=None, choices=[0, 1, 2],
+                    help='fused kernel: march the CPML z slabs (1), the whole z extent of the '
+                         "interior's x-y box (2), or sweep the slabs with the shell (0)")
     ap.add_argument('--dtype', default='float32', choices=['float32', 'float64'])
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-cpu-baseline', action='store_true')
@@ -450,7 +451,7 @@ def run_ours(a):
                            parallelism=f'replicas x{world}' if world > 1 else 'single GPU',
                            kernel=kname, tile=[choice['tile_x'], choice['tile_y']]
                            if choice['kernel'] == _native.FDTD_KERNEL_FUSED else None,
-                           zchunk=choice.get('zchunk', 0), z_slabs_fused=bool(choice.get('slab', 0)),
+                           zchunk=choice.get('zchunk', 0), z_slabs_fused=int(choice.get('slab', 0)),
                            shell=shell_name(choice),
                            autotuned=None if tuned is None else
                            [{'ms': t, 'kernel': 'fused' if c['kernel'] else 'split',

@@ -66,8 +66,12 @@ extern "C" {
 #define FDTD_OPT_CHECK_EVERY  6  /* non-finite check period in steps (0 = off) */
 #define FDTD_OPT_TIMING       7  /* 1: record CUDA events around every kernel */
 #define FDTD_OPT_ZCHUNK       8  /* fused kernel z planes per block (0 = automatic) */
-#define FDTD_OPT_FUSED_SLAB   9  /* 1: the fused step marches the CPML z slabs too
-                                    (default 0: the split passes sweep them) */
+#define FDTD_OPT_FUSED_SLAB   9  /* 1: the fused step marches the CPML z slabs too;
+                                    2: the column march, the interior's x-y box
+                                    over every z plane (z faces and injection
+                                    plane in the march), the split passes then
+                                    sweep only the x and y strips (default 0:
+                                    the split passes sweep the z slabs) */
 #define FDTD_OPT_BATCH_STREAMS 10 /* fdtd_batch_set_option: 1 runs every member's
                                     own step path on its own stream, side by
                                     side; 0 (default) one launch per pass for
@@ -358,8 +362,10 @@ int fdtd_check_cell_division(int dtype, double cell_size, int device, int64_t *t
  * step's decomposition of a grid, host computation only (no device use).
  * mode 0: the shell by the split passes (FDTD_SHELL_SPLIT, the default
  * step), 1: the same with the CPML z slabs marched (FDTD_OPT_FUSED_SLAB),
- * 2: the shell marched (FDTD_SHELL_MARCH). Rows of 7 ints (kind, x0, x1, y0,
- * y1, z0, z1), kind 0 the interior z-march, 1 the CPML z slabs, 2 a shell
+ * 2: the shell marched (FDTD_SHELL_MARCH), 3: the column march
+ * (FDTD_OPT_FUSED_SLAB = 2). Rows of 7 ints (kind, x0, x1, y0,
+ * y1, z0, z1), kind 0 the interior z-march, 1 the CPML z slabs (mode 3:
+ * the column), 2 a shell
  * box swept by the split passes, 3 a shell box of the general march; every
  * cell lies in exactly one box. */
 int fdtd_fused_plan_boxes(int nx, int ny, int nz, int npml, int tfsf_z, int tile_y, int zchunk,

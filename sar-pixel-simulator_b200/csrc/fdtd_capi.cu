@@ -365,7 +365,7 @@ int enqueue_steps(fdtd_sim* s, int n, int ph_g0 = 0, int ph_ng = 6) {
       if (!s->plan_ok || s->plan_tile_y != s->tile_y || s->plan_zchunk != s->zchunk ||
           s->plan_slab != s->slab || s->plan_shell != s->shell) {
         const fdtd_geometry& g = s->g;
-        s->plan = make_fused_plan(g.nx, g.ny, g.nz, g.npml, g.tfsf_z, s->tile_y, s->zchunk, s->slab != 0,
+        s->plan = make_fused_plan(g.nx, g.ny, g.nz, g.npml, g.tfsf_z, s->tile_y, s->zchunk, s->slab,
                                   s->shell == FDTD_SHELL_MARCH);
         s->plan_slab = s->slab;
         s->plan_shell = s->shell;
@@ -388,9 +388,11 @@ int enqueue_steps(fdtd_sim* s, int n, int ph_g0 = 0, int ph_ng = 6) {
         CK(cudaEventRecord(s->join, s->side));
         CK(cudaStreamWaitEvent(s->stream, s->join, 0));
       } else {
-        // the z slabs' march and the shell H pass beside the interior march
-        launch_fused_slab<T>(st, s->plan, s->tile_y, s->side);
+        // the shell H pass (and the z slabs' march) beside the interior
+        // march, or beside the column march
+        if (!s->plan.column) launch_fused_slab<T>(st, s->plan, s->tile_y, s->tdev, k, s->side);
         launch_shell_pass<T>(st, s->tdev, k, s->plan.shell, true, s->side);
+        if (s->plan.column) launch_fused_slab<T>(st, s->plan, s->tile_y, s->tdev, k, s->stream);
         launch_fused_interior<T>(st, s->plan, s->tile_y, s->stream);
         CK(cudaEventRecord(s->join, s->side));
         CK(cudaStreamWaitEvent(s->stream, s->join, 0));
@@ -720,7 +722,8 @@ int fdtd_set_option(fdtd_sim* s, int option, int value) {
       s->zchunk = value;
       return FDTD_OK;
     case FDTD_OPT_FUSED_SLAB:
-      s->slab = value ? 1 : 0;
+      if (value < 0 || value > 2) return fail(FDTD_ERR_INVALID, "FDTD_OPT_FUSED_SLAB %d: 0, 1 or 2", value);
+      s->slab = value;
       return FDTD_OK;
     case FDTD_OPT_SHELL:
       if (value != FDTD_SHELL_MARCH && value != FDTD_SHELL_SPLIT)
@@ -1406,7 +1409,7 @@ int batch_build_queue(fdtd_batch* b) {
       bm.tdev = s->tdev;
       bm.ph_n = ph_n;
     }
-    const FusedPlan plan = make_fused_plan(g.nx, g.ny, g.nz, g.npml, g.tfsf_z, 4, kQueueZChunk, false, false);
+    const FusedPlan plan = make_fused_plan(g.nx, g.ny, g.nz, g.npml, g.tfsf_z, 4, kQueueZChunk, 0, false);
     if (plan.shell.dropped) return fail(FDTD_ERR_INVALID, "member %d: too many shell boxes", m);
     QueueMember& q = qm[m];
     memset(&q, 0, sizeof(q));
@@ -2117,8 +2120,9 @@ int fdtd_fused_plan_boxes(int nx, int ny, int nz, int npml, int tfsf_z, int tile
   if (!out || !count || cap < 0) return fail(FDTD_ERR_INVALID, "null argument");
   if (npml < 2 || npml > kMaxPml || nx < 2 * npml + 3 || ny < 2 * npml + 3 || nz < 2 * npml + 3)
     return fail(FDTD_ERR_INVALID, "grid %dx%dx%d too small for npml %d", nz, ny, nx, npml);
-  if (mode < 0 || mode > 2) return fail(FDTD_ERR_INVALID, "unknown plan mode %d", mode);
-  const FusedPlan p = make_fused_plan(nx, ny, nz, npml, tfsf_z, tile_y, zchunk, mode == 1, mode == 2);
+  if (mode < 0 || mode > 3) return fail(FDTD_ERR_INVALID, "unknown plan mode %d", mode);
+  const FusedPlan p =
+      make_fused_plan(nx, ny, nz, npml, tfsf_z, tile_y, zchunk, mode == 1 ? 1 : mode == 3 ? 2 : 0, mode == 2);
   if (p.shell.dropped || p.mshell.dropped)
     return fail(FDTD_ERR_INVALID, "plan needs more than %d shell boxes", kMaxShellBoxes);
   int n = 0;

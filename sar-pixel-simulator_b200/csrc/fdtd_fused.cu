@@ -63,21 +63,26 @@ k_fused_interior(const __grid_constant__ State<T> s, InteriorBox ib) {
   interior_tile<T, TY>(s, ib, threadIdx.x, threadIdx.y, blockIdx.x, blockIdx.y, blockIdx.z, sEx, sEz, sHx, sHz);
 }
 
-// The z slabs of the same x-y box: z in [0, npml) and [nz - npml, nz), one
-// chunk each (blockIdx.z), marched like the interior. Every plane carries
-// z-face CPML terms with coefficients uniform over the plane (Taflove 7.x:
+// The z slabs of the same x-y box (z in [0, npml) and [nz - npml, nz), one
+// chunk each), or the whole z extent of the x-y box (the column march), in
+// z chunks (blockIdx.z, mapped to the box's z ranges as the interior's),
+// marched like the interior. A plane in a z face carries the z-face CPML
+// terms, with coefficients uniform over the plane (Taflove 7.x:
 // psi_H = bh psi_H + (ch / dx) dE, psi_E = be psi_E + (ce / dx) dH,
 // cpu/field_updates.py:66-105, 243-282), applied after the curl update of
-// the same component as the split kernels apply them; the domain's first and
-// last planes keep the components outside their update ranges
-// (cpu/field_updates.py:18-63, 198-240). No x or y face touches the box.
+// the same component as the split kernels apply them; the injection plane
+// (while t < nt_inc) carries the incident terms after them
+// (cpu/main_sim.py:147-161); the domain's first and last planes keep the
+// components outside their update ranges (cpu/field_updates.py:18-63,
+// 198-240). Every term is uniform over a plane, so the march's recomputed
+// plane below a chunk gets them too. No x or y face touches the box.
 // (four blocks per SM in float32 at 4-row tiles: the interior's 95 registers)
 template <class T, int TY>
 constexpr int slab_min_blocks() { return sizeof(T) == 4 && TY <= 4 ? 4 : 1; }
 
 template <class T, int TY>
 __global__ void __launch_bounds__(kLanes * (TY + 1), slab_min_blocks<T, TY>())
-k_fused_slab(const __grid_constant__ State<T> s, InteriorBox ib) {
+k_fused_slab(const __grid_constant__ State<T> s, InteriorBox ib, const int* __restrict__ tp, int toff) {
   using M = R<T>;
   __shared__ __align__(32) T sEx[TY + 1][kRowCells];
   __shared__ __align__(32) T sEz[TY + 1][kRowCells];
@@ -88,9 +93,12 @@ k_fused_slab(const __grid_constant__ State<T> s, InteriorBox ib) {
   const int lane = threadIdx.x, r = threadIdx.y;
   const int x0 = ib.xa + blockIdx.x * kRowCells + lane * kVec;
   const int y = ib.ya + blockIdx.y * TY + r - 1;
-  const int k = blockIdx.z;
-  const int z0 = ib.z0[k], z1 = ib.z1[k];
-  const int zs = max(z0 - 1, 0);   // the bottom slab starts at plane 0: nothing below
+  int c = blockIdx.z, k = 0;
+  if (c >= ib.chunks0) { c -= ib.chunks0; k = 1; }
+  const int z0 = ib.z0[k] + c * ib.zchunk;
+  const int z1 = min(ib.z1[k], z0 + ib.zchunk);
+  const int zs = max(z0 - 1, 0);   // a chunk at plane 0 has nothing below
+  const int t = *tp + toff;
   const bool vin = x0 < s.pitch && y < s.ny;
   const bool own = vin && r >= 1 && y < ib.yb && x0 < ib.xb;
   const long long P = s.plane, W = s.pitch;
@@ -106,6 +114,60 @@ k_fused_slab(const __grid_constant__ State<T> s, InteriorBox ib) {
 
   for (int z = zs; z < z1; ++z, i += P) {
     const bool work = own && z >= z0;
+    if (z >= m && z < nz - m && !(z == s.tfsf_z && t < s.nt_inc)) {
+      // a plane with no z face, no domain edge and no injection: the
+      // interior march's plain update (the same operations as below, with
+      // every plane-dependent term absent)
+      if (vin) {
+        ld4(e.exz, s.iex + i + P); ld4(e.eyz, s.iey + i + P); ld4(ezz, s.iez + i + P);
+        ld4(h.hx, s.ihx + i); ld4(h.hy, s.ihy + i); ld4(h.hz, s.ihz + i);
+      } else {
+        zero4(e.exz); zero4(e.eyz); zero4(ezz); zero4(h.hx); zero4(h.hy); zero4(h.hz);
+      }
+      T ca[kVec], cb[kVec];
+      if (work) { ld4(ca, s.ca + i); ld4(cb, s.cb + i); }
+      else { zero4(ca); zero4(cb); }
+      if (r == TY) {
+        if (vin && y + 1 < s.ny) { ld4(e.exy, s.iex + i + W); ld4(e.ezy, s.iez + i + W); }
+        else { zero4(e.exy); zero4(e.ezy); }
+      }
+      T eyr = T(0), ezr = T(0);
+      if (lane == kLanes - 1 && vin && x0 + kVec < s.pitch) { eyr = ldc(s.iey + (i + kVec)); ezr = ldc(s.iez + (i + kVec)); }
+      T gx = T(0), gy = T(0), gz = T(0), gxz = T(0), gxy = T(0), ghy = T(0), ghz = T(0);
+      if (work && lane == 0) {
+        const long long j = i - 1;
+        gx = ldc(s.iex + (j)); gy = ldc(s.iey + (j)); gz = ldc(s.iez + (j));
+        ghy = ldc(s.ihy + (j)); ghz = ldc(s.ihz + (j));
+        gxz = ldc(s.iex + (j + P)); gxy = ldc(s.iex + (j + W));
+      }
+      st4(&sEx[r][so], e.ex);
+      st4(&sEz[r][so], e.ez);
+      __syncthreads();
+      if (r < TY) { ld4(e.exy, &sEx[r + 1][so]); ld4(e.ezy, &sEz[r + 1][so]); }
+      e.eyn = __shfl_down_sync(kFull, e.ey[0], 1);
+      e.ezn = __shfl_down_sync(kFull, e.ez[0], 1);
+      if (lane == kLanes - 1) { e.eyn = eyr; e.ezn = ezr; }
+      h_vec_interior(s, e, h.hx, h.hy, h.hz);
+      st4(&sHx[r][so], h.hx);
+      st4(&sHz[r][so], h.hz);
+      __syncthreads();
+      h.hyp = __shfl_up_sync(kFull, h.hy[kVec - 1], 1);
+      h.hzp = __shfl_up_sync(kFull, h.hz[kVec - 1], 1);
+      if (work) {
+        ld4(h.hxy, &sHx[r - 1][so]);
+        ld4(h.hzy, &sHz[r - 1][so]);
+        if (lane == 0) {
+          h.hyp = M::sub(ghy, M::mul(s.db, M::sub(M::sub(gxz, gx), M::sub(e.ez[0], gz))));
+          h.hzp = M::sub(ghz, M::mul(s.db, M::sub(M::sub(e.ey[0], gy), M::sub(gxy, gx))));
+        }
+        e_vec_interior(h, ca, cb, e.ex, e.ey, e.ez);
+        st4(s.ohx + i, h.hx); st4(s.ohy + i, h.hy); st4(s.ohz + i, h.hz);
+        st4(s.oex + i, e.ex); st4(s.oey + i, e.ey); st4(s.oez + i, e.ez);
+      }
+      copy4(e.ex, e.exz); copy4(e.ey, e.eyz); copy4(e.ez, ezz);
+      copy4(h.hxz, h.hx); copy4(h.hyz, h.hy);
+      continue;
+    }
     const bool top = z + 1 >= nz;   // last plane: nothing above, nothing updated
     // update ranges and CPML faces of plane z (uniform over the plane)
     const bool h_xy = z < nz - 1, h_z = z >= 1 && z < nz - 1;
@@ -114,6 +176,8 @@ k_fused_slab(const __grid_constant__ State<T> s, InteriorBox ib) {
     const bool ef = z < nz - 1 && ((z >= 1 && z < m) || z >= nz - m);
     const int hside = z < m - 1 ? 0 : 1, hq = hside ? z - (nz - m) : z;
     const int eside = z < m ? 0 : 1, eq = eside ? z - (nz - m) : z;
+    const bool inj = z == s.tfsf_z && t < s.nt_inc;   // injection plane
+    const long long ki = ((long long)t * s.ny + y) * W + x0;   // incident planes (t, y, x)
     if (vin && !top) {
       ld4(e.exz, s.iex + i + P); ld4(e.eyz, s.iey + i + P); ld4(ezz, s.iez + i + P);
     } else {
@@ -130,14 +194,15 @@ k_fused_slab(const __grid_constant__ State<T> s, InteriorBox ib) {
     }
     T eyr = T(0), ezr = T(0);
     if (lane == kLanes - 1 && vin && x0 + kVec < s.pitch) { eyr = ldc(s.iey + (i + kVec)); ezr = ldc(s.iez + (i + kVec)); }
-    T gx = T(0), gy = T(0), gz = T(0), gxz = T(0), gxy = T(0), ghy = T(0), ghz = T(0), gpy = T(0);
+    T gx = T(0), gy = T(0), gz = T(0), gxz = T(0), gxy = T(0), ghy = T(0), ghz = T(0), gpy = T(0), gix = T(0);
     if (work && lane == 0) {
       const long long j = i - 1;
       gx = ldc(s.iex + (j)); gy = ldc(s.iey + (j)); gz = ldc(s.iez + (j));
       ghy = ldc(s.ihy + (j)); ghz = ldc(s.ihz + (j));
       gxz = top ? T(0) : ldc(s.iex + (j + P));
       gxy = ldc(s.iex + (j + W));
-      if (hf) gpy = s.ps.z[hside][3][((long long)hq * s.ny + y) * W + x0 - 1];
+      if (hf) gpy = ldc(s.ps.z[hside][3] + (((long long)hq * s.ny + y) * W + x0 - 1));
+      if (inj) gix = ldc(s.inc_ex + (ki - 1));
     }
     // ---- H^{n+1/2}(z) -----------------------------------------------------
     st4(&sEx[r][so], e.ex);
@@ -170,6 +235,17 @@ k_fused_slab(const __grid_constant__ State<T> s, InteriorBox ib) {
       }
       if (work) { st4(s.pd.z[hside][3] + kq, p3); st4(s.pd.z[hside][2] + kq, p2); }
     }
+    if (inj) {   // E-field injection into H (cpu/main_sim.py:147-150)
+      T iey[kVec], iex[kVec];
+      if (vin) { ld4(iey, s.inc_ey + ki); ld4(iex, s.inc_ex + ki); }
+      else { zero4(iey); zero4(iex); }
+#pragma unroll
+      for (int j = 0; j < kVec; ++j) {
+        if (x0 + j >= s.nx) continue;
+        h.hx[j] = M::add(h.hx[j], M::mul(s.db, iey[j]));
+        h.hy[j] = M::sub(h.hy[j], M::mul(s.db, iex[j]));
+      }
+    }
     st4(&sHx[r][so], h.hx);
     st4(&sHz[r][so], h.hz);
     __syncthreads();
@@ -190,6 +266,7 @@ k_fused_slab(const __grid_constant__ State<T> s, InteriorBox ib) {
             hyp = M::sub(hyp, M::mul(s.dtm0, p3));
           }
         }
+        if (inj) hyp = M::sub(hyp, M::mul(s.db, gix));
         if (h_z) hzp = M::sub(ghz, M::mul(s.db, M::sub(M::sub(e.ey[0], gy), M::sub(gxy, gx))));
         h.hyp = hyp;
         h.hzp = hzp;
@@ -219,6 +296,17 @@ k_fused_slab(const __grid_constant__ State<T> s, InteriorBox ib) {
         st4(s.pd.z[eside][1] + kq, p1);
         st4(s.pd.z[eside][0] + kq, p0);
       }
+      if (inj) {   // H-field injection into E (cpu/main_sim.py:158-161)
+        T ihx[kVec], ihy[kVec];
+        ld4(ihx, s.inc_hx + ki);
+        ld4(ihy, s.inc_hy + ki);
+#pragma unroll
+        for (int j = 0; j < kVec; ++j) {
+          if (x0 + j >= s.nx) continue;
+          oy[j] = M::add(oy[j], M::mul(s.dte0dx, ihx[j]));
+          ox[j] = M::sub(ox[j], M::mul(s.dte0dx, ihy[j]));
+        }
+      }
       st4(s.ohx + i, h.hx); st4(s.ohy + i, h.hy); st4(s.ohz + i, h.hz);
       st4(s.oex + i, ox); st4(s.oey + i, oy); st4(s.oez + i, oz);
     }
@@ -228,10 +316,10 @@ k_fused_slab(const __grid_constant__ State<T> s, InteriorBox ib) {
 }
 
 template <class T, int TY>
-void launch_slab_ty(const State<T>& s, const InteriorBox& sb, cudaStream_t st) {
+void launch_slab_ty(const State<T>& s, const InteriorBox& sb, const int* tdev, int toff, cudaStream_t st) {
   const dim3 blk(kLanes, TY + 1, 1);
-  const dim3 grd((sb.xb - sb.xa + kRowCells - 1) / kRowCells, (sb.yb - sb.ya + TY - 1) / TY, sb.nz_ranges);
-  k_fused_slab<T, TY><<<grd, blk, 0, st>>>(s, sb);
+  const dim3 grd((sb.xb - sb.xa + kRowCells - 1) / kRowCells, (sb.yb - sb.ya + TY - 1) / TY, sb.chunks);
+  k_fused_slab<T, TY><<<grd, blk, 0, st>>>(s, sb, tdev, toff);
 }
 
 template <class T, int TY>
@@ -256,11 +344,12 @@ bool fused_supported_tile(int tile_x, int tile_y, int elem_bytes) {
 // injection plane tfsf_z (and tfsf_z + 1, whose recomputed plane below would
 // be the injection plane).
 FusedPlan make_fused_plan(int nx, int ny, int nz, int npml, int tfsf_z, int tile_y, int zchunk,
-                          bool use_slab, bool march) {
+                          int slab_mode, bool march) {
   FusedPlan p;
   memset(&p, 0, sizeof(p));
   p.march = march ? 1 : 0;
-  if (march) use_slab = false;
+  if (march) slab_mode = 0;
+  const bool use_slab = slab_mode == 1;
   const int m = npml;
   InteriorBox& ib = p.interior;
   // rows start on a 128-byte line. Measured against starting at npml + 1
@@ -293,10 +382,43 @@ FusedPlan make_fused_plan(int nx, int ny, int nz, int npml, int tfsf_z, int tile
     }
     return p;
   }
+  auto add = [&](int x0, int x1, int y0, int y1, int z0, int z1) {
+    if (march) add_march_box(p.mshell, x0, x1, y0, y1, z0, z1, kMarchZChunk);
+    else add_shell_box(bl, x0, x1, y0, y1, z0, z1);
+  };
+  auto auto_zchunk = [&](int planes) {
+    // about twelve waves of two resident blocks per SM on 148 SMs (measured
+    // on 203 x 761 x 761: chunks of ~50 planes beat ~60 by 6 %), chunks of
+    // at least 16 planes (each recomputes the plane below it)
+    const long long per_layer = (long long)((ib.xb - ib.xa + kRowCells - 1) / kRowCells) *
+                                ((ib.yb - ib.ya + tile_y - 1) / tile_y);
+    long long layers = (12LL * 2 * 148 + per_layer - 1) / per_layer;
+    layers = std::max(1LL, std::min(layers, (long long)planes / 16));
+    return (int)((planes + layers - 1) / layers);
+  };
+  if (slab_mode == 2) {
+    // the column march: the interior's x-y box over every z plane (z faces,
+    // edges planes and the injection plane in the march); the shell is the
+    // y strips (whole rows) and the x strips beside the box, over every z
+    InteriorBox& cb = p.slab;
+    cb = ib;
+    cb.nz_ranges = 1;
+    cb.z0[0] = 0;
+    cb.z1[0] = nz;
+    cb.zchunk = zchunk > 0 ? zchunk : auto_zchunk(nz);
+    cb.chunks0 = cb.chunks = (nz + cb.zchunk - 1) / cb.zchunk;
+    p.has_slab = 1;
+    p.column = 1;
+    p.has_interior = 0;
+    add(0, nx, 0, ib.ya, 0, nz);
+    add(0, nx, ib.yb, ny, 0, nz);
+    add(0, ib.xa, ib.ya, ib.yb, 0, nz);
+    add(ib.xb, nx, ib.ya, ib.yb, 0, nz);
+    return p;
+  }
   // with use_slab, the z slabs of the same x-y box (CPML in z only):
   // [0, m) and [nz - m, nz), each unless the injection plane lies in it or
-  // is the plane below it (the slab kernel does not inject); otherwise the
-  // split passes sweep the whole slab planes
+  // is the plane below it (those the split passes sweep as whole planes)
   InteriorBox& sb = p.slab;
   sb = ib;
   sb.nz_ranges = 0;
@@ -313,16 +435,7 @@ FusedPlan make_fused_plan(int nx, int ny, int nz, int npml, int tfsf_z, int tile
   p.has_slab = sb.nz_ranges > 0;
   int planes = 0;
   for (int k = 0; k < nzr; ++k) planes += zr[k][1] - zr[k][0];
-  if (zchunk <= 0) {
-    // about twelve waves of two resident blocks per SM on 148 SMs (measured
-    // on 203 x 761 x 761: chunks of ~50 planes beat ~60 by 6 %), chunks of
-    // at least 16 planes (each recomputes the plane below it)
-    const long long per_layer = (long long)((ib.xb - ib.xa + kRowCells - 1) / kRowCells) *
-                                ((ib.yb - ib.ya + tile_y - 1) / tile_y);
-    long long layers = (12LL * 2 * 148 + per_layer - 1) / per_layer;
-    layers = std::max(1LL, std::min(layers, (long long)planes / 16));
-    zchunk = (int)((planes + layers - 1) / layers);
-  }
+  if (zchunk <= 0) zchunk = auto_zchunk(planes);
   ib.zchunk = zchunk;
   ib.nz_ranges = nzr;
   ib.chunks = 0;
@@ -341,10 +454,6 @@ FusedPlan make_fused_plan(int nx, int ny, int nz, int npml, int tfsf_z, int tile
   for (int k = 0; k < nzr; ++k) { cz0[nc] = ib.z0[k]; cz1[nc++] = ib.z1[k]; }
   for (int k = 0; k < sb.nz_ranges; ++k)
     if (sb.z0[k] != 0) { cz0[nc] = sb.z0[k]; cz1[nc++] = sb.z1[k]; }
-  auto add = [&](int x0, int x1, int y0, int y1, int z0, int z1) {
-    if (march) add_march_box(p.mshell, x0, x1, y0, y1, z0, z1, kMarchZChunk);
-    else add_shell_box(bl, x0, x1, y0, y1, z0, z1);
-  };
   int zc = 0;
   for (int k = 0; k < nc; ++k) {
     add(0, nx, 0, ny, zc, cz0[k]);
@@ -379,24 +488,26 @@ bool launch_fused_interior(const State<T>& s, const FusedPlan& p, int tile_y, cu
 }
 
 template <class T>
-bool launch_fused_slab(const State<T>& s, const FusedPlan& p, int tile_y, cudaStream_t st) {
+bool launch_fused_slab(const State<T>& s, const FusedPlan& p, int tile_y, const int* tdev, int toff,
+                       cudaStream_t st) {
   if (!p.has_slab) return true;
   switch (tile_y) {
-    case 4: launch_slab_ty<T, 4>(s, p.slab, st); return true;
-    case 7: launch_slab_ty<T, 7>(s, p.slab, st); return true;
-    case 8: launch_slab_ty<T, 8>(s, p.slab, st); return true;
+    case 4: launch_slab_ty<T, 4>(s, p.slab, tdev, toff, st); return true;
+    case 7: launch_slab_ty<T, 7>(s, p.slab, tdev, toff, st); return true;
+    case 8: launch_slab_ty<T, 8>(s, p.slab, tdev, toff, st); return true;
   }
   if constexpr (sizeof(T) == 4) {
     switch (tile_y) {
-      case 15: launch_slab_ty<T, 15>(s, p.slab, st); return true;
-      case 16: launch_slab_ty<T, 16>(s, p.slab, st); return true;
+      case 15: launch_slab_ty<T, 15>(s, p.slab, tdev, toff, st); return true;
+      case 16: launch_slab_ty<T, 16>(s, p.slab, tdev, toff, st); return true;
     }
   }
   return false;
 }
 
-template bool launch_fused_slab<float>(const State<float>&, const FusedPlan&, int, cudaStream_t);
-template bool launch_fused_slab<double>(const State<double>&, const FusedPlan&, int, cudaStream_t);
+template bool launch_fused_slab<float>(const State<float>&, const FusedPlan&, int, const int*, int, cudaStream_t);
+template bool launch_fused_slab<double>(const State<double>&, const FusedPlan&, int, const int*, int,
+                                        cudaStream_t);
 template bool launch_fused_interior<float>(const State<float>&, const FusedPlan&, int, cudaStream_t);
 template bool launch_fused_interior<double>(const State<double>&, const FusedPlan&, int, cudaStream_t);
 

@@ -101,17 +101,22 @@ struct FusedPlan {
   int has_interior;
   InteriorBox interior;
   int has_slab;
-  InteriorBox slab;   // the z slabs [0, npml), [nz - npml, nz) of the same x-y box
+  InteriorBox slab;   // the z slabs [0, npml), [nz - npml, nz) of the same x-y box, or its column
+  int column;         // slab holds the column march (the whole z extent)
   ShellBoxes shell;   // the shell swept by the split passes (shell mode 1)
   int march;          // shell mode 0: the shell is marched by k_march
   MarchBoxes mshell;  // the shell's boxes for k_march (shell mode 0)
 };
 
-// Interior box, z slabs (with use_slab) and shell boxes of a grid; zchunk 0
-// picks the z chunk. With march, the shell goes to k_march boxes (mshell)
-// and use_slab is ignored; otherwise to the split passes (shell).
+// Interior box, z slabs and shell boxes of a grid; zchunk 0 picks the z
+// chunk. slab 0: no z-slab march; 1: the z slabs of the interior's x-y box
+// marched (FDTD_OPT_FUSED_SLAB = 1); 2: the column march, the whole z
+// extent of the interior's x-y box in one march (slab box, has_interior 0),
+// the shell then only the x and y strips. With march, the shell goes to
+// k_march boxes (mshell) and slab is ignored; otherwise to the split
+// passes (shell).
 FusedPlan make_fused_plan(int nx, int ny, int nz, int npml, int tfsf_z, int tile_y, int zchunk,
-                          bool use_slab, bool march = false);
+                          int slab, bool march = false);
 
 // Appends the box [x0, x1) x [y0, y1) x [z0, z1) to a march box list: the
 // row width (32, 16 or 8 lanes) that pads the box least, z chunks of about
@@ -135,7 +140,8 @@ bool fused_supported_tile(int tile_x, int tile_y, int elem_bytes);
 template <class T>
 bool launch_fused_interior(const State<T>& s, const FusedPlan& p, int tile_y, cudaStream_t st);
 template <class T>
-bool launch_fused_slab(const State<T>& s, const FusedPlan& p, int tile_y, cudaStream_t st);
+bool launch_fused_slab(const State<T>& s, const FusedPlan& p, int tile_y, const int* tdev, int toff,
+                       cudaStream_t st);
 
 // Appends the box [x0, x1) x [y0, y1) x [z0, z1) to a box list, with the
 // row width (32, 16, 8 or 4 lanes) that pads x the least.

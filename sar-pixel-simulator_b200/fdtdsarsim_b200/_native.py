@@ -546,12 +546,14 @@ def bounds_check_enabled():
 def fused_plan_boxes(nx, ny, nz, npml, tfsf_z, tile_y=4, zchunk=0, slab=False, march=False):
     """(kind, x0, x1, y0, y1, z0, z1) rows of the fused step's boxes
     (fdtd_fused_plan_boxes; host computation, no device needed): kind 0
-    interior march, 1 CPML z slab march, 2 split-pass shell box, 3 general
-    march shell box. ``march`` gives the default step's plan (shell marched);
-    otherwise the split-pass shell, with ``slab`` the z slabs marched."""
+    interior march, 1 CPML z slab march (with ``slab=2`` the column march),
+    2 split-pass shell box, 3 general march shell box. ``march`` gives the
+    plan with the shell marched; otherwise the split-pass shell, with
+    ``slab`` 1 the z slabs marched, 2 the column march
+    (FDTD_OPT_FUSED_SLAB)."""
     out = np.zeros((64, 7), np.int32)
     n = ctypes.c_int(0)
-    mode = 2 if march else int(bool(slab))
+    mode = 2 if march else (3 if int(slab) == 2 else int(bool(slab)))
     check(lib.fdtd_fused_plan_boxes(int(nx), int(ny), int(nz), int(npml), int(tfsf_z), int(tile_y),
                                     int(zchunk), mode, ptr(out), out.shape[0], ctypes.byref(n)))
     return out[:n.value].copy()

@@ -22,7 +22,8 @@ _MARCH, _SPLIT = _native.SHELL_MARCH, _native.SHELL_SPLIT
 
 # (kernel, tile_y, zchunk, slab, shell); zchunk 0 lets the library pick;
 # shell: the fused step's shell marched (_MARCH) or swept by the split
-# passes (_SPLIT), then slab 1 marches the CPML z slabs
+# passes (_SPLIT), then slab 1 marches the CPML z slabs, slab 2 the whole
+# z extent of the interior's x-y box (the column march)
 CANDIDATES = [
     (_native.FDTD_KERNEL_SPLIT, 4, 0, 0, _MARCH),
     (_native.FDTD_KERNEL_FUSED, 4, 0, 0, _MARCH),
@@ -31,10 +32,11 @@ CANDIDATES = [
     (_native.FDTD_KERNEL_FUSED, 4, 0, 0, _SPLIT),
     (_native.FDTD_KERNEL_FUSED, 8, 0, 0, _SPLIT),
     (_native.FDTD_KERNEL_FUSED, 4, 0, 1, _SPLIT),
+    (_native.FDTD_KERNEL_FUSED, 4, 0, 2, _SPLIT),
 ]
 
 # cache entries measured with another candidate set are measured again
-_VERSION = 'v2'
+_VERSION = 'v3'
 
 
 def cache_path():

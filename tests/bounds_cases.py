@@ -32,6 +32,8 @@ PATHS = [
     ('fused_split_shell', dict(kernel=FUSED, tile=(32, 4), shell=_native.SHELL_SPLIT)),
     ('fused_march_shell', dict(kernel=FUSED, tile=(32, 8), shell=_native.SHELL_MARCH)),
     ('fused_zchunk_3', dict(kernel=FUSED, tile=(32, 4), zchunk=3, shell=_native.SHELL_MARCH)),
+    ('fused_column', dict(kernel=FUSED, tile=(32, 4), slab=2, shell=_native.SHELL_SPLIT)),
+    ('fused_column_zchunk_3', dict(kernel=FUSED, tile=(32, 4), zchunk=3, slab=2, shell=_native.SHELL_SPLIT)),
 ]
 
 

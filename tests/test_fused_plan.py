@@ -17,19 +17,23 @@ GRIDS = [
 ]
 
 
-@pytest.mark.parametrize('mode', ['shell', 'slab', 'march'])
+@pytest.mark.parametrize('mode', ['shell', 'slab', 'march', 'column'])
 @pytest.mark.parametrize('tile_y', [4, 8])
 @pytest.mark.parametrize('grid', GRIDS)
 def test_boxes_partition_the_grid(grid, tile_y, mode):
     nx, ny, nz, m, tfsf = grid
-    boxes = _native.fused_plan_boxes(nx, ny, nz, m, tfsf, tile_y, slab=mode == 'slab',
-                                     march=mode == 'march')
+    slab = {'slab': 1, 'column': 2}.get(mode, 0)
+    boxes = _native.fused_plan_boxes(nx, ny, nz, m, tfsf, tile_y, slab=slab, march=mode == 'march')
     # the march plan sends the whole shell to the general march, the others
     # to the split passes
     shell_kind = 3 if mode == 'march' else 2
     assert set(boxes[:, 0]) <= {0, 1, shell_kind}
-    if mode != 'slab':
+    if mode not in ('slab', 'column'):
         assert 1 not in boxes[:, 0]
+    if mode == 'column' and (boxes[:, 0] == 1).any():
+        # the column march replaces the interior march and spans every plane
+        assert 0 not in boxes[:, 0]
+        assert [tuple(b[5:]) for b in boxes if b[0] == 1] == [(0, nz)]
     count = np.zeros((nz, ny, nx), np.int32)
     for kind, x0, x1, y0, y1, z0, z1 in boxes:
         assert x0 % 4 == 0
@@ -37,9 +41,10 @@ def test_boxes_partition_the_grid(grid, tile_y, mode):
         if kind in (0, 1):
             # no x / y face at the box or at the halo it recomputes
             assert x0 - 1 >= m - 1 and x1 <= nx - m and y0 - 1 >= m - 1 and y1 <= ny - m
-            assert not (z0 - 1 <= tfsf < z1), (kind, z0, z1)
+            if mode != 'column':   # the column march injects; the others keep clear
+                assert not (z0 - 1 <= tfsf < z1), (kind, z0, z1)
         if kind == 0:   # the interior: no z face either
             assert z0 - 1 >= m - 1 and z1 <= nz - m
     assert (count == 1).all()
     if nx - m >= 36:   # room for a 32-aligned interior start
-        assert (boxes[:, 0] == 0).any()
+        assert (boxes[:, 0] == (1 if mode == 'column' else 0)).any()

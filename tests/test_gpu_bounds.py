@@ -1,5 +1,5 @@
 """The bounds-checked build (libfdtd_b200_check.so) on tiny and ragged
-grids: every step path (split, fused with the split-pass shell, fused with
+grids: every step path (split, fused with the split-pass shell, the column march, fused with
 the marched shell, one-plane z chunks, the batched tile queue) runs with
 every global access of its kernels checked against the library's live
 allocations and every shared index against its array, and must report no

@@ -99,18 +99,46 @@ def test_march_shell_tiles(tile_y):
         sim.close()
 
 
+@pytest.mark.parametrize('slab', [1, 2])
 @pytest.mark.parametrize('case', CASES + WIDE)
-def test_fused_slab_matches_oracle_bit_exact(case):
-    """FDTD_OPT_FUSED_SLAB: the CPML z slabs marched by the slab kernel."""
+def test_fused_slab_matches_oracle_bit_exact(case, slab):
+    """FDTD_OPT_FUSED_SLAB: 1, the CPML z slabs marched by the slab kernel;
+    2, the column march (the interior's x-y box over every plane, z faces,
+    domain edge planes and injection plane in the march)."""
     pc = make_params(*case[:6], dtype=case[6])
     _, _, ca, cb, inc = random_problem(pc, 71)
     o = oracle_for(pc)
     o.run(ca, cb, inc, pc.geom_params.size_t)
-    sim = native_for(pc, FUSED, (32, 4), slab=True)
+    sim = native_for(pc, FUSED, (32, 4), slab=slab)
     try:
         sim.set_materials(ca, cb)
         sim.set_incident(inc['ex'], inc['ey'], inc['hx'], inc['hy'])
         sim.run(pc.geom_params.size_t)
+        sim.synchronize()
+        for c in ('ex', 'ey', 'ez', 'hx', 'hy', 'hz'):
+            assert bits_equal(sim.get_field(c), getattr(o, c)), c
+        for k, name in enumerate(_native.PHASOR_NAMES):
+            assert bits_equal(sim.get_phasor(k), o.ph[name]), name
+    finally:
+        sim.close()
+
+
+@pytest.mark.parametrize('zchunk', [1, 3, 7])
+@pytest.mark.parametrize('case', [WIDE[0], WIDE[3], WIDE[4], WIDE[7]])
+def test_column_march_chunks_start_anywhere(case, zchunk):
+    """The column march in short z chunks: chunks start on the injection
+    plane, the plane above it, inside the CPML slabs and at plane 0; each
+    recomputes the plane below it with every plane-uniform term."""
+    pc = make_params(*case[:6], dtype=case[6])
+    _, _, ca, cb, inc = random_problem(pc, 73 + zchunk)
+    o = oracle_for(pc)
+    steps = min(pc.geom_params.size_t, 12)
+    o.run(ca, cb, inc, steps)
+    sim = native_for(pc, FUSED, (32, 4), zchunk=zchunk, slab=2)
+    try:
+        sim.set_materials(ca, cb)
+        sim.set_incident(inc['ex'], inc['ey'], inc['hx'], inc['hy'])
+        sim.run(steps)
         sim.synchronize()
         for c in ('ex', 'ey', 'ez', 'hx', 'hy', 'hz'):
             assert bits_equal(sim.get_field(c), getattr(o, c)), c
