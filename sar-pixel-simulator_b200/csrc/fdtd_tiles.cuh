@@ -114,6 +114,240 @@ __device__ __forceinline__ void interior_tile(const State<T>& s, const InteriorB
 }
 
 
+// One tile of a z-slab or column box (the slab march, fdtd_fused.cu): tile
+// (bx, by) of the box's x-y tiling and z chunk bz, by 32 x (TY + 1)
+// threads (lane, row r), the step being t. Plain planes take the interior
+// march's update; planes in a z face, the domain's edge planes and the
+// injection plane take the general one. sEx, sEz, sHx, sHz: shared arrays
+// of (TY + 1) * 128 elements each, as interior_tile's.
+template <class T, int TY>
+__device__ __forceinline__ void slab_tile(const State<T>& s, const InteriorBox& ib, int t, int lane, int r,
+                                          int bx, int by, int bz, T* sEx, T* sEz, T* sHx, T* sHz) {
+  using M = R<T>;
+  const int nz = s.nz, m = s.npml;
+  const int x0 = ib.xa + bx * kRowCells + lane * kVec;
+  const int y = ib.ya + by * TY + r - 1;
+  int c = bz, k = 0;
+  if (c >= ib.chunks0) { c -= ib.chunks0; k = 1; }
+  const int z0 = ib.z0[k] + c * ib.zchunk;
+  const int z1 = min(ib.z1[k], z0 + ib.zchunk);
+  const int zs = max(z0 - 1, 0);   // a chunk at plane 0 has nothing below
+  const bool vin = x0 < s.pitch && y < s.ny;
+  const bool own = vin && r >= 1 && y < ib.yb && x0 < ib.xb;
+  const long long P = s.plane, W = s.pitch;
+  long long i = (long long)zs * P + (vin ? (long long)y * W + x0 : 0);
+  const int so = lane * kVec;
+
+  EVec<T> e;
+  HVec<T> h;
+  T ezz[kVec];
+  if (vin) { ld4(e.ex, s.iex + i); ld4(e.ey, s.iey + i); ld4(e.ez, s.iez + i); }
+  else { zero4(e.ex); zero4(e.ey); zero4(e.ez); }
+  zero4(h.hxz); zero4(h.hyz);
+
+  for (int z = zs; z < z1; ++z, i += P) {
+    const bool work = own && z >= z0;
+    if (z >= m && z < nz - m && !(z == s.tfsf_z && t < s.nt_inc)) {
+      // a plane with no z face, no domain edge and no injection: the
+      // interior march's plain update (the same operations as below, with
+      // every plane-dependent term absent)
+      if (vin) {
+        ld4(e.exz, s.iex + i + P); ld4(e.eyz, s.iey + i + P); ld4(ezz, s.iez + i + P);
+        ld4(h.hx, s.ihx + i); ld4(h.hy, s.ihy + i); ld4(h.hz, s.ihz + i);
+      } else {
+        zero4(e.exz); zero4(e.eyz); zero4(ezz); zero4(h.hx); zero4(h.hy); zero4(h.hz);
+      }
+      T ca[kVec], cb[kVec];
+      if (work) { ld4(ca, s.ca + i); ld4(cb, s.cb + i); }
+      else { zero4(ca); zero4(cb); }
+      if (r == TY) {
+        if (vin && y + 1 < s.ny) { ld4(e.exy, s.iex + i + W); ld4(e.ezy, s.iez + i + W); }
+        else { zero4(e.exy); zero4(e.ezy); }
+      }
+      T eyr = T(0), ezr = T(0);
+      if (lane == kLanes - 1 && vin && x0 + kVec < s.pitch) { eyr = ldc(s.iey + (i + kVec)); ezr = ldc(s.iez + (i + kVec)); }
+      T gx = T(0), gy = T(0), gz = T(0), gxz = T(0), gxy = T(0), ghy = T(0), ghz = T(0);
+      if (work && lane == 0) {
+        const long long j = i - 1;
+        gx = ldc(s.iex + (j)); gy = ldc(s.iey + (j)); gz = ldc(s.iez + (j));
+        ghy = ldc(s.ihy + (j)); ghz = ldc(s.ihz + (j));
+        gxz = ldc(s.iex + (j + P)); gxy = ldc(s.iex + (j + W));
+      }
+      st4(&sEx[r * kRowCells + so], e.ex);
+      st4(&sEz[r * kRowCells + so], e.ez);
+      __syncthreads();
+      if (r < TY) { ld4(e.exy, &sEx[(r + 1) * kRowCells + so]); ld4(e.ezy, &sEz[(r + 1) * kRowCells + so]); }
+      e.eyn = __shfl_down_sync(kFullMask, e.ey[0], 1);
+      e.ezn = __shfl_down_sync(kFullMask, e.ez[0], 1);
+      if (lane == kLanes - 1) { e.eyn = eyr; e.ezn = ezr; }
+      h_vec_interior(s, e, h.hx, h.hy, h.hz);
+      st4(&sHx[r * kRowCells + so], h.hx);
+      st4(&sHz[r * kRowCells + so], h.hz);
+      __syncthreads();
+      h.hyp = __shfl_up_sync(kFullMask, h.hy[kVec - 1], 1);
+      h.hzp = __shfl_up_sync(kFullMask, h.hz[kVec - 1], 1);
+      if (work) {
+        ld4(h.hxy, &sHx[(r - 1) * kRowCells + so]);
+        ld4(h.hzy, &sHz[(r - 1) * kRowCells + so]);
+        if (lane == 0) {
+          h.hyp = M::sub(ghy, M::mul(s.db, M::sub(M::sub(gxz, gx), M::sub(e.ez[0], gz))));
+          h.hzp = M::sub(ghz, M::mul(s.db, M::sub(M::sub(e.ey[0], gy), M::sub(gxy, gx))));
+        }
+        e_vec_interior(h, ca, cb, e.ex, e.ey, e.ez);
+        st4(s.ohx + i, h.hx); st4(s.ohy + i, h.hy); st4(s.ohz + i, h.hz);
+        st4(s.oex + i, e.ex); st4(s.oey + i, e.ey); st4(s.oez + i, e.ez);
+      }
+      copy4(e.ex, e.exz); copy4(e.ey, e.eyz); copy4(e.ez, ezz);
+      copy4(h.hxz, h.hx); copy4(h.hyz, h.hy);
+      continue;
+    }
+    const bool top = z + 1 >= nz;   // last plane: nothing above, nothing updated
+    // update ranges and CPML faces of plane z (uniform over the plane)
+    const bool h_xy = z < nz - 1, h_z = z >= 1 && z < nz - 1;
+    const bool e_xy = z >= 1 && z < nz - 1, e_z = z < nz - 1;
+    const bool hf = z < nz - 1 && (z < m - 1 || z >= nz - m);
+    const bool ef = z < nz - 1 && ((z >= 1 && z < m) || z >= nz - m);
+    const int hside = z < m - 1 ? 0 : 1, hq = hside ? z - (nz - m) : z;
+    const int eside = z < m ? 0 : 1, eq = eside ? z - (nz - m) : z;
+    const bool inj = z == s.tfsf_z && t < s.nt_inc;   // injection plane
+    const long long ki = ((long long)t * s.ny + y) * W + x0;   // incident planes (t, y, x)
+    if (vin && !top) {
+      ld4(e.exz, s.iex + i + P); ld4(e.eyz, s.iey + i + P); ld4(ezz, s.iez + i + P);
+    } else {
+      zero4(e.exz); zero4(e.eyz); zero4(ezz);
+    }
+    if (vin) { ld4(h.hx, s.ihx + i); ld4(h.hy, s.ihy + i); ld4(h.hz, s.ihz + i); }
+    else { zero4(h.hx); zero4(h.hy); zero4(h.hz); }
+    T ca[kVec], cb[kVec];
+    if (work) { ld4(ca, s.ca + i); ld4(cb, s.cb + i); }
+    else { zero4(ca); zero4(cb); }
+    if (r == TY) {
+      if (vin && y + 1 < s.ny) { ld4(e.exy, s.iex + i + W); ld4(e.ezy, s.iez + i + W); }
+      else { zero4(e.exy); zero4(e.ezy); }
+    }
+    T eyr = T(0), ezr = T(0);
+    if (lane == kLanes - 1 && vin && x0 + kVec < s.pitch) { eyr = ldc(s.iey + (i + kVec)); ezr = ldc(s.iez + (i + kVec)); }
+    T gx = T(0), gy = T(0), gz = T(0), gxz = T(0), gxy = T(0), ghy = T(0), ghz = T(0), gpy = T(0), gix = T(0);
+    if (work && lane == 0) {
+      const long long j = i - 1;
+      gx = ldc(s.iex + (j)); gy = ldc(s.iey + (j)); gz = ldc(s.iez + (j));
+      ghy = ldc(s.ihy + (j)); ghz = ldc(s.ihz + (j));
+      gxz = top ? T(0) : ldc(s.iex + (j + P));
+      gxy = ldc(s.iex + (j + W));
+      if (hf) gpy = ldc(s.ps.z[hside][3] + (((long long)hq * s.ny + y) * W + x0 - 1));
+      if (inj) gix = ldc(s.inc_ex + (ki - 1));
+    }
+    // ---- H^{n+1/2}(z) -----------------------------------------------------
+    st4(&sEx[r * kRowCells + so], e.ex);
+    st4(&sEz[r * kRowCells + so], e.ez);
+    __syncthreads();
+    if (r < TY) { ld4(e.exy, &sEx[(r + 1) * kRowCells + so]); ld4(e.ezy, &sEz[(r + 1) * kRowCells + so]); }
+    e.eyn = __shfl_down_sync(kFullMask, e.ey[0], 1);
+    e.ezn = __shfl_down_sync(kFullMask, e.ez[0], 1);
+    if (lane == kLanes - 1) { e.eyn = eyr; e.ezn = ezr; }
+    {
+      T hx[kVec], hy[kVec], hz[kVec];
+      copy4(hx, h.hx); copy4(hy, h.hy); copy4(hz, h.hz);
+      h_vec_interior(s, e, hx, hy, hz);
+      if (h_xy) { copy4(h.hx, hx); copy4(h.hy, hy); }
+      if (h_z) copy4(h.hz, hz);
+    }
+    if (hf) {   // z faces: psi_Hyz from dEx/dz, psi_Hxz from dEy/dz
+      const long long kq = ((long long)hq * s.ny + y) * W + x0;
+      const T b = s.prof[hside ? BH_U : BH_D][hq];
+      const T c = s.prof[hside ? CH_U : CH_D][hq];
+      T p3[kVec], p2[kVec];
+      if (vin) { ld4(p3, s.ps.z[hside][3] + kq); ld4(p2, s.ps.z[hside][2] + kq); }
+      else { zero4(p3); zero4(p2); }
+#pragma unroll
+      for (int j = 0; j < kVec; ++j) {
+        p3[j] = M::add(M::mul(b, p3[j]), div_dx(s, M::mul(c, M::sub(e.exz[j], e.ex[j]))));
+        p2[j] = M::add(M::mul(b, p2[j]), div_dx(s, M::mul(c, M::sub(e.eyz[j], e.ey[j]))));
+        h.hy[j] = M::sub(h.hy[j], M::mul(s.dtm0, p3[j]));
+        h.hx[j] = M::add(h.hx[j], M::mul(s.dtm0, p2[j]));
+      }
+      if (work) { st4(s.pd.z[hside][3] + kq, p3); st4(s.pd.z[hside][2] + kq, p2); }
+    }
+    if (inj) {   // E-field injection into H (cpu/main_sim.py:147-150)
+      T iey[kVec], iex[kVec];
+      if (vin) { ld4(iey, s.inc_ey + ki); ld4(iex, s.inc_ex + ki); }
+      else { zero4(iey); zero4(iex); }
+#pragma unroll
+      for (int j = 0; j < kVec; ++j) {
+        if (x0 + j >= s.nx) continue;
+        h.hx[j] = M::add(h.hx[j], M::mul(s.db, iey[j]));
+        h.hy[j] = M::sub(h.hy[j], M::mul(s.db, iex[j]));
+      }
+    }
+    st4(&sHx[r * kRowCells + so], h.hx);
+    st4(&sHz[r * kRowCells + so], h.hz);
+    __syncthreads();
+    // ---- E^{n+1}(z) ---------------------------------------------------------
+    h.hyp = __shfl_up_sync(kFullMask, h.hy[kVec - 1], 1);
+    h.hzp = __shfl_up_sync(kFullMask, h.hz[kVec - 1], 1);
+    if (work) {
+      ld4(h.hxy, &sHx[(r - 1) * kRowCells + so]);
+      ld4(h.hzy, &sHz[(r - 1) * kRowCells + so]);
+      if (lane == 0) {   // hy, hz at x0 - 1, with the z-face term of hy
+        T hyp = ghy, hzp = ghz;
+        if (h_xy) {
+          hyp = M::sub(ghy, M::mul(s.db, M::sub(M::sub(gxz, gx), M::sub(e.ez[0], gz))));
+          if (hf) {
+            const T b = s.prof[hside ? BH_U : BH_D][hq];
+            const T c = s.prof[hside ? CH_U : CH_D][hq];
+            const T p3 = M::add(M::mul(b, gpy), div_dx(s, M::mul(c, M::sub(gxz, gx))));
+            hyp = M::sub(hyp, M::mul(s.dtm0, p3));
+          }
+        }
+        if (inj) hyp = M::sub(hyp, M::mul(s.db, gix));
+        if (h_z) hzp = M::sub(ghz, M::mul(s.db, M::sub(M::sub(e.ey[0], gy), M::sub(gxy, gx))));
+        h.hyp = hyp;
+        h.hzp = hzp;
+      }
+      T ex[kVec], ey[kVec], ez[kVec];
+      copy4(ex, e.ex); copy4(ey, e.ey); copy4(ez, e.ez);
+      e_vec_interior(h, ca, cb, ex, ey, ez);
+      T ox[kVec], oy[kVec], oz[kVec];
+      copy4(ox, e.ex); copy4(oy, e.ey); copy4(oz, e.ez);
+      if (e_xy) { copy4(ox, ex); copy4(oy, ey); }
+      if (e_z) copy4(oz, ez);
+      if (ef) {   // z faces: psi_Eyz from dHx/dz, psi_Exz from dHy/dz
+        const long long kq = ((long long)eq * s.ny + y) * W + x0;
+        const T b = s.prof[eside ? BE_U : BE_D][eq];
+        const T c = s.prof[eside ? CE_U : CE_D][eq];
+        T p1[kVec], p0[kVec];
+        ld4(p1, s.ps.z[eside][1] + kq);
+        ld4(p0, s.ps.z[eside][0] + kq);
+#pragma unroll
+        for (int j = 0; j < kVec; ++j) {
+          const T cbdx = M::mul(cb[j], s.dx);
+          p1[j] = M::add(M::mul(b, p1[j]), div_dx(s, M::mul(c, M::sub(h.hx[j], h.hxz[j]))));
+          p0[j] = M::add(M::mul(b, p0[j]), div_dx(s, M::mul(c, M::sub(h.hy[j], h.hyz[j]))));
+          oy[j] = M::add(oy[j], M::mul(cbdx, p1[j]));
+          ox[j] = M::sub(ox[j], M::mul(cbdx, p0[j]));
+        }
+        st4(s.pd.z[eside][1] + kq, p1);
+        st4(s.pd.z[eside][0] + kq, p0);
+      }
+      if (inj) {   // H-field injection into E (cpu/main_sim.py:158-161)
+        T ihx[kVec], ihy[kVec];
+        ld4(ihx, s.inc_hx + ki);
+        ld4(ihy, s.inc_hy + ki);
+#pragma unroll
+        for (int j = 0; j < kVec; ++j) {
+          if (x0 + j >= s.nx) continue;
+          oy[j] = M::add(oy[j], M::mul(s.dte0dx, ihx[j]));
+          ox[j] = M::sub(ox[j], M::mul(s.dte0dx, ihy[j]));
+        }
+      }
+      st4(s.ohx + i, h.hx); st4(s.ohy + i, h.hy); st4(s.ohz + i, h.hz);
+      st4(s.oex + i, ox); st4(s.oey + i, oy); st4(s.oez + i, oz);
+    }
+    copy4(e.ex, e.exz); copy4(e.ey, e.eyz); copy4(e.ez, ezz);
+    copy4(h.hxz, h.hx); copy4(h.hyz, h.hy);
+  }
+}
+
 // Dynamic shared memory of a march tile, in elements of T: the four
 // exchange arrays, then two stages of the per-thread staging area. A stage
 // holds, per thread, kSlots vectors (E(z+1) x, y, z; H(z) x, y, z; Ca, Cb;
